@@ -1,0 +1,111 @@
+"""ctypes binding of libdmffb200.so (the C ABI declared in include/dmffb200.h).
+
+The shared library is built in-tree by ``dmff_b200/csrc/build.sh`` (or ``__graft_entry__.build``).
+There is no CPU fallback: importing the engine without the library raises immediately.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdmffb200.so")
+
+DMFFB_OK = 0
+DMFFB_BAD_ARG = 1
+DMFFB_OOM = 2
+DMFFB_CUDA_ERROR = 3
+DMFFB_NOT_CONVERGED = 4
+DMFFB_NEIGHBOR_OVERFLOW = 5
+DMFFB_NONFINITE = 6
+DMFFB_CUFFT_ERROR = 7
+
+DMFFB_FP32 = 0
+DMFFB_FP64 = 1
+DMFFB_SOLVER_CG = 0
+DMFFB_SOLVER_REFERENCE = 1
+
+# every function the header declares (checked by the CPU test suite)
+EXPORTED = [
+    "dmffb_admp_create", "dmffb_destroy", "dmffb_last_error", "dmffb_admp_set_params",
+    "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
+    "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
+]
+
+
+class AdmpDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int32),
+        ("lmax", ctypes.c_int32),
+        ("lpol", ctypes.c_int32),
+        ("lpme", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("rc", ctypes.c_double),
+        ("kappa", ctypes.c_double),
+        ("K", ctypes.c_int32 * 3),
+        ("axis_types", ctypes.POINTER(ctypes.c_int32)),
+        ("axis_indices", ctypes.POINTER(ctypes.c_int32)),
+        ("n_cov", ctypes.c_int64),
+        ("cov_rows", ctypes.POINTER(ctypes.c_int32)),
+        ("mscales", ctypes.c_double * 6),
+        ("pscales", ctypes.c_double * 6),
+        ("dscales", ctypes.c_double * 6),
+        ("solver", ctypes.c_int32),
+        ("cg_tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32),
+        ("steps_pol", ctypes.c_int32),
+    ]
+
+
+class AdmpResult(ctypes.Structure):
+    _fields_ = [
+        ("energy", ctypes.c_double),
+        ("e_real", ctypes.c_double),
+        ("e_recip", ctypes.c_double),
+        ("e_self", ctypes.c_double),
+        ("e_pol", ctypes.c_double),
+        ("box_grad", ctypes.c_double * 9),
+        ("n_iter", ctypes.c_int32),
+        ("converged", ctypes.c_int32),
+        ("residual_rms", ctypes.c_double),
+        ("n_pairs", ctypes.c_int64),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """Load the engine library; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libdmffb200.so not found at {LIB_PATH}; build it with dmff_b200/csrc/build.sh")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+    P = ctypes.POINTER
+    lib.dmffb_admp_create.argtypes = [P(AdmpDesc), P(vp)]
+    lib.dmffb_admp_create.restype = ctypes.c_int
+    lib.dmffb_destroy.argtypes = [vp]
+    lib.dmffb_destroy.restype = None
+    lib.dmffb_last_error.argtypes = [vp]
+    lib.dmffb_last_error.restype = ctypes.c_char_p
+    lib.dmffb_admp_set_params.argtypes = [vp, vp, vp, vp]
+    lib.dmffb_admp_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp, P(AdmpResult)]
+    lib.dmffb_admp_compute_host.argtypes = [vp, vp, vp, vp, i64, vp, vp, P(AdmpResult)]
+    lib.dmffb_admp_field.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp]
+    lib.dmffb_admp_multipole_grads.argtypes = [vp, vp, vp, vp]
+    lib.dmffb_build_neighbors.argtypes = [vp, vp, vp, vp, dbl, vp, i64, P(i64)]
+    lib.dmffb_admp_build_neighbors.argtypes = [vp, vp, vp, vp]
+    lib.dmffb_get_timings.argtypes = [vp, P(dbl), i32]
+    lib.dmffb_set_timing.argtypes = [vp, i32]
+    for name in EXPORTED:
+        if name not in ("dmffb_destroy", "dmffb_last_error"):
+            getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+class EngineError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"dmffb status {status}: {msg}")
+        self.status = status

@@ -1,0 +1,173 @@
+"""ADMPPmeForce backed by the B200 engine (drop-in for dmff/admp/pme.py:36-423).
+
+``get_energy`` keeps the reference's signature (positions and box in Angstrom, Q_local per
+atom, pol, tholes, m/p/dScales, U_init, aux) and returns a torch scalar whose autograd yields
+dE/dpositions and dE/dbox (the reference's jax.value_and_grad over those arguments).  The
+induced dipoles are solved on the GPU: by CG to ``cg_tol`` (default) or with the reference's
+fixed-step iteration (``pol_solver='reference'``); as in the reference (pme.py:212-213) the
+gradients treat the converged dipoles as constants (Hellmann-Feynman).
+"""
+import math
+
+import numpy as np
+import torch
+
+from ..engine import AdmpEngine
+
+DIELECTRIC = 1389.35455846
+POL_CONV = 1.0  # dmff/admp/settings.py:2
+MAX_N_POL = 30  # dmff/admp/settings.py:3
+
+
+def setup_ewald_parameters(rc, ethresh, box=None, spacing=None, method="openmm"):
+    """dmff/admp/pme.py:426-492 (float64 host arithmetic)."""
+    if method == "openmm":
+        kappa = math.sqrt(-math.log(2 * ethresh)) / rc
+        box = np.asarray(box, dtype=np.float64)
+        K = [int(math.ceil(2 * kappa * box[d, d] / 3 / ethresh ** 0.2)) for d in range(3)]
+        return kappa, K[0], K[1], K[2]
+    if method == "gromacs":
+        kappa, i = 5.0, 0
+        while math.erfc(kappa * rc) > ethresh:
+            i += 1
+            kappa *= 2
+        low, high = 0.0, kappa
+        for _ in range(i + 60):
+            kappa = (low + high) / 2
+            if math.erfc(kappa * rc) > ethresh:
+                low = kappa
+            else:
+                high = kappa
+        box = np.asarray(box, dtype=np.float64)
+        K = [int(math.ceil(box[d, d] / spacing)) for d in range(3)]
+        return kappa, K[0], K[1], K[2]
+    raise ValueError(f"Invalid method: {method}.Valid methods: 'openmm', 'gromacs'")
+
+
+def _as_cuda_pairs(pairs, device):
+    if pairs is None:
+        return None
+    if torch.is_tensor(pairs):
+        p = pairs
+    else:
+        p = torch.as_tensor(np.asarray(pairs))
+    p = p[:, :3].to(device=device, dtype=torch.int32)
+    return p.contiguous()
+
+
+class _AdmpEnergy(torch.autograd.Function):
+    """E(positions, box); backward returns -forces and dE/dbox from the engine's forward pass."""
+
+    @staticmethod
+    def forward(ctx, positions, box, force, pairs, U0, aux):
+        dev = force.engine.device
+        pos = positions.detach().to(device=dev, dtype=torch.float64).contiguous()
+        U = None
+        if force.lpol:
+            U = (U0.detach().to(device=dev, dtype=torch.float64).contiguous().clone() if U0 is not None
+                 else torch.zeros((force.n_atoms, 3), dtype=torch.float64, device=dev))
+        res, forces, U = force.engine.compute(pos, box, pairs=pairs, U=U)
+        force.last_result = res
+        if aux is not None:
+            aux["U_ind_A"] = U
+            aux["lconverg"] = bool(res.converged)
+            aux["n_cycle"] = int(res.n_iter)
+        ctx.save_for_backward(forces.clone())
+        ctx.box_grad = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
+        ctx.pos_device, ctx.box_device = positions.device, box.device if torch.is_tensor(box) else None
+        return torch.tensor(res.energy, dtype=torch.float64, device=positions.device)
+
+    @staticmethod
+    def backward(ctx, g):
+        (forces,) = ctx.saved_tensors
+        gpos = (-forces * g.to(forces.device)).to(ctx.pos_device)
+        gbox = None
+        if ctx.box_device is not None:
+            gbox = (ctx.box_grad.to(ctx.box_device) * g.to(ctx.box_device))
+        return gpos, gbox, None, None, None, None
+
+
+class ADMPPmeForce:
+    def __init__(self, box, map_atomtype, axis_type, axis_indices, rc, ethresh, lmax, lpol=False, lpme=True,
+                 steps_pol=None, has_aux=False, cov_rows=None, precision="fp32", pol_solver="cg", cg_tol=1e-6,
+                 max_iter=500, device=None):
+        self.map_atomtype = np.asarray(map_atomtype)
+        self.axis_type = np.asarray(axis_type)
+        self.axis_indices = None if axis_indices is None else np.asarray(axis_indices)
+        self.rc = rc
+        self.ethresh = ethresh
+        self.lmax = int(lmax)
+        self.lpme = lpme
+        if lpme:
+            self.kappa, self.K1, self.K2, self.K3 = setup_ewald_parameters(rc, ethresh, box)
+        else:
+            self.kappa, self.K1, self.K2, self.K3 = 0.0, 0, 0, 0
+        self.pme_order = 6
+        self.lpol = lpol
+        self.steps_pol = steps_pol
+        self.n_atoms = len(self.axis_type)
+        self.has_aux = has_aux
+        self.cov_rows = np.zeros((0, 3), np.int32) if cov_rows is None else np.asarray(cov_rows)
+        self.precision = precision
+        self.pol_solver = pol_solver if steps_pol is None else "reference"
+        self.cg_tol = cg_tol if self.pol_solver == "cg" else POL_CONV
+        self.max_iter = max_iter if self.pol_solver == "cg" else MAX_N_POL
+        self.device = device
+        self.U_ind = torch.zeros((self.n_atoms, 3), dtype=torch.float64)
+        self._engine = None
+        self._param_key = None
+        self.last_result = None
+
+    @property
+    def engine(self):
+        if self._engine is None:
+            self._engine = AdmpEngine(
+                self.n_atoms, self.lmax, self.lpol, self.lpme, self.rc, self.kappa, (self.K1, self.K2, self.K3),
+                self.axis_type if self.lmax > 0 else None, self.axis_indices if self.lmax > 0 else None,
+                self.cov_rows, [0, 0, 1, 1, 1, 1], precision=self.precision, solver=self.pol_solver,
+                cg_tol=self.cg_tol, max_iter=self.max_iter, steps_pol=self.steps_pol, device=self.device)
+        return self._engine
+
+    def _sync_params(self, Q_local, pol, tholes, mScales, pScales, dScales):
+        key = tuple(None if t is None else (t.data_ptr() if torch.is_tensor(t) else id(t), getattr(t, "_version", 0))
+                    for t in (Q_local, pol, tholes)) + tuple(
+            tuple(np.asarray(torch.as_tensor(s).detach().cpu()).tolist()) if s is not None else None
+            for s in (mScales, pScales, dScales))
+        if key == self._param_key:
+            return
+        eng = self.engine
+        d = eng.lib  # scales are part of the description: rebuild when they change
+        ms = np.asarray(torch.as_tensor(mScales).detach().cpu(), np.float64)
+        ps = np.asarray(torch.as_tensor(pScales).detach().cpu(), np.float64) if pScales is not None else None
+        ds = np.asarray(torch.as_tensor(dScales).detach().cpu(), np.float64) if dScales is not None else None
+        scales = (tuple(ms), None if ps is None else tuple(ps), None if ds is None else tuple(ds))
+        if getattr(self, "_scales", None) != scales:
+            self._engine = AdmpEngine(
+                self.n_atoms, self.lmax, self.lpol, self.lpme, self.rc, self.kappa, (self.K1, self.K2, self.K3),
+                self.axis_type if self.lmax > 0 else None, self.axis_indices if self.lmax > 0 else None,
+                self.cov_rows, ms, ps, ds, precision=self.precision, solver=self.pol_solver, cg_tol=self.cg_tol,
+                max_iter=self.max_iter, steps_pol=self.steps_pol, device=self.device)
+            self._scales = scales
+        del d
+        self.engine.set_params(Q_local, pol if self.lpol else None, tholes if self.lpol else None)
+        self._param_key = key
+
+    def get_energy(self, positions, box, pairs, Q_local, pol=None, tholes=None, mScales=None, pScales=None,
+                   dScales=None, U_init=None, aux=None):
+        """Energy (kJ/mol) for positions / box in Angstrom; pairs (i, j, nbond) rows or None for the
+        engine's own cell-list pairs.  U_init in Angstrom (the reference scales aux U by 10 before)."""
+        if not self.lpol:
+            # non-polarizable signature: get_energy(positions, box, pairs, Q_local, mScales)
+            if mScales is None and pol is not None:
+                mScales, pol = pol, None
+        self._sync_params(Q_local, pol, tholes, mScales, pScales, dScales)
+        eng = self.engine
+        if not torch.is_tensor(box):
+            box = torch.as_tensor(np.asarray(box), dtype=torch.float64)
+        pairs_d = _as_cuda_pairs(pairs, eng.device)
+        U0 = None
+        if self.lpol:
+            U0 = U_init if U_init is not None else self.U_ind
+            U0 = torch.as_tensor(U0, dtype=torch.float64)
+        E = _AdmpEnergy.apply(positions, box, self, pairs_d, U0, aux)
+        return E

@@ -1,0 +1,490 @@
+// Reciprocal-space smooth PME for multipoles up to quadrupoles (sm_100a).
+//
+// Follows dmff/admp/recip.py:9-471: order-6 cardinal B-splines on a K1 x K2 x K3 mesh, the
+// multipole "gradient operator" spread (recip.py:254-349), an FFT, the influence function
+// C_k / theta_k^2 (recip.py:438-466, Ck_1 at :474) and the energy sum.  The reference gets
+// forces by autodiff; here the gather is explicit: the convolved mesh phi is interpolated
+// with B-spline derivatives up to third order (20 sums per atom), giving dE/dpos, dE/dQ,
+// torques and the box gradient in one pass.
+//
+// Layout: each atom's 6x6x6 stencil is split into 36 (x, y) lines of 6 contiguous z points;
+// one warp owns one atom, lanes own lines.  The multipole is first mapped to mesh-derivative
+// coefficients c_abc (mu^u = -B mu, Theta^u = B Theta B^T with B the reference's derivative
+// operator, recip.py:213/251), so the per-point work is a 3-term dot product.  Spreading uses
+// FP32/FP64 atomics on the mesh (it lives in L2); the gather is atomics-free.
+#pragma once
+#include "common.cuh"
+
+namespace dmffb {
+
+struct MeshGeom {
+    double NA[9];   // grid coordinates x_j = sum_c NA[j][c] R_c  (NA = diag(K) h^-T)
+    double B[9];    // derivative operator used by the reference: B = NA^T
+    int K[3];
+};
+
+// order-6 B-spline values and derivatives at u = w + j, j = 0..5, w in [0, 1]
+template <typename T>
+__device__ __forceinline__ void bspline6(T w, T M0[6], T M1[6], T M2[6], T M3[6]) {
+    T m2[2] = {w, T(1) - w};
+    T m3[3], m4[4], m5[5];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        T a = j < 2 ? m2[j] : T(0);
+        T b = j > 0 ? m2[j - 1] : T(0);
+        m3[j] = ((w + T(j)) * a + (T(3) - w - T(j)) * b) * T(0.5);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        T a = j < 3 ? m3[j] : T(0);
+        T b = j > 0 ? m3[j - 1] : T(0);
+        m4[j] = ((w + T(j)) * a + (T(4) - w - T(j)) * b) * T(1.0 / 3.0);
+    }
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        T a = j < 4 ? m4[j] : T(0);
+        T b = j > 0 ? m4[j - 1] : T(0);
+        m5[j] = ((w + T(j)) * a + (T(5) - w - T(j)) * b) * T(0.25);
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        T a = j < 5 ? m5[j] : T(0);
+        T b = j > 0 ? m5[j - 1] : T(0);
+        M0[j] = ((w + T(j)) * a + (T(6) - w - T(j)) * b) * T(0.2);
+        M1[j] = a - b;
+        T c0 = j < 4 ? m4[j] : T(0), c1 = (j >= 1 && j - 1 < 4) ? m4[j - 1] : T(0), c2 = j >= 2 ? m4[j - 2] : T(0);
+        M2[j] = c0 - T(2) * c1 + c2;
+        T e0 = j < 3 ? m3[j] : T(0), e1 = (j >= 1 && j - 1 < 3) ? m3[j - 1] : T(0);
+        T e2 = (j >= 2 && j - 2 < 3) ? m3[j - 2] : T(0), e3 = j >= 3 ? m3[j - 3] : T(0);
+        M3[j] = e0 - T(3) * e1 + T(3) * e2 - e3;
+    }
+}
+
+__device__ __forceinline__ int wrapi(int g, int K) {
+    g %= K;
+    return g < 0 ? g + K : g;
+}
+
+// mesh-derivative coefficients of one site: c[0]=000, 1..3 = e_x,e_y,e_z, 4..9 = xx,yy,zz,xy,xz,yz
+// (second-order entries hold Theta^u_jk summed over both orders for j != k).
+template <typename T>
+__device__ __forceinline__ void site_coefs(const double* B, T q, const T mu[3], const T Th[3][3], T c[10]) {
+    c[0] = q;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) c[1 + j] = -(T(B[3 * j]) * mu[0] + T(B[3 * j + 1]) * mu[1] + T(B[3 * j + 2]) * mu[2]);
+    T BT[3][3];  // (B Theta)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) BT[j][d] = T(B[3 * j]) * Th[0][d] + T(B[3 * j + 1]) * Th[1][d] + T(B[3 * j + 2]) * Th[2][d];
+    T Tu[3][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) Tu[j][k] = BT[j][0] * T(B[3 * k]) + BT[j][1] * T(B[3 * k + 1]) + BT[j][2] * T(B[3 * k + 2]);
+    c[4] = Tu[0][0];
+    c[5] = Tu[1][1];
+    c[6] = Tu[2][2];
+    c[7] = Tu[0][1] + Tu[1][0];
+    c[8] = Tu[0][2] + Tu[2][0];
+    c[9] = Tu[1][2] + Tu[2][1];
+}
+
+// harmonic quadrupole (Q4..Q8, recip.py:317-349 with the /3) -> Cartesian coefficient matrix
+template <typename T>
+__device__ __forceinline__ void quad_cart(const T* Qq, T Th[3][3]) {
+    const T s = T(DMFFB_SQRT3 / 6.0);
+    Th[2][2] = Qq[0] * T(1.0 / 3.0);
+    Th[0][0] = -Qq[0] * T(1.0 / 6.0) + Qq[3] * s;
+    Th[1][1] = -Qq[0] * T(1.0 / 6.0) - Qq[3] * s;
+    Th[0][2] = Th[2][0] = Qq[1] * s;
+    Th[1][2] = Th[2][1] = Qq[2] * s;
+    Th[0][1] = Th[1][0] = Qq[4] * s;
+}
+
+template <typename T>
+struct SpreadArgs {
+    int n;
+    const double* pos;  // [n*3]
+    const T* Qg;        // [n*9] permanent (may be null)
+    const double* U;    // [n*3] Cartesian dipoles (may be null)
+    const T* q1;        // [n] plain charges for charge-only channels (may be null)
+    int lmax;           // 0: charge only, 1: up to dipole, 2: up to quadrupole
+    MeshGeom g;
+    T* grid;
+};
+
+template <typename T>
+__device__ __forceinline__ void site_multipole(const SpreadArgs<T>& a, int at, T& q, T mu[3], T Th[3][3]) {
+    q = T(0);
+    mu[0] = mu[1] = mu[2] = T(0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Th[r][c] = T(0);
+    if (a.q1) q = a.q1[at];
+    if (a.Qg) {
+        const T* Q = a.Qg + 9 * at;
+        q += Q[0];
+        if (a.lmax >= 1) { mu[0] = Q[2]; mu[1] = Q[3]; mu[2] = Q[1]; }
+        if (a.lmax >= 2) quad_cart(Q + 4, Th);
+    }
+    if (a.U) {
+        mu[0] += (T)a.U[3 * at];
+        mu[1] += (T)a.U[3 * at + 1];
+        mu[2] += (T)a.U[3 * at + 2];
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void stencil_setup(const MeshGeom& g, const double* pos, int at, int m0[3], T Mx[4][6],
+                                              T My[4][6], T Mz[4][6]) {
+    const double R0 = pos[3 * at], R1 = pos[3 * at + 1], R2 = pos[3 * at + 2];
+    T (*Ms[3])[6] = {Mx, My, Mz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double x = g.NA[3 * d] * R0 + g.NA[3 * d + 1] * R1 + g.NA[3 * d + 2] * R2;
+        const double c = ceil(x);
+        m0[d] = (int)c;
+        bspline6<T>((T)(c - x), Ms[d][0], Ms[d][1], Ms[d][2], Ms[d][3]);
+    }
+}
+
+// one warp per site; lanes cover the 36 (x, y) lines of the 6^3 stencil
+template <typename T>
+__global__ void __launch_bounds__(256) k_spread(SpreadArgs<T> a) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.n) return;
+    const int at = warp;
+    int m0[3];
+    T Mx[4][6], My[4][6], Mz[4][6];
+    stencil_setup<T>(a.g, a.pos, at, m0, Mx, My, Mz);
+    T q, mu[3], Th[3][3];
+    site_multipole(a, at, q, mu, Th);
+    T c[10];
+    site_coefs<T>(a.g.B, q, mu, Th, c);
+    const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
+    int gz[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) gz[t] = wrapi(m0[2] - 3 + t, K2);
+    for (int L = lane; L < 36; L += 32) {
+        const int ix = L / 6, iy = L % 6;
+        const T x0 = Mx[0][ix], x1 = Mx[1][ix], x2 = Mx[2][ix];
+        const T y0 = My[0][iy], y1 = My[1][iy], y2 = My[2][iy];
+        const T s0 = c[0] * x0 * y0 + c[1] * x1 * y0 + c[2] * x0 * y1 + c[4] * x2 * y0 + c[5] * x0 * y2 + c[7] * x1 * y1;
+        const T s1 = c[3] * x0 * y0 + c[8] * x1 * y0 + c[9] * x0 * y1;
+        const T s2 = c[6] * x0 * y0;
+        const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
+        T* line = a.grid + ((size_t)gx * K1 + gy) * K2;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+            const T v = s0 * Mz[0][t] + s1 * Mz[1][t] + s2 * Mz[2][t];
+            atomicAdd(line + gz[t], v);
+        }
+    }
+}
+
+enum { CK_COUL = 0, CK_DISP6 = 1, CK_DISP8 = 2, CK_DISP10 = 3 };
+
+template <typename T>
+struct ConvArgs {
+    int K[3];
+    int Kh;              // K3/2 + 1
+    T* S;                // [K1*K2*Kh] interleaved complex (re, im), overwritten by G*S
+    const double* bmod;  // [K1 + K2 + K3] per-dimension B-spline moduli (recip.py:440-448)
+    double hinv[9];
+    double V;
+    double kappa;
+    double escale;       // DIELECTRIC for Coulomb, 1 for dispersion
+    int kind;
+    double* scal;        // [0] energy, [1..6] sum E_k (dlnC/dk2) k k  (xx,yy,zz,xy,xz,yz)
+    int want_energy;
+};
+
+// influence function C(k^2) and d ln C / d k^2
+__device__ __forceinline__ void influence(int kind, double ksq, double kappa, double V, double& C, double& dlnC) {
+    const double SQRT_PI = 1.7724538509055159;
+    const double PI = 3.141592653589793;
+    if (kind == CK_COUL) {
+        C = 2.0 * PI / V / ksq * exp(-ksq / 4.0 / (kappa * kappa));
+        dlnC = -1.0 / ksq - 1.0 / (4.0 * kappa * kappa);
+        return;
+    }
+    // dispersion (recip.py:477-508): ksq thresholded at 1e-16
+    const double ks = ksq < 1e-16 ? 1e-16 : ksq;
+    const double x2 = ks / 4.0 / (kappa * kappa);
+    const double x = sqrt(x2);
+    const double ex = exp(-x2);
+    const double ec = erfc(x);
+    double f, dfdx, pref;
+    if (kind == CK_DISP6) {
+        const double x3 = x2 * x;
+        f = (1 - 2 * x2) * ex + 2 * x3 * SQRT_PI * ec;
+        // d/dx: (-4x)e + (1-2x^2)(-2x)e + 6x^2 sqrt(pi) erfc - 2x^3 * 2 e
+        dfdx = -4 * x * ex - 2 * x * (1 - 2 * x2) * ex + 6 * x2 * SQRT_PI * ec - 4 * x3 * ex;
+        pref = SQRT_PI * PI / 2 / V * kappa * kappa * kappa / 3;
+    } else if (kind == CK_DISP8) {
+        const double x4 = x2 * x2, x5 = x4 * x;
+        f = (3 - 2 * x2 + 4 * x4) * ex - 4 * x5 * SQRT_PI * ec;
+        dfdx = (-4 * x + 16 * x2 * x) * ex - 2 * x * (3 - 2 * x2 + 4 * x4) * ex - 20 * x4 * SQRT_PI * ec + 8 * x5 * ex;
+        pref = SQRT_PI * PI / 2 / V * pow(kappa, 5) / 45;
+    } else {
+        const double x4 = x2 * x2, x6 = x4 * x2, x7 = x6 * x;
+        f = (15 - 6 * x2 + 4 * x4 - 8 * x6) * ex + 8 * x7 * SQRT_PI * ec;
+        dfdx = (-12 * x + 16 * x2 * x - 48 * x4 * x) * ex - 2 * x * (15 - 6 * x2 + 4 * x4 - 8 * x6) * ex + 56 * x6 * SQRT_PI * ec - 16 * x7 * ex;
+        pref = SQRT_PI * PI / 2 / V * pow(kappa, 7) / 1260;
+    }
+    C = pref * f;
+    // d/dk2 = dx/dk2 d/dx, x = sqrt(k2)/(2 kappa) -> dx/dk2 = 1/(8 kappa^2 x)
+    dlnC = (ksq < 1e-16) ? 0.0 : dfdx / f / (8.0 * kappa * kappa * x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_conv(ConvArgs<T> a) {
+    const int64_t total = (int64_t)a.K[0] * a.K[1] * a.Kh;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double red[7] = {0, 0, 0, 0, 0, 0, 0};
+    if (idx < total) {
+        const int k3 = (int)(idx % a.Kh);
+        const int k2 = (int)((idx / a.Kh) % a.K[1]);
+        const int k1 = (int)(idx / ((int64_t)a.Kh * a.K[1]));
+        const int m1 = k1 < (a.K[0] + 1) / 2 ? k1 : k1 - a.K[0];
+        const int m2 = k2 < (a.K[1] + 1) / 2 ? k2 : k2 - a.K[1];
+        const int m3 = k3 < (a.K[2] + 1) / 2 ? k3 : k3 - a.K[2];
+        const double TWO_PI = 6.283185307179586;
+        double kv[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) kv[c] = TWO_PI * (a.hinv[3 * c] * m1 + a.hinv[3 * c + 1] * m2 + a.hinv[3 * c + 2] * m3);
+        const double ksq = kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2];
+        const double th = a.bmod[k1] * a.bmod[a.K[0] + k2] * a.bmod[a.K[0] + a.K[1] + k3];
+        double G = 0.0, dlnC = 0.0;
+        const bool zero = (m1 == 0 && m2 == 0 && m3 == 0);
+        if (!(zero && a.kind == CK_COUL)) {
+            double C;
+            influence(a.kind, ksq, a.kappa, a.V, C, dlnC);
+            G = C / (th * th);
+        }
+        T* s = a.S + 2 * idx;
+        const double re = (double)s[0], im = (double)s[1];
+        if (a.want_energy) {
+            const bool self_conj = (k3 == 0) || ((a.K[2] % 2 == 0) && k3 == a.K[2] / 2);
+            const double w = self_conj ? 1.0 : 2.0;
+            const double Ek = a.escale * w * G * (re * re + im * im);
+            red[0] = Ek;
+            const double f = Ek * dlnC;
+            red[1] = f * kv[0] * kv[0];
+            red[2] = f * kv[1] * kv[1];
+            red[3] = f * kv[2] * kv[2];
+            red[4] = f * kv[0] * kv[1];
+            red[5] = f * kv[0] * kv[2];
+            red[6] = f * kv[1] * kv[2];
+        }
+        s[0] = (T)(re * G);
+        s[1] = (T)(im * G);
+    }
+    if (a.want_energy) block_reduce_add<7>(red, a.scal);
+}
+
+enum { GATHER_FULL = 0, GATHER_FIELD = 1 };
+
+template <typename T>
+struct GatherArgs {
+    int n;
+    const double* pos;
+    const T* Qg;          // permanent multipoles (torque and coefficients), may be null
+    const double* U;      // induced dipoles added to the spread multipole, may be null
+    const T* q1;          // plain charges (charge-only channel), may be null
+    int lmax;
+    MeshGeom g;
+    const T* phi;         // convolved mesh (real)
+    double scale;         // dE/dmesh = scale * phi   (2*DIELECTRIC or 2)
+    double* grad;         // [n*3] += dE/dpos
+    T* torque;            // [n*3] += torque of permanent multipoles (may be null)
+    double* field;        // [n*3] dE/dU (Cartesian); written (FIELD) or accumulated
+    int field_accumulate;
+    double* gQ;           // [n*9] += dE/dQ_global (may be null)
+    double* dq1;          // [n] += dE/dq for the charge channel (may be null)
+    double* scal;         // [0] energy (1/2 sum c P), [1..9] X_NA
+    int want_box;
+    int mode;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather(GatherArgs<T> a) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const bool active = warp < a.n;
+    const int at = active ? warp : 0;
+    int m0[3];
+    T Mx[4][6], My[4][6], Mz[4][6];
+    stencil_setup<T>(a.g, a.pos, at, m0, Mx, My, Mz);
+    const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
+    int gz[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) gz[t] = wrapi(m0[2] - 3 + t, K2);
+    // partial sums P_abc, a+b+c <= 3, order: index via table below
+    // 0:000 1:100 2:010 3:001 4:200 5:020 6:002 7:110 8:101 9:011
+    // 10:300 11:030 12:003 13:210 14:201 15:120 16:021 17:102 18:012 19:111
+    T P[20];
+#pragma unroll
+    for (int k = 0; k < 20; ++k) P[k] = T(0);
+    const int maxo = (a.mode == GATHER_FIELD) ? 2 : 3;
+    if (active) {
+        for (int L = lane; L < 36; L += 32) {
+            const int ix = L / 6, iy = L % 6;
+            const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
+            const T* line = a.phi + ((size_t)gx * K1 + gy) * K2;
+            T s[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+                const T v = line[gz[t]];
+                s[0] += v * Mz[0][t];
+                s[1] += v * Mz[1][t];
+                s[2] += v * Mz[2][t];
+                s[3] += v * Mz[3][t];
+            }
+            const T x0 = Mx[0][ix], x1 = Mx[1][ix], x2 = Mx[2][ix], x3 = Mx[3][ix];
+            const T y0 = My[0][iy], y1 = My[1][iy], y2 = My[2][iy], y3 = My[3][iy];
+            P[0] += x0 * y0 * s[0];
+            P[1] += x1 * y0 * s[0];
+            P[2] += x0 * y1 * s[0];
+            P[3] += x0 * y0 * s[1];
+            P[4] += x2 * y0 * s[0];
+            P[5] += x0 * y2 * s[0];
+            P[6] += x0 * y0 * s[2];
+            P[7] += x1 * y1 * s[0];
+            P[8] += x1 * y0 * s[1];
+            P[9] += x0 * y1 * s[1];
+            if (maxo == 3) {
+                P[10] += x3 * y0 * s[0];
+                P[11] += x0 * y3 * s[0];
+                P[12] += x0 * y0 * s[3];
+                P[13] += x2 * y1 * s[0];
+                P[14] += x2 * y0 * s[1];
+                P[15] += x1 * y2 * s[0];
+                P[16] += x0 * y2 * s[1];
+                P[17] += x1 * y0 * s[2];
+                P[18] += x0 * y1 * s[2];
+                P[19] += x1 * y1 * s[1];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 20; ++k) P[k] = warp_sum(P[k]);
+
+    double red[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) red[k] = 0.0;
+    if (active && lane == 0) {
+        const double sc = a.scale;
+        double Pd[20];
+#pragma unroll
+        for (int k = 0; k < 20; ++k) Pd[k] = sc * (double)P[k];
+        // site multipole (the one that was spread)
+        SpreadArgs<T> sa;
+        sa.Qg = a.Qg; sa.U = a.U; sa.q1 = a.q1; sa.lmax = a.lmax;
+        T q, mu[3], Th[3][3];
+        site_multipole(sa, at, q, mu, Th);
+        T cT[10];
+        site_coefs<T>(a.g.B, q, mu, Th, cT);
+        double c[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) c[k] = (double)cT[k];
+        const double* B = a.g.B;
+        // dE/dmu^u_j and dE/dTheta^u_jk
+        const double Pu[3] = {Pd[1], Pd[2], Pd[3]};
+        const double P2[3][3] = {{Pd[4], Pd[7], Pd[8]}, {Pd[7], Pd[5], Pd[9]}, {Pd[8], Pd[9], Pd[6]}};
+        double dmu[3];
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) dmu[cc] = -(Pu[0] * B[cc] + Pu[1] * B[3 + cc] + Pu[2] * B[6 + cc]);
+        if (a.mode == GATHER_FIELD) {
+            double* f = a.field + 3 * at;
+            if (a.field_accumulate) { f[0] += dmu[0]; f[1] += dmu[1]; f[2] += dmu[2]; }
+            else { f[0] = dmu[0]; f[1] = dmu[1]; f[2] = dmu[2]; }
+        } else {
+            // dE/dx_j = -sum_abc c_abc P_{abc + e_j}
+            // coefficient -> (a,b,c) exponents; index of abc+e_j in P
+            const int up[10][3] = {{1, 2, 3},   {4, 7, 8},   {7, 5, 9},   {8, 9, 6},    {10, 13, 14},
+                                   {15, 11, 16}, {17, 18, 12}, {13, 15, 19}, {14, 19, 17}, {19, 16, 18}};
+            double Y[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < 10; ++k)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) Y[j] -= c[k] * Pd[up[k][j]];
+            double* gr = a.grad + 3 * at;
+            const double* NA = a.g.NA;
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) gr[cc] += NA[cc] * Y[0] + NA[3 + cc] * Y[1] + NA[6 + cc] * Y[2];
+            double e = 0.0;
+#pragma unroll
+            for (int k = 0; k < 10; ++k) e += c[k] * Pd[k];
+            red[0] = 0.5 * e;
+            // dE/dTheta (Cartesian) = B^T P2 B
+            double BP[3][3];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) BP[cc][k] = B[cc] * P2[0][k] + B[3 + cc] * P2[1][k] + B[6 + cc] * P2[2][k];
+            double dTh[3][3];
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) dTh[cc][d] = BP[cc][0] * B[d] + BP[cc][1] * B[3 + d] + BP[cc][2] * B[6 + d];
+            double g[9];
+            g[0] = Pd[0];
+            g[1] = dmu[2];
+            g[2] = dmu[0];
+            g[3] = dmu[1];
+            const double s6 = DMFFB_SQRT3 / 6.0;
+            g[4] = dTh[2][2] / 3.0 - dTh[0][0] / 6.0 - dTh[1][1] / 6.0;
+            g[5] = (dTh[0][2] + dTh[2][0]) * s6;
+            g[6] = (dTh[1][2] + dTh[2][1]) * s6;
+            g[7] = (dTh[0][0] - dTh[1][1]) * s6;
+            g[8] = (dTh[0][1] + dTh[1][0]) * s6;
+            if (a.field) {
+                double* f = a.field + 3 * at;
+                if (a.field_accumulate) { f[0] += dmu[0]; f[1] += dmu[1]; f[2] += dmu[2]; }
+                else { f[0] = dmu[0]; f[1] = dmu[1]; f[2] = dmu[2]; }
+            }
+            if (a.gQ) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) a.gQ[9 * at + k] += g[k];
+            }
+            if (a.dq1) a.dq1[at] += g[0];
+            if (a.torque && a.Qg) {
+                T qp[9], gT[9], t[3];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) { qp[k] = a.Qg[9 * at + k]; gT[k] = (T)g[k]; }
+                if (a.lmax < 2) { for (int k = 4; k < 9; ++k) qp[k] = T(0); }
+                if (a.lmax < 1) { qp[1] = qp[2] = qp[3] = T(0); }
+                torque9(qp, gT, t);
+                a.torque[3 * at] += t[0];
+                a.torque[3 * at + 1] += t[1];
+                a.torque[3 * at + 2] += t[2];
+            }
+            if (a.want_box) {
+                // X_NA = Y (x) R + (dE/dB)^T,  dE/dB = -Pu (x) mu + 2 P2 B Theta
+                const double R[3] = {a.pos[3 * at], a.pos[3 * at + 1], a.pos[3 * at + 2]};
+                double PB[3][3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) PB[j][k] = P2[j][0] * B[k] + P2[j][1] * B[3 + k] + P2[j][2] * B[6 + k];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+#pragma unroll
+                    for (int cc = 0; cc < 3; ++cc) {
+                        double dB = -Pu[j] * (double)mu[cc];
+                        dB += 2.0 * (PB[j][0] * (double)Th[0][cc] + PB[j][1] * (double)Th[1][cc] + PB[j][2] * (double)Th[2][cc]);
+                        // (dE/dB)^T[cc][j] adds to X_NA[cc][j]; Y (x) R adds to X_NA[j][cc]
+                        red[1 + 3 * cc + j] += dB;
+                        red[1 + 3 * j + cc] += Y[j] * R[cc];
+                    }
+            }
+        }
+    }
+    if (a.mode == GATHER_FULL) block_reduce_add<10>(red, a.scal);
+}
+
+}  // namespace dmffb

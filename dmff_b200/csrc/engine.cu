@@ -1,0 +1,978 @@
+// libdmffb200: ADMP multipolar PME engine for B200 (sm_100a) behind the C ABI in
+// include/dmffb200.h.  The handle owns every device workspace (allocated in create /
+// reserve, never inside compute); callers own their inputs and outputs.
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dmffb200.h"
+#include "admp_frames.cuh"
+#include "admp_real.cuh"
+#include "admp_recip.cuh"
+#include "common.cuh"
+#include "nblist.cuh"
+
+using namespace dmffb;
+
+namespace {
+
+enum {
+    S_EREAL = 0,    // [0] energy, [1..9] box grad (pair kernel)
+    S_RECIP = 16,   // [0] energy, [1..6] k-space tensor (conv kernel)
+    S_GATHER = 24,  // [0] energy check, [1..9] X_NA
+    S_SELF = 40,    // [0] E_self, [1] E_pol, [2..10] frame box grad
+    S_CG = 56,      // CG scalars
+    N_SCAL = 80
+};
+
+}  // namespace
+
+struct dmffb_engine {
+    // ---- static description
+    int n = 0, lmax = 0, lpol = 0, lpme = 1, prec = DMFFB_FP32;
+    double rc = 0, kappa = 0;
+    int K[3] = {0, 0, 0};
+    double ms[6], ps[6], dsc[6];
+    int solver = DMFFB_SOLVER_CG;
+    double cg_tol = 1e-6;
+    int max_iter = 500, steps_pol = 0;
+    std::string err;
+    bool params_set = false;
+    // ---- device data
+    int32_t* d_axis_type = nullptr;
+    int32_t* d_axis_idx = nullptr;
+    int32_t *d_cov_ptr = nullptr, *d_cov_j = nullptr, *d_cov_nb = nullptr;
+    double* d_Qloc = nullptr;
+    double* d_pol = nullptr;
+    void* d_thole = nullptr;
+    void* d_polsix = nullptr;
+    double* d_pos = nullptr;  // host-path staging
+    double* d_U = nullptr;    // host-path staging / internal dipoles
+    double* d_forces = nullptr;
+    void* d_posT = nullptr;
+    double* d_Qg = nullptr;
+    void* d_QgT = nullptr;
+    void* d_gpair = nullptr;
+    void* d_torque = nullptr;
+    void* d_fieldT = nullptr;
+    double* d_grad = nullptr;
+    double* d_scal = nullptr;
+    double *d_b = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_Ap = nullptr, *d_fr = nullptr;
+    double* d_gQ = nullptr;
+    void* d_grid = nullptr;
+    void* d_cgrid = nullptr;
+    double* d_bmod = nullptr;
+    cufftHandle plan_f = 0, plan_b = 0;
+    bool have_plans = false;
+    // ---- neighbour list
+    int32_t* d_pairs = nullptr;
+    int64_t pair_cap = 0, npairs = 0;
+    bool have_pairs = false;
+    int32_t *d_atom_cell = nullptr, *d_cell_count = nullptr, *d_cell_start = nullptr, *d_cell_cursor = nullptr,
+            *d_cell_atoms = nullptr, *d_pcount = nullptr;
+    int64_t* d_poff = nullptr;
+    int ncell_cap = 0;
+    void* d_cub = nullptr;
+    size_t cub_bytes = 0;
+    double* h_scal = nullptr;  // pinned
+    // ---- timing
+    bool timing = false;
+    cudaEvent_t ev[8];
+    double t_ms[6] = {0, 0, 0, 0, 0, 0};
+    // ---- last result book-keeping
+    Box last_box;
+    const double* cur_pos = nullptr;  // FP64 positions of the evaluation in flight
+};
+
+namespace {
+
+int fail(dmffb_engine* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(h, DMFFB_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKFFT(call)                                                                        \
+    do {                                                                                   \
+        cufftResult r_ = (call);                                                           \
+        if (r_ != CUFFT_SUCCESS) return fail(h, DMFFB_CUFFT_ERROR, std::string(#call) + " failed"); \
+    } while (0)
+
+template <typename P>
+int dalloc(dmffb_engine* h, P** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void**)p, bytes);
+    if (e != cudaSuccess) return fail(h, DMFFB_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaMemset(*p, 0, bytes);
+    return DMFFB_OK;
+}
+
+void make_box(const double* b, Box& bx) {
+    for (int k = 0; k < 9; ++k) bx.h[k] = b[k];
+    const double* m = b;
+    double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
+    double inv[9];
+    inv[0] = (m[4] * m[8] - m[5] * m[7]) / det;
+    inv[1] = (m[2] * m[7] - m[1] * m[8]) / det;
+    inv[2] = (m[1] * m[5] - m[2] * m[4]) / det;
+    inv[3] = (m[5] * m[6] - m[3] * m[8]) / det;
+    inv[4] = (m[0] * m[8] - m[2] * m[6]) / det;
+    inv[5] = (m[2] * m[3] - m[0] * m[5]) / det;
+    inv[6] = (m[3] * m[7] - m[4] * m[6]) / det;
+    inv[7] = (m[1] * m[6] - m[0] * m[7]) / det;
+    inv[8] = (m[0] * m[4] - m[1] * m[3]) / det;
+    // diagonal boxes: exact reciprocals, as a LU inverse would give
+    if (m[1] == 0 && m[2] == 0 && m[3] == 0 && m[5] == 0 && m[6] == 0 && m[7] == 0) {
+        for (int k = 0; k < 9; ++k) inv[k] = 0.0;
+        inv[0] = 1.0 / m[0];
+        inv[4] = 1.0 / m[4];
+        inv[8] = 1.0 / m[8];
+    }
+    for (int k = 0; k < 9; ++k) bx.hinv[k] = inv[k];
+}
+
+double det3(const double* m) {
+    return m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) + m[2] * (m[3] * m[7] - m[4] * m[6]);
+}
+
+template <typename T>
+BoxT<T> boxT(const Box& b) {
+    BoxT<T> r;
+    for (int k = 0; k < 9; ++k) {
+        r.h[k] = (T)b.h[k];
+        r.hinv[k] = (T)b.hinv[k];
+    }
+    return r;
+}
+
+MeshGeom mesh_geom(const Box& b, const int K[3]) {
+    MeshGeom g;
+    // NA[j][c] = K_j * hinv[c][j]
+    for (int j = 0; j < 3; ++j)
+        for (int c = 0; c < 3; ++c) g.NA[3 * j + c] = K[j] * b.hinv[3 * c + j];
+    for (int j = 0; j < 3; ++j)
+        for (int c = 0; c < 3; ++c) g.B[3 * j + c] = g.NA[3 * c + j];
+    for (int k = 0; k < 3; ++k) g.K[k] = K[k];
+    return g;
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+// ------------------------------------------------------------------ small vector kernels
+template <typename T>
+__global__ void k_field_combine(int n, const double* recip, const T* fT, const double* U, const double* Qg,
+                                const double* pol, double self1, int include_perm, double* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    const int a = k / 3, c = k % 3;
+    double p = pol[a];
+    p = p < 1e-8 ? 1e-8 : p;
+    double v = (recip ? recip[k] : 0.0) + (double)fT[k];
+    if (U) v += (DMFFB_DIELECTRIC / p + self1) * U[k];
+    if (include_perm) {
+        const int hidx = c == 0 ? 2 : (c == 1 ? 3 : 1);
+        v += self1 * Qg[9 * a + hidx];
+    }
+    out[k] = v;
+}
+
+// CG helpers; scalars live in s[]: [0] rz(even) [1] rz(odd) [2] pAp [3] rr
+__global__ void k_dot2(int m, const double* a, const double* b, const double* c, const double* d, double* s0,
+                       double* s1) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double v0[1] = {0.0}, v1[1] = {0.0};
+    if (k < m) {
+        v0[0] = a[k] * b[k];
+        if (c) v1[0] = c[k] * d[k];
+    }
+    block_reduce_add<1>(v0, s0);
+    if (s1) block_reduce_add<1>(v1, s1);
+}
+
+__global__ void k_cg_init(int n, const double* b, const double* Ax, const double* pol, double* r, double* z,
+                          double* p) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    double pp = pol[k / 3];
+    pp = pp < 1e-8 ? 1e-8 : pp;
+    const double rv = -(b[k] + (Ax ? Ax[k] : 0.0));
+    r[k] = rv;
+    z[k] = rv * pp / DMFFB_DIELECTRIC;
+    p[k] = z[k];
+}
+
+__global__ void k_cg_update(int n, const double* s, int slot, double* x, double* r, double* z, const double* p,
+                            const double* Ap, const double* pol, double* rz_new, double* rr) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double alpha = s[slot] / s[2];
+    double v[1] = {0.0}, w[1] = {0.0};
+    if (k < 3 * n) {
+        double pp = pol[k / 3];
+        pp = pp < 1e-8 ? 1e-8 : pp;
+        x[k] += alpha * p[k];
+        const double rv = r[k] - alpha * Ap[k];
+        r[k] = rv;
+        const double zv = rv * pp / DMFFB_DIELECTRIC;
+        z[k] = zv;
+        v[0] = rv * zv;
+        w[0] = rv * rv;
+    }
+    block_reduce_add<1>(v, rz_new);
+    block_reduce_add<1>(w, rr);
+}
+
+__global__ void k_cg_p(int n, const double* s, int slot_old, int slot_new, const double* z, double* p) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    const double beta = s[slot_new] / s[slot_old];
+    p[k] = z[k] + beta * p[k];
+}
+
+__global__ void k_ref_step(int n, const double* f, const double* pol, double* U, double* maxf) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    const double p = pol[k / 3];
+    U[k] -= f[k] * p / DMFFB_DIELECTRIC;
+    (void)maxf;
+}
+
+__global__ void k_absmax(int n, const double* f, const double* pol, double thresh_pol, unsigned long long* out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    if (pol[k / 3] > thresh_pol) {
+        const double v = fabs(f[k]);
+        atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+template <typename T>
+__global__ void k_set_thole(int n, const double* pol, const double* thole, T* th, T* psix) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    th[a] = thole ? (T)thole[a] : T(0);
+    psix[a] = pol ? (T)pow(pol[a] > 0 ? pol[a] : 0.0, 1.0 / 6.0) : T(0);
+}
+
+// ------------------------------------------------------------------ engine pieces
+template <typename T>
+PairArgs<T> pair_args(dmffb_engine* h, const Box& bx, const int32_t* pairs, int64_t npairs, const double* U) {
+    PairArgs<T> a;
+    a.n = h->n;
+    a.npairs = npairs;
+    a.pairs = pairs;
+    a.pos = (const T*)h->d_posT;
+    a.posd = h->cur_pos;
+    a.Qg = (const T*)h->d_QgT;
+    a.Qgd = h->d_Qg;
+    a.U = U;
+    a.thole = (const T*)h->d_thole;
+    a.polsix = (const T*)h->d_polsix;
+    for (int k = 0; k < 6; ++k) {
+        a.ms[k] = (T)h->ms[k];
+        a.ps[k] = (T)h->ps[k];
+        a.dsc[k] = (T)h->dsc[k];
+    }
+    a.kappa = (T)(h->lpme ? h->kappa : 0.0);
+    a.boxd = bx;
+    a.grad = (T*)h->d_gpair;
+    a.torque = (T*)h->d_torque;
+    a.field = (T*)h->d_fieldT;
+    a.scal = h->d_scal + S_EREAL;
+    a.want_box = 1;
+    return a;
+}
+
+int lmax_eff(const dmffb_engine* h) { return (h->lmax == 0 && h->lpol) ? 1 : h->lmax; }
+
+// reciprocal pass: spread (Qg and/or U) -> FFT -> convolution -> inverse FFT -> gather
+template <typename T>
+int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, bool use_Qg, const double* U,
+               int mode, double* field_out, int field_acc) {
+    const MeshGeom g = mesh_geom(bx, h->K);
+    const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
+    CK(cudaMemsetAsync(h->d_grid, 0, K3 * sizeof(T), s));
+    SpreadArgs<T> sa;
+    sa.n = h->n;
+    sa.pos = pos;
+    sa.Qg = use_Qg ? (const T*)h->d_QgT : nullptr;
+    sa.U = U;
+    sa.q1 = nullptr;
+    sa.lmax = lmax_eff(h);
+    sa.g = g;
+    sa.grid = (T*)h->d_grid;
+    k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa);
+    CKFFT(cufftSetStream(h->plan_f, s));
+    CKFFT(cufftSetStream(h->plan_b, s));
+    if (sizeof(T) == 4) {
+        CKFFT(cufftExecR2C(h->plan_f, (cufftReal*)h->d_grid, (cufftComplex*)h->d_cgrid));
+    } else {
+        CKFFT(cufftExecD2Z(h->plan_f, (cufftDoubleReal*)h->d_grid, (cufftDoubleComplex*)h->d_cgrid));
+    }
+    ConvArgs<T> ca;
+    for (int k = 0; k < 3; ++k) ca.K[k] = h->K[k];
+    ca.Kh = h->K[2] / 2 + 1;
+    ca.S = (T*)h->d_cgrid;
+    ca.bmod = h->d_bmod;
+    for (int k = 0; k < 9; ++k) ca.hinv[k] = bx.hinv[k];
+    ca.V = fabs(det3(bx.h));
+    ca.kappa = h->kappa;
+    ca.escale = DMFFB_DIELECTRIC;
+    ca.kind = CK_COUL;
+    ca.scal = h->d_scal + S_RECIP;
+    ca.want_energy = (mode == GATHER_FULL) ? 1 : 0;
+    const int64_t nk = (int64_t)h->K[0] * h->K[1] * ca.Kh;
+    k_conv<T><<<nblk(nk, 256), 256, 0, s>>>(ca);
+    if (sizeof(T) == 4) {
+        CKFFT(cufftExecC2R(h->plan_b, (cufftComplex*)h->d_cgrid, (cufftReal*)h->d_grid));
+    } else {
+        CKFFT(cufftExecZ2D(h->plan_b, (cufftDoubleComplex*)h->d_cgrid, (cufftDoubleReal*)h->d_grid));
+    }
+    GatherArgs<T> ga;
+    ga.n = h->n;
+    ga.pos = pos;
+    ga.Qg = use_Qg ? (const T*)h->d_QgT : nullptr;
+    ga.U = U;
+    ga.q1 = nullptr;
+    ga.lmax = lmax_eff(h);
+    ga.g = g;
+    ga.phi = (const T*)h->d_grid;
+    ga.scale = 2.0 * DMFFB_DIELECTRIC;
+    ga.grad = h->d_grad;
+    ga.torque = (T*)h->d_torque;
+    ga.field = field_out;
+    ga.field_accumulate = field_acc;
+    ga.gQ = (mode == GATHER_FULL) ? h->d_gQ : nullptr;
+    ga.dq1 = nullptr;
+    ga.scal = h->d_scal + S_GATHER;
+    ga.want_box = 1;
+    ga.mode = mode;
+    k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga);
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
+// dE/dU at U (include_perm) or its linear part A U (!include_perm), into out
+template <typename T>
+int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
+               int64_t npairs, const double* U, bool include_perm, double* out) {
+    CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
+    const unsigned nb = nblk(npairs, 128);
+    if (include_perm && npairs > 0) {
+        PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
+        k_admp_pair<T, true, PAIR_FIELD><<<nb, 128, 0, s>>>(a);
+    }
+    if (U && npairs > 0) {
+        PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, U);
+        k_admp_pair<T, true, PAIR_MATVEC><<<nb, 128, 0, s>>>(a);
+    }
+    const double* recip = nullptr;
+    if (h->lpme && h->have_plans) {
+        int st = recip_pass<T>(h, s, pos, bx, include_perm, U, GATHER_FIELD, h->d_fr, 0);
+        if (st) return st;
+        recip = h->d_fr;
+    }
+    const double k = h->kappa;
+    const double self1 = h->lpme ? -2.0 * DMFFB_DIELECTRIC * (k / 1.7724538509055159) * 2.0 * k * k / 3.0 : 0.0;
+    k_field_combine<T><<<nblk(3 * h->n, 256), 256, 0, s>>>(h->n, recip, (const T*)h->d_fieldT, U, h->d_Qg, h->d_pol,
+                                                           self1, include_perm ? 1 : 0, out);
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
+template <typename T>
+int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
+                  int64_t npairs, double* U, dmffb_admp_result* res) {
+    const int n = h->n;
+    const unsigned nb3 = nblk(3 * n, 256);
+    double* sc = h->d_scal + S_CG;
+    int st;
+    if (h->solver == DMFFB_SOLVER_REFERENCE) {
+        int it = 0;
+        bool conv = false;
+        const int maxit = h->steps_pol > 0 ? h->steps_pol : h->max_iter;
+        for (it = 0; it < maxit; ++it) {
+            if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, h->d_b))) return st;
+            if (h->steps_pol <= 0) {
+                CK(cudaMemsetAsync(sc + 8, 0, sizeof(double), s));
+                k_absmax<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_pol, 0.001, (unsigned long long*)(sc + 8));
+                CK(cudaMemcpyAsync(h->h_scal, sc + 8, sizeof(double), cudaMemcpyDeviceToHost, s));
+                CK(cudaStreamSynchronize(s));
+                if (h->h_scal[0] < h->cg_tol) {
+                    conv = true;
+                    break;
+                }
+            }
+            k_ref_step<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_pol, U, nullptr);
+        }
+        if (h->steps_pol > 0) {
+            conv = true;
+            it = h->steps_pol;
+        }
+        res->n_iter = it;
+        res->converged = conv ? 1 : 0;
+        res->residual_rms = conv && h->steps_pol <= 0 ? h->h_scal[0] : -1.0;
+        return DMFFB_OK;
+    }
+    // CG on A U = -b
+    if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b))) return st;
+    if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
+    k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_Ap, h->d_pol, h->d_r, h->d_z, h->d_p);
+    CK(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
+    k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_r, h->d_z, h->d_r, h->d_r, sc + 0, sc + 3);
+    k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_b, h->d_b, nullptr, nullptr, sc + 4, nullptr);
+    int it = 0;
+    bool conv = false;
+    double rms = 0.0, rms_b = 0.0;
+    int slot = 0;
+    for (it = 0; it <= h->max_iter; ++it) {
+        CK(cudaMemcpyAsync(h->h_scal, sc + 3, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        rms = sqrt(h->h_scal[0] / (3.0 * n));
+        if (it == 0) rms_b = sqrt(h->h_scal[1] / (3.0 * n));
+        if (!std::isfinite(rms)) return fail(h, DMFFB_NONFINITE, "non-finite residual in the dipole solve");
+        // relative criterion: RMS(dE/dU) below cg_tol times the RMS permanent field
+        if (rms <= h->cg_tol * rms_b) {
+            conv = true;
+            break;
+        }
+        if (it == h->max_iter) break;
+        if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, h->d_p, false, h->d_Ap))) return st;
+        CK(cudaMemsetAsync(sc + 2, 0, 2 * sizeof(double), s));  // pAp, rr
+        CK(cudaMemsetAsync(sc + (1 - slot), 0, sizeof(double), s));
+        k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_p, h->d_Ap, nullptr, nullptr, sc + 2, nullptr);
+        k_cg_update<<<nb3, 256, 0, s>>>(n, sc, slot, U, h->d_r, h->d_z, h->d_p, h->d_Ap, h->d_pol, sc + (1 - slot),
+                                        sc + 3);
+        k_cg_p<<<nb3, 256, 0, s>>>(n, sc, slot, 1 - slot, h->d_z, h->d_p);
+        slot = 1 - slot;
+    }
+    res->n_iter = it;
+    res->converged = conv ? 1 : 0;
+    res->residual_rms = rms;
+    return DMFFB_OK;
+}
+
+template <typename T>
+int ensure_pairs(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx);
+
+template <typename T>
+int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const double* box, const int32_t* pairs,
+                 int64_t npairs, double* U, double* forces, dmffb_admp_result* res) {
+    if (!h->params_set) return fail(h, DMFFB_BAD_ARG, "dmffb_admp_set_params was not called");
+    if (!pos || !box || !res) return fail(h, DMFFB_BAD_ARG, "null pos/box/result");
+    if (h->lpol && !U) return fail(h, DMFFB_BAD_ARG, "polarizable system needs U_inout");
+    Box bx;
+    make_box(box, bx);
+    h->last_box = bx;
+    h->cur_pos = pos;
+    memset(res, 0, sizeof(*res));
+    const int n = h->n;
+    int st;
+    if (!pairs) {
+        if (!h->have_pairs)
+            if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        pairs = h->d_pairs;
+        npairs = h->npairs;
+    }
+    res->n_pairs = npairs;
+    if (h->timing) CK(cudaEventRecord(h->ev[0], s));
+    CK(cudaMemsetAsync(h->d_scal, 0, N_SCAL * sizeof(double), s));
+    CK(cudaMemsetAsync(h->d_gpair, 0, (size_t)3 * n * sizeof(T), s));
+    CK(cudaMemsetAsync(h->d_torque, 0, (size_t)3 * n * sizeof(T), s));
+    CK(cudaMemsetAsync(h->d_grad, 0, (size_t)3 * n * sizeof(double), s));
+    CK(cudaMemsetAsync(h->d_gQ, 0, (size_t)9 * n * sizeof(double), s));
+    PrepArgs<T> pa;
+    pa.f.n = n;
+    pa.f.pos = pos;
+    pa.f.axis_type = h->d_axis_type;
+    pa.f.axis_idx = h->d_axis_idx;
+    pa.f.box = bx;
+    pa.Qloc = h->d_Qloc;
+    pa.lmax = h->lmax;
+    pa.posT = (T*)h->d_posT;
+    pa.QgT = (T*)h->d_QgT;
+    pa.Qg = h->d_Qg;
+    k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa);
+    CK(cudaGetLastError());
+    if (h->timing) CK(cudaEventRecord(h->ev[1], s));
+    if (h->lpol) {
+        if ((st = solve_dipoles<T>(h, s, pos, bx, pairs, npairs, U, res))) return st;
+    } else {
+        res->converged = 1;
+    }
+    if (h->timing) CK(cudaEventRecord(h->ev[2], s));
+    if (npairs > 0) {
+        PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, h->lpol ? U : nullptr);
+        if (h->lpol) k_admp_pair<T, true, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a);
+        else k_admp_pair<T, false, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a);
+        CK(cudaGetLastError());
+    }
+    if (h->timing) CK(cudaEventRecord(h->ev[3], s));
+    if (h->lpme && h->have_plans) {
+        if ((st = recip_pass<T>(h, s, pos, bx, true, h->lpol ? U : nullptr, GATHER_FULL, nullptr, 0))) return st;
+    }
+    if (h->timing) CK(cudaEventRecord(h->ev[4], s));
+    SelfArgs<T> sa;
+    sa.f = pa.f;
+    sa.Qg = h->d_Qg;
+    sa.U = h->lpol ? U : nullptr;
+    sa.pol = h->lpol ? h->d_pol : nullptr;
+    sa.torque = (const T*)h->d_torque;
+    sa.kappa = h->kappa;
+    sa.lmax_eff = lmax_eff(h);
+    sa.lpme = h->lpme;
+    sa.want_box = 1;
+    sa.grad = h->d_grad;
+    sa.scal = h->d_scal + S_SELF;
+    sa.tau_out = nullptr;
+    if (h->lmax == 0) sa.f.axis_idx = nullptr;
+    k_self_frames<T><<<nblk(n, 128), 128, 0, s>>>(sa);
+    if (forces) k_finalize_forces<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_gpair, h->d_grad, forces);
+    CK(cudaGetLastError());
+    if (h->timing) CK(cudaEventRecord(h->ev[5], s));
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double* sc = h->h_scal;
+    res->e_real = sc[S_EREAL];
+    res->e_recip = sc[S_RECIP];
+    res->e_self = sc[S_SELF];
+    res->e_pol = sc[S_SELF + 1];
+    res->energy = res->e_real + res->e_recip + res->e_self + res->e_pol;
+    // box gradient: pair images + frame images + reciprocal (k-space and mesh-coordinate parts)
+    double bg[9];
+    for (int k = 0; k < 9; ++k) bg[k] = sc[S_EREAL + 1 + k] + sc[S_SELF + 2 + k];
+    if (h->lpme && h->have_plans) {
+        const double* hi = bx.hinv;  // h^-T[a][b] = hinv[b][a]
+        const double E = sc[S_RECIP];
+        const double* t = sc + S_RECIP + 1;
+        const double Tkk[9] = {t[0], t[3], t[4], t[3], t[1], t[5], t[4], t[5], t[2]};
+        const MeshGeom g = mesh_geom(bx, h->K);
+        const double* X = sc + S_GATHER + 1;  // X_NA[j][c]
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                double v = -E * hi[3 * b + a];
+                double s2 = 0.0;
+                for (int k = 0; k < 3; ++k) s2 += hi[3 * k + a] * Tkk[3 * k + b];
+                v -= 2.0 * s2;
+                // -(h^-T X^T NA)[a][b] = -sum_{k,j} hinv[k][a] X[j][k] NA[j][b]
+                double s3 = 0.0;
+                for (int k = 0; k < 3; ++k)
+                    for (int j = 0; j < 3; ++j) s3 += hi[3 * k + a] * X[3 * j + k] * g.NA[3 * j + b];
+                v -= s3;
+                bg[3 * a + b] += v;
+            }
+    }
+    for (int k = 0; k < 9; ++k) res->box_grad[k] = bg[k];
+    if (h->timing) {
+        float ms;
+        for (int k = 0; k < 5; ++k) {
+            cudaEventElapsedTime(&ms, h->ev[k], h->ev[k + 1]);
+            h->t_ms[k] = ms;
+        }
+        cudaEventElapsedTime(&ms, h->ev[0], h->ev[5]);
+        h->t_ms[5] = ms;
+    }
+    if (!std::isfinite(res->energy)) return fail(h, DMFFB_NONFINITE, "non-finite energy");
+    if (h->lpol && !res->converged) {
+        h->err = "induced dipoles did not converge";
+        return DMFFB_NOT_CONVERGED;
+    }
+    return DMFFB_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* dmffb_last_error(const dmffb_engine* h) { return h ? h->err.c_str() : "null handle"; }
+
+int dmffb_admp_create(const dmffb_admp_desc* d, dmffb_engine** out) {
+    if (!d || !out) return DMFFB_BAD_ARG;
+    *out = nullptr;
+    if (d->n_atoms <= 0 || d->lmax < 0 || d->lmax > 2 || (d->precision != DMFFB_FP32 && d->precision != DMFFB_FP64))
+        return DMFFB_BAD_ARG;
+    if (d->lpme && (d->K[0] <= 0 || d->K[1] <= 0 || d->K[2] <= 0 || !(d->kappa > 0))) return DMFFB_BAD_ARG;
+    dmffb_engine* h = new dmffb_engine();
+    h->n = d->n_atoms;
+    h->lmax = d->lmax;
+    h->lpol = d->lpol ? 1 : 0;
+    h->lpme = d->lpme ? 1 : 0;
+    h->prec = d->precision;
+    h->rc = d->rc;
+    h->kappa = d->lpme ? d->kappa : 0.0;
+    for (int k = 0; k < 3; ++k) h->K[k] = d->lpme ? d->K[k] : 0;
+    for (int k = 0; k < 6; ++k) {
+        h->ms[k] = d->mscales[k];
+        h->ps[k] = d->pscales[k];
+        h->dsc[k] = d->dscales[k];
+    }
+    h->solver = d->solver;
+    h->cg_tol = d->cg_tol > 0 ? d->cg_tol : 1e-6;
+    h->max_iter = d->max_iter > 0 ? d->max_iter : 500;
+    h->steps_pol = d->steps_pol;
+    const int n = h->n;
+    const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
+    int st = 0;
+#define AL(p, b)                                  \
+    if ((st = dalloc(h, &(p), (b))) != DMFFB_OK) { \
+        *out = h;                                 \
+        return st;                                \
+    }
+    AL(h->d_axis_type, n * sizeof(int32_t));
+    AL(h->d_axis_idx, 3 * n * sizeof(int32_t));
+    {
+        std::vector<int32_t> at(n, DMFFB_NOAXISTYPE), ai(3 * n, -1);
+        if (d->axis_types) for (int i = 0; i < n; ++i) at[i] = d->axis_types[i];
+        if (d->axis_indices) for (int i = 0; i < 3 * n; ++i) ai[i] = d->axis_indices[i];
+        for (int i = 0; i < n; ++i) {
+            if (at[i] < 0 || at[i] > 5) { *out = h; return fail(h, DMFFB_BAD_ARG, "bad axis type"); }
+            for (int k = 0; k < 3; ++k)
+                if (ai[3 * i + k] >= n) { *out = h; return fail(h, DMFFB_BAD_ARG, "axis index out of range"); }
+            // every axis atom the frame type reads must exist
+            const int need = (at[i] == DMFFB_ZBISECT || at[i] == DMFFB_THREEFOLD) ? 3
+                             : (at[i] == DMFFB_ZONLY ? 1 : (at[i] == DMFFB_NOAXISTYPE ? 0 : 2));
+            if (d->lmax > 0)
+                for (int k = 0; k < need; ++k)
+                    if (ai[3 * i + k] < 0) { *out = h; return fail(h, DMFFB_BAD_ARG, "missing axis atom"); }
+        }
+        cudaMemcpy(h->d_axis_type, at.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(h->d_axis_idx, ai.data(), 3 * n * sizeof(int32_t), cudaMemcpyHostToDevice);
+        // sparse covalent map -> per-atom rows of j > i
+        std::vector<int32_t> cnt(n + 1, 0);
+        for (int64_t r = 0; r < d->n_cov; ++r) {
+            int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
+            if (i < 0 || j < 0 || i >= n || j >= n || i == j) { *out = h; return fail(h, DMFFB_BAD_ARG, "bad covalent row"); }
+            cnt[std::min(i, j) + 1]++;
+        }
+        for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+        std::vector<int32_t> cj(std::max<int64_t>(d->n_cov, 1)), cn(std::max<int64_t>(d->n_cov, 1)), cur(cnt.begin(), cnt.end() - 1);
+        for (int64_t r = 0; r < d->n_cov; ++r) {
+            int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
+            int lo = std::min(i, j), hi = std::max(i, j);
+            int k = cur[lo]++;
+            cj[k] = hi;
+            cn[k] = d->cov_rows[3 * r + 2];
+        }
+        AL(h->d_cov_ptr, (n + 1) * sizeof(int32_t));
+        AL(h->d_cov_j, cj.size() * sizeof(int32_t));
+        AL(h->d_cov_nb, cn.size() * sizeof(int32_t));
+        cudaMemcpy(h->d_cov_ptr, cnt.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(h->d_cov_j, cj.data(), cj.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+        cudaMemcpy(h->d_cov_nb, cn.data(), cn.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    }
+    AL(h->d_Qloc, 9 * n * sizeof(double));
+    AL(h->d_pol, n * sizeof(double));
+    AL(h->d_thole, n * ts);
+    AL(h->d_polsix, n * ts);
+    AL(h->d_pos, 3 * n * sizeof(double));
+    AL(h->d_U, 3 * n * sizeof(double));
+    AL(h->d_forces, 3 * n * sizeof(double));
+    AL(h->d_posT, 4 * n * ts);
+    AL(h->d_Qg, 9 * n * sizeof(double));
+    AL(h->d_QgT, 9 * n * ts);
+    AL(h->d_gpair, 3 * n * ts);
+    AL(h->d_torque, 3 * n * ts);
+    AL(h->d_fieldT, 3 * n * ts);
+    AL(h->d_grad, 3 * n * sizeof(double));
+    AL(h->d_scal, N_SCAL * sizeof(double));
+    AL(h->d_gQ, 9 * n * sizeof(double));
+    if (h->lpol) {
+        AL(h->d_b, 3 * n * sizeof(double));
+        AL(h->d_r, 3 * n * sizeof(double));
+        AL(h->d_z, 3 * n * sizeof(double));
+        AL(h->d_p, 3 * n * sizeof(double));
+        AL(h->d_Ap, 3 * n * sizeof(double));
+        AL(h->d_fr, 3 * n * sizeof(double));
+    }
+    if (cudaMallocHost((void**)&h->h_scal, N_SCAL * sizeof(double)) != cudaSuccess) {
+        *out = h;
+        return fail(h, DMFFB_OOM, "cudaMallocHost failed");
+    }
+    if (h->lpme) {
+        const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
+        const int64_t Kc = (int64_t)h->K[0] * h->K[1] * (h->K[2] / 2 + 1);
+        AL(h->d_grid, K3 * ts);
+        AL(h->d_cgrid, 2 * Kc * ts);
+        AL(h->d_bmod, (h->K[0] + h->K[1] + h->K[2]) * sizeof(double));
+        // per-dimension B-spline moduli, recip.py:440-448: sum_{m=-2..2} M6(m+3) cos(2 pi m k / K)
+        const double M6[5] = {1.0 / 120, 26.0 / 120, 66.0 / 120, 26.0 / 120, 1.0 / 120};
+        std::vector<double> bm;
+        for (int dd = 0; dd < 3; ++dd)
+            for (int k = 0; k < h->K[dd]; ++k) {
+                const int m = k < (h->K[dd] + 1) / 2 ? k : k - h->K[dd];
+                double s = 0;
+                for (int q = -2; q <= 2; ++q) s += M6[q + 2] * cos(2.0 * M_PI * q * m / h->K[dd]);
+                bm.push_back(s);
+            }
+        cudaMemcpy(h->d_bmod, bm.data(), bm.size() * sizeof(double), cudaMemcpyHostToDevice);
+        cufftType tf = h->prec == DMFFB_FP32 ? CUFFT_R2C : CUFFT_D2Z;
+        cufftType tb = h->prec == DMFFB_FP32 ? CUFFT_C2R : CUFFT_Z2D;
+        if (cufftPlan3d(&h->plan_f, h->K[0], h->K[1], h->K[2], tf) != CUFFT_SUCCESS ||
+            cufftPlan3d(&h->plan_b, h->K[0], h->K[1], h->K[2], tb) != CUFFT_SUCCESS) {
+            *out = h;
+            return fail(h, DMFFB_CUFFT_ERROR, "cufftPlan3d failed");
+        }
+        h->have_plans = true;
+    }
+    for (int k = 0; k < 8; ++k) cudaEventCreate(&h->ev[k]);
+#undef AL
+    cudaError_t e = cudaDeviceSynchronize();
+    *out = h;
+    if (e != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, cudaGetErrorString(e));
+    return DMFFB_OK;
+}
+
+void dmffb_destroy(dmffb_engine* h) {
+    if (!h) return;
+    void* ptrs[] = {h->d_axis_type, h->d_axis_idx, h->d_cov_ptr, h->d_cov_j, h->d_cov_nb, h->d_Qloc, h->d_pol,
+                    h->d_thole, h->d_polsix, h->d_pos, h->d_U, h->d_forces, h->d_posT, h->d_Qg, h->d_QgT,
+                    h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
+                    h->d_Ap, h->d_fr, h->d_gQ, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
+                    h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
+                    h->d_cub};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->have_plans) {
+        cufftDestroy(h->plan_f);
+        cufftDestroy(h->plan_b);
+    }
+    for (int k = 0; k < 8; ++k) cudaEventDestroy(h->ev[k]);
+    delete h;
+}
+
+int dmffb_admp_set_params(dmffb_engine* h, const double* Q_local, const double* pol, const double* thole) {
+    if (!h || !Q_local) return fail(h, DMFFB_BAD_ARG, "null handle or Q_local");
+    if (h->lpol && (!pol || !thole)) return fail(h, DMFFB_BAD_ARG, "polarizable system needs pol and thole");
+    const int n = h->n;
+    CK(cudaMemcpy(h->d_Qloc, Q_local, 9 * n * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<double> pz(n, 0.0);
+    CK(cudaMemcpy(h->d_pol, pol ? pol : pz.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    double* dth = nullptr;
+    if (thole) {
+        CK(cudaMalloc((void**)&dth, n * sizeof(double)));
+        CK(cudaMemcpy(dth, thole, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (h->prec == DMFFB_FP32)
+        k_set_thole<float><<<nblk(n, 128), 128>>>(n, h->d_pol, dth, (float*)h->d_thole, (float*)h->d_polsix);
+    else
+        k_set_thole<double><<<nblk(n, 128), 128>>>(n, h->d_pol, dth, (double*)h->d_thole, (double*)h->d_polsix);
+    CK(cudaDeviceSynchronize());
+    if (dth) cudaFree(dth);
+    h->params_set = true;
+    return DMFFB_OK;
+}
+
+int dmffb_admp_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                       int64_t npairs, double* U_inout, double* forces_out, dmffb_admp_result* result) {
+    if (!h) return DMFFB_BAD_ARG;
+    if (pairs && npairs < 0) return fail(h, DMFFB_BAD_ARG, "negative npairs");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (h->prec == DMFFB_FP32) return compute_impl<float>(h, s, pos, box, pairs, npairs, U_inout, forces_out, result);
+    return compute_impl<double>(h, s, pos, box, pairs, npairs, U_inout, forces_out, result);
+}
+
+int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* box, const int32_t* pairs,
+                            int64_t npairs, double* U_inout, double* forces_out, dmffb_admp_result* result) {
+    if (!h || !pos) return fail(h, DMFFB_BAD_ARG, "null handle or positions");
+    const int n = h->n;
+    cudaStream_t s = 0;
+    CK(cudaMemcpyAsync(h->d_pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    int32_t* dp = nullptr;
+    if (pairs) {
+        CK(cudaMalloc((void**)&dp, std::max<int64_t>(npairs, 1) * 3 * sizeof(int32_t)));
+        CK(cudaMemcpyAsync(dp, pairs, npairs * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    }
+    if (h->lpol) {
+        if (U_inout) CK(cudaMemcpyAsync(h->d_U, U_inout, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+        else CK(cudaMemsetAsync(h->d_U, 0, 3 * n * sizeof(double), s));
+    }
+    int st = dmffb_admp_compute(h, s, h->d_pos, box, dp, npairs, h->lpol ? h->d_U : nullptr, h->d_forces, result);
+    if (dp) cudaFree(dp);
+    if (st != DMFFB_OK && st != DMFFB_NOT_CONVERGED) return st;
+    if (forces_out) CK(cudaMemcpy(forces_out, h->d_forces, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (h->lpol && U_inout) CK(cudaMemcpy(U_inout, h->d_U, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    return st;
+}
+
+int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                     int64_t npairs, const double* U, double* field_out) {
+    if (!h || !pos || !box || !field_out) return fail(h, DMFFB_BAD_ARG, "null argument");
+    if (!h->lpol) return fail(h, DMFFB_BAD_ARG, "field requires a polarizable system");
+    cudaStream_t s = (cudaStream_t)stream;
+    Box bx;
+    make_box(box, bx);
+    h->cur_pos = pos;
+    if (!pairs) {
+        if (!h->have_pairs) {
+            int st = dmffb_admp_build_neighbors(h, stream, pos, box);
+            if (st) return st;
+        }
+        pairs = h->d_pairs;
+        npairs = h->npairs;
+    }
+    const int n = h->n;
+    auto run = [&](auto tag) -> int {
+        using T = decltype(tag);
+        PrepArgs<T> pa;
+        pa.f.n = n;
+        pa.f.pos = pos;
+        pa.f.axis_type = h->d_axis_type;
+        pa.f.axis_idx = h->d_axis_idx;
+        pa.f.box = bx;
+        pa.Qloc = h->d_Qloc;
+        pa.lmax = h->lmax;
+        pa.posT = (T*)h->d_posT;
+        pa.QgT = (T*)h->d_QgT;
+        pa.Qg = h->d_Qg;
+        k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa);
+        int st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out);
+        if (st) return st;
+        CK(cudaStreamSynchronize(s));
+        return DMFFB_OK;
+    };
+    if (h->prec == DMFFB_FP32) return run(float(0));
+    return run(double(0));
+}
+
+int dmffb_admp_multipole_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal) {
+    (void)stream;
+    (void)dE_dQlocal;
+    if (!h || !dE_dQglobal) return fail(h, DMFFB_BAD_ARG, "null argument");
+    CK(cudaMemcpy(dE_dQglobal, h->d_gQ, 9 * h->n * sizeof(double), cudaMemcpyDeviceToDevice));
+    return DMFFB_OK;
+}
+
+int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box, double rc,
+                          int32_t* pairs_out, int64_t capacity, int64_t* npairs_out) {
+    if (!h || !pos || !box || !npairs_out) return fail(h, DMFFB_BAD_ARG, "null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = h->n;
+    Box bx;
+    make_box(box, bx);
+    // cells per axis from the perpendicular widths V / |a_i x a_j|
+    const double* m = bx.h;
+    const double V = fabs(det3(m));
+    int nc[3];
+    bool cells = true;
+    for (int k = 0; k < 3; ++k) {
+        const double* u = m + 3 * ((k + 1) % 3);
+        const double* w = m + 3 * ((k + 2) % 3);
+        const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+        const double width = V / sqrt(cx * cx + cy * cy + cz * cz);
+        nc[k] = (int)floor(width / rc);
+        if (nc[k] > 64) nc[k] = 64;
+        if (nc[k] < 3) cells = false;
+    }
+    int st;
+    if (!h->d_pcount) {
+        if ((st = dalloc(h, &h->d_pcount, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_poff, (n + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_atom_cell, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_atoms, n * sizeof(int32_t)))) return st;
+    }
+    const int ncell = cells ? nc[0] * nc[1] * nc[2] : 1;
+    if (ncell + 1 > h->ncell_cap) {
+        if (h->d_cell_count) { cudaFree(h->d_cell_count); cudaFree(h->d_cell_start); cudaFree(h->d_cell_cursor); }
+        h->ncell_cap = ncell + 1;
+        if ((st = dalloc(h, &h->d_cell_count, h->ncell_cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_start, h->ncell_cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_cursor, h->ncell_cap * sizeof(int32_t)))) return st;
+    }
+    // scan workspace
+    size_t need = 0, need2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, (int32_t*)nullptr, (int32_t*)nullptr, ncell + 1);
+    cub::DeviceScan::InclusiveSum(nullptr, need2, (int32_t*)nullptr, (int64_t*)nullptr, n);
+    need = std::max(need, need2);
+    if (need > h->cub_bytes) {
+        if (h->d_cub) cudaFree(h->d_cub);
+        h->cub_bytes = need;
+        if ((st = dalloc(h, &h->d_cub, need))) return st;
+    }
+    NbArgs a;
+    a.n = n;
+    a.pos = pos;
+    a.box = bx;
+    a.rc = rc;
+    for (int k = 0; k < 3; ++k) a.nc[k] = cells ? nc[k] : 1;
+    a.cov_ptr = h->d_cov_ptr;
+    a.cov_j = h->d_cov_j;
+    a.cov_nb = h->d_cov_nb;
+    a.count = h->d_pcount;
+    a.offset = h->d_poff;
+    a.pairs = pairs_out;
+    a.cap = capacity;
+    if (cells) {
+        CK(cudaMemsetAsync(h->d_cell_count, 0, (ncell + 1) * sizeof(int32_t), s));
+        CK(cudaMemsetAsync(h->d_cell_cursor, 0, (ncell + 1) * sizeof(int32_t), s));
+        k_cell_count<<<nblk(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], h->d_atom_cell, h->d_cell_count);
+        size_t tb = h->cub_bytes;
+        cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_cell_count, h->d_cell_start, ncell + 1, s);
+        k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(n, h->d_atom_cell, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms);
+        a.cell_start = h->d_cell_start;
+        a.cell_atoms = h->d_cell_atoms;
+        k_pairs<0><<<nblk(n, 128), 128, 0, s>>>(a);
+    } else {
+        k_pairs_all<0><<<nblk(n, 128), 128, 0, s>>>(a);
+    }
+    {
+        size_t tb = h->cub_bytes;
+        CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
+        cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount, h->d_poff + 1, n, s);
+    }
+    int64_t total = 0;
+    CK(cudaMemcpyAsync(&total, h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *npairs_out = total;
+    if (total > capacity || !pairs_out) {
+        h->err = "neighbour capacity too small";
+        return DMFFB_NEIGHBOR_OVERFLOW;
+    }
+    if (cells) k_pairs<1><<<nblk(n, 128), 128, 0, s>>>(a);
+    else k_pairs_all<1><<<nblk(n, 128), 128, 0, s>>>(a);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return DMFFB_OK;
+}
+
+int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box) {
+    if (!h) return DMFFB_BAD_ARG;
+    int64_t need = 0;
+    int st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
+    if (st == DMFFB_NEIGHBOR_OVERFLOW) {
+        if (h->d_pairs) cudaFree(h->d_pairs);
+        h->pair_cap = (int64_t)(need * 1.3) + 64;  // headroom as in nblist.py:37-38
+        if ((st = dalloc(h, &h->d_pairs, h->pair_cap * 3 * sizeof(int32_t)))) return st;
+        st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
+    }
+    if (st) return st;
+    h->npairs = need;
+    h->have_pairs = true;
+    return DMFFB_OK;
+}
+
+int dmffb_get_timings(const dmffb_engine* h, double* ms_out, int32_t n) {
+    if (!h || !ms_out) return DMFFB_BAD_ARG;
+    for (int k = 0; k < n && k < 6; ++k) ms_out[k] = h->t_ms[k];
+    return DMFFB_OK;
+}
+
+int dmffb_set_timing(dmffb_engine* h, int32_t enabled) {
+    if (!h) return DMFFB_BAD_ARG;
+    h->timing = enabled != 0;
+    return DMFFB_OK;
+}
+
+}  // extern "C"

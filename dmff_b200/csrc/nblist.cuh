@@ -1,0 +1,154 @@
+// Cell-list neighbour build (sm_100a), replacing the freud AABB query behind
+// NeighborList.allocate (dmff/common/nblist.py:27-55).
+//
+// Output rows (i, j, nbond), i < j, sorted by i: exactly the pairs whose minimum-image distance
+// (the reference's pbc_shift, spatial.py:14-32) is < rc, with nbond read from a sparse
+// covalent map (the reference reads a dense N x N map, nblist.py:22-25).  The distance test
+// runs in FP64 with every product and sum rounded separately in a fixed order, so the pair set
+// is reproducible bit for bit by an elementwise float64 computation on the host.
+//
+// Atoms are binned by fractional coordinates into nc_k >= 3 cells per axis (cell width >=
+// rc measured perpendicular to the other two lattice vectors), counting-sorted by cell,
+// and each atom scans the 27 surrounding cells twice (count, then write).
+#pragma once
+#include "common.cuh"
+
+namespace dmffb {
+
+struct NbArgs {
+    int n;
+    const double* pos;
+    Box box;
+    double rc;
+    int nc[3];
+    const int32_t* cell_start;  // [ncell+1]
+    const int32_t* cell_atoms;  // [n]
+    const int32_t* cov_ptr;     // [n+1] rows of j > i
+    const int32_t* cov_j;
+    const int32_t* cov_nb;
+    int32_t* count;             // [n] (pass 0) per-atom pair counts
+    const int64_t* offset;      // [n+1] (pass 1)
+    int32_t* pairs;             // [cap*3]
+    int64_t cap;
+};
+
+// exact, non-contracted FP64 minimum-image distance test (order: x, y, z; left to right)
+__device__ __forceinline__ bool within_rc(const Box& b, const double* pi, const double* pj, double rc) {
+    const double d0 = __dsub_rn(pj[0], pi[0]);
+    const double d1 = __dsub_rn(pj[1], pi[1]);
+    const double d2 = __dsub_rn(pj[2], pi[2]);
+    double s[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double t = __dadd_rn(__dadd_rn(__dmul_rn(d0, b.hinv[k]), __dmul_rn(d1, b.hinv[3 + k])), __dmul_rn(d2, b.hinv[6 + k]));
+        s[k] = __dsub_rn(t, floor(__dadd_rn(t, 0.5)));
+    }
+    double e[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        e[c] = __dadd_rn(__dadd_rn(__dmul_rn(s[0], b.h[c]), __dmul_rn(s[1], b.h[3 + c])), __dmul_rn(s[2], b.h[6 + c]));
+    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(e[0], e[0]), __dmul_rn(e[1], e[1])), __dmul_rn(e[2], e[2]));
+    return __dsqrt_rn(r2) < rc;
+}
+
+__device__ __forceinline__ int cell_of(const Box& b, const int nc[3], const double* p, int c3[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double s = p[0] * b.hinv[k] + p[1] * b.hinv[3 + k] + p[2] * b.hinv[6 + k];
+        s -= floor(s);
+        int c = (int)(s * nc[k]);
+        c = c < 0 ? 0 : (c >= nc[k] ? nc[k] - 1 : c);
+        c3[k] = c;
+    }
+    return (c3[0] * nc[1] + c3[1]) * nc[2] + c3[2];
+}
+
+__global__ void k_cell_count(int n, const double* pos, Box b, int nc0, int nc1, int nc2, int32_t* atom_cell,
+                             int32_t* cell_count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nc[3] = {nc0, nc1, nc2};
+    int c3[3];
+    const int c = cell_of(b, nc, pos + 3 * i, c3);
+    atom_cell[i] = c;
+    atomicAdd(cell_count + c, 1);
+}
+
+__global__ void k_cell_fill(int n, const int32_t* atom_cell, const int32_t* cell_start, int32_t* cursor,
+                            int32_t* cell_atoms) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = atom_cell[i];
+    const int k = atomicAdd(cursor + c, 1);
+    cell_atoms[cell_start[c] + k] = i;
+}
+
+__device__ __forceinline__ int lookup_nbond(const NbArgs& a, int i, int j) {
+    for (int k = a.cov_ptr[i]; k < a.cov_ptr[i + 1]; ++k)
+        if (a.cov_j[k] == j) return a.cov_nb[k];
+    return 0;
+}
+
+// pass 0: count pairs per atom; pass 1: write rows at offset[i]
+template <int PASS>
+__global__ void __launch_bounds__(128) k_pairs(NbArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double* pi = a.pos + 3 * i;
+    int c3[3];
+    cell_of(a.box, a.nc, pi, c3);
+    int cnt = 0;
+    int64_t out = (PASS == 1) ? a.offset[i] : 0;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
+                const int c = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+                for (int k = a.cell_start[c]; k < a.cell_start[c + 1]; ++k) {
+                    const int j = a.cell_atoms[k];
+                    if (j <= i) continue;
+                    if (!within_rc(a.box, pi, a.pos + 3 * j, a.rc)) continue;
+                    if (PASS == 1) {
+                        if (out < a.cap) {
+                            a.pairs[3 * out] = i;
+                            a.pairs[3 * out + 1] = j;
+                            a.pairs[3 * out + 2] = lookup_nbond(a, i, j);
+                        }
+                        ++out;
+                    } else {
+                        ++cnt;
+                    }
+                }
+            }
+        }
+    }
+    if (PASS == 0) a.count[i] = cnt;
+}
+
+// small boxes (fewer than 3 cells on an axis): every j > i is a candidate
+template <int PASS>
+__global__ void __launch_bounds__(128) k_pairs_all(NbArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const double* pi = a.pos + 3 * i;
+    int cnt = 0;
+    int64_t out = (PASS == 1) ? a.offset[i] : 0;
+    for (int j = i + 1; j < a.n; ++j) {
+        if (!within_rc(a.box, pi, a.pos + 3 * j, a.rc)) continue;
+        if (PASS == 1) {
+            if (out < a.cap) {
+                a.pairs[3 * out] = i;
+                a.pairs[3 * out + 1] = j;
+                a.pairs[3 * out + 2] = lookup_nbond(a, i, j);
+            }
+            ++out;
+        } else {
+            ++cnt;
+        }
+    }
+    if (PASS == 0) a.count[i] = cnt;
+}
+
+}  // namespace dmffb

@@ -1,0 +1,206 @@
+"""Python handle over the C-ABI engine (libdmffb200.so).
+
+``AdmpEngine`` owns one ``dmffb_engine*``: static system data goes in at construction,
+per-atom parameters through ``set_params``, and ``compute`` evaluates energy, forces,
+box gradient and induced dipoles for positions already on the GPU (torch tensors are used
+only as device buffers; their data pointers go through the C ABI).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+_SOLVERS = {"cg": L.DMFFB_SOLVER_CG, "reference": L.DMFFB_SOLVER_REFERENCE}
+_PREC = {"fp32": L.DMFFB_FP32, "fp64": L.DMFFB_FP64}
+
+
+def _i32(a, shape=None):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _dev(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class AdmpEngine:
+    """One ADMP multipolar PME system on one GPU.
+
+    Parameters mirror ``ADMPPmeForce`` (dmff/admp/pme.py:43-114): ``lmax``, ``lpol``, ``lpme``,
+    ``rc`` (A), ``kappa`` (1/A) and mesh ``K``; ``axis_types``/``axis_indices`` as built by the
+    generator; ``cov_rows`` the sparse covalent map (i, j, nbond); scales of length 6 with the
+    trailing 1.0.  ``precision`` 'fp32' (FP32 pair/mesh arithmetic, FP64 accumulation) or 'fp64'.
+    ``solver`` 'cg' (converged to ``cg_tol`` RMS dE/dU) or 'reference' (the reference's fixed step
+    iteration, ``steps_pol`` steps or until max|dE/dU| < ``cg_tol``)."""
+
+    def __init__(self, n_atoms, lmax, lpol, lpme, rc, kappa, K, axis_types, axis_indices, cov_rows,
+                 mscales, pscales=None, dscales=None, precision="fp32", solver="cg", cg_tol=1e-6, max_iter=500,
+                 steps_pol=None, device=None):
+        self.lib = L.load()
+        self.n = int(n_atoms)
+        self.lpol = bool(lpol)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        d = L.AdmpDesc()
+        d.n_atoms = self.n
+        d.lmax = int(lmax)
+        d.lpol = int(bool(lpol))
+        d.lpme = int(bool(lpme))
+        d.precision = _PREC[precision]
+        d.rc = float(rc)
+        d.kappa = float(kappa) if lpme else 0.0
+        for k in range(3):
+            d.K[k] = int(K[k]) if lpme else 0
+        at = _i32(axis_types if axis_types is not None else np.full(self.n, 5), (self.n,))
+        ai = _i32(axis_indices if axis_indices is not None else np.full((self.n, 3), -1), (self.n * 3,))
+        cov = _i32(cov_rows if cov_rows is not None else np.zeros((0, 3)), (-1,))
+        self._keep = (at, ai, cov)
+        d.axis_types = _ptr(at)
+        d.axis_indices = _ptr(ai)
+        d.n_cov = cov.size // 3
+        d.cov_rows = _ptr(cov)
+        one6 = [0.0, 0.0, 1.0, 1.0, 1.0, 1.0]
+        for k in range(6):
+            d.mscales[k] = float(mscales[k])
+            d.pscales[k] = float((pscales if pscales is not None else one6)[k])
+            d.dscales[k] = float((dscales if dscales is not None else one6)[k])
+        d.solver = _SOLVERS[solver]
+        d.cg_tol = float(cg_tol)
+        d.max_iter = int(max_iter)
+        d.steps_pol = int(steps_pol) if steps_pol else 0
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = self.lib.dmffb_admp_create(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if st != L.DMFFB_OK:
+            msg = self.lib.dmffb_last_error(h).decode() if h.value else "invalid description"
+            if h.value:
+                self.lib.dmffb_destroy(h)
+            self.h = None
+            raise L.EngineError(st, msg)
+        self.U = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+        self.forces = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            try:
+                self.lib.dmffb_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    def _check(self, st, allow=()):
+        if st != L.DMFFB_OK and st not in allow:
+            raise L.EngineError(st, self.lib.dmffb_last_error(self.h).decode())
+        return st
+
+    def set_params(self, Q_local, pol=None, thole=None):
+        Q = np.zeros((self.n, 9), dtype=np.float64)
+        Qi = np.asarray(Q_local.detach().cpu() if torch.is_tensor(Q_local) else Q_local, dtype=np.float64)
+        Q[:, : Qi.shape[1]] = Qi
+        Q = np.ascontiguousarray(Q)
+        p = t = None
+        if pol is not None:
+            p = np.ascontiguousarray(np.asarray(pol.detach().cpu() if torch.is_tensor(pol) else pol, np.float64))
+            t = np.ascontiguousarray(np.asarray(thole.detach().cpu() if torch.is_tensor(thole) else thole, np.float64))
+        with torch.cuda.device(self.device):
+            self._check(self.lib.dmffb_admp_set_params(
+                self.h, Q.ctypes.data_as(ctypes.c_void_p), None if p is None else p.ctypes.data_as(ctypes.c_void_p),
+                None if t is None else t.ctypes.data_as(ctypes.c_void_p)))
+
+    @staticmethod
+    def _box(box):
+        b = np.ascontiguousarray(np.asarray(box.detach().cpu() if torch.is_tensor(box) else box, np.float64).reshape(9))
+        return b
+
+    def compute(self, pos, box, pairs=None, U=None, forces=None, stream=None):
+        """pos: cuda float64 [n,3] (A); box: 3x3 (A); pairs: cuda int32 [np,3] or None (internal list);
+        U: cuda float64 [n,3] initial / output induced dipoles (defaults to the engine's buffer).
+        Returns (result struct, forces tensor, U tensor); forces = -dE/dpos."""
+        assert pos.is_cuda and pos.dtype == torch.float64 and pos.is_contiguous()
+        b = self._box(box)
+        if pairs is not None:
+            assert pairs.is_cuda and pairs.dtype == torch.int32 and pairs.is_contiguous()
+        if U is None:
+            U = self.U
+        if forces is None:
+            forces = self.forces
+        res = L.AdmpResult()
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        st = self.lib.dmffb_admp_compute(
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p),
+            _dev(pairs), 0 if pairs is None else pairs.shape[0], _dev(U) if self.lpol else None, _dev(forces),
+            ctypes.byref(res))
+        self._check(st, allow=(L.DMFFB_NOT_CONVERGED,))
+        return res, forces, U
+
+    def compute_host(self, pos, box, pairs=None, U=None):
+        """Host-buffer entry point: numpy in, numpy out (copies inside the engine)."""
+        pos = np.ascontiguousarray(np.asarray(pos, np.float64))
+        b = self._box(box)
+        pr = None if pairs is None else np.ascontiguousarray(np.asarray(pairs, np.int32))
+        Uh = np.zeros((self.n, 3)) if U is None else np.ascontiguousarray(np.asarray(U, np.float64)).copy()
+        F = np.zeros((self.n, 3))
+        res = L.AdmpResult()
+        with torch.cuda.device(self.device):
+            st = self.lib.dmffb_admp_compute_host(
+                self.h, pos.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p),
+                None if pr is None else pr.ctypes.data_as(ctypes.c_void_p), 0 if pr is None else pr.shape[0],
+                Uh.ctypes.data_as(ctypes.c_void_p), F.ctypes.data_as(ctypes.c_void_p), ctypes.byref(res))
+        self._check(st, allow=(L.DMFFB_NOT_CONVERGED,))
+        return res, F, Uh
+
+    def field(self, pos, box, pairs, U):
+        out = torch.empty((self.n, 3), dtype=torch.float64, device=self.device)
+        b = self._box(box)
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_admp_field(
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p), _dev(pairs),
+            0 if pairs is None else pairs.shape[0], _dev(U), _dev(out)))
+        return out
+
+    def multipole_grads(self):
+        out = torch.empty((self.n, 9), dtype=torch.float64, device=self.device)
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_admp_multipole_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out), None))
+        return out
+
+    def build_neighbors(self, pos, box, rc, capacity=None):
+        """All i<j within rc (FP64 minimum-image test) as a cuda int32 [np,3] tensor sorted by i."""
+        b = self._box(box)
+        s = torch.cuda.current_stream(self.device)
+        need = ctypes.c_int64(0)
+        cap = int(capacity) if capacity else 0
+        buf = torch.empty((max(cap, 1), 3), dtype=torch.int32, device=self.device)
+        st = self.lib.dmffb_build_neighbors(self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos),
+                                            b.ctypes.data_as(ctypes.c_void_p), float(rc), _dev(buf), cap,
+                                            ctypes.byref(need))
+        if st == L.DMFFB_NEIGHBOR_OVERFLOW:
+            cap = int(need.value)
+            buf = torch.empty((max(cap, 1), 3), dtype=torch.int32, device=self.device)
+            st = self.lib.dmffb_build_neighbors(self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos),
+                                                b.ctypes.data_as(ctypes.c_void_p), float(rc), _dev(buf), cap,
+                                                ctypes.byref(need))
+        self._check(st)
+        return buf[: need.value]
+
+    def rebuild_internal_pairs(self, pos, box):
+        b = self._box(box)
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_admp_build_neighbors(self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos),
+                                                        b.ctypes.data_as(ctypes.c_void_p)))
+
+    def set_timing(self, on=True):
+        self.lib.dmffb_set_timing(self.h, int(on))
+
+    def timings(self):
+        arr = (ctypes.c_double * 6)()
+        self.lib.dmffb_get_timings(self.h, arr, 6)
+        return list(arr)

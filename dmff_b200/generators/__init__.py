@@ -1,0 +1,2 @@
+"""Generator registry: importing this package registers the drop-in generator classes."""
+from . import admp  # noqa: F401

@@ -1,0 +1,147 @@
+"""Seeded synthetic inputs with the shapes of the ADMP benchmark workloads.
+
+Water boxes: an m^3 lattice (m = ceil(n^(1/3)), spacing L/m; a seeded random subset of sites
+when n < m^3), rigid waters (O-H 0.9572 A, H-O-H 104.52 deg) jittered by U(+-0.3 A) per axis
+with a uniform random orientation.  Atom order per molecule is O, H1, H2.  Local frames follow
+the water convention of the reference's examples: O is Bisector (z between O->H1 and O->H2, x
+toward H2), H is ZThenX (z toward O, x toward the other H).  The covalent map holds O-H (1) and
+H-H (2).  Per-type multipoles: charges O -0.8 / H +0.4, Cartesian dipoles ~ N(0, 0.1 e A) and
+traceless quadrupoles ~ N(0, 0.1 e A^2) in the reference's internal Angstrom convention, turned
+into harmonics with the reference's cart->harm matrices (dmff/admp/multipole.py:36-72).
+"""
+import math
+
+import numpy as np
+
+# dmff/admp/multipole.py:11-31
+_RT3 = 1.73205080757
+_INV_RT3 = 1.0 / _RT3
+C1_C2H = np.array([[0, 0, 1], [1, 0, 0], [0, 1, 0]], dtype=np.float64)
+C2_C2H = np.array([
+    [0, 0, 1, 0, 0, 0],
+    [0, 0, 0, 0, 2 * _INV_RT3, 0],
+    [0, 0, 0, 0, 0, 2 * _INV_RT3],
+    [_INV_RT3, -_INV_RT3, 0, 0, 0, 0],
+    [0, 0, 0, 2 * _INV_RT3, 0, 0],
+], dtype=np.float64)
+
+BISECTOR, ZTHENX = 1, 0
+
+
+def cart2harm(theta):
+    """Cartesian (c0, dX, dY, dZ, qXX, qYY, qZZ, qXY, qXZ, qYZ) -> 9 harmonic components."""
+    theta = np.atleast_2d(np.asarray(theta, dtype=np.float64))
+    out = np.zeros((theta.shape[0], 9))
+    out[:, 0] = theta[:, 0]
+    if theta.shape[1] >= 4:
+        out[:, 1:4] = theta[:, 1:4] @ C1_C2H.T
+    if theta.shape[1] >= 10:
+        out[:, 4:9] = theta[:, 4:10] @ C2_C2H.T
+    return out
+
+
+def _random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], axis=1)
+
+
+def water_positions(n_waters, L, rng):
+    m = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
+    sites = np.array([(i, j, k) for i in range(m) for j in range(m) for k in range(m)], dtype=np.float64)
+    if n_waters < m ** 3:
+        sites = sites[np.sort(rng.choice(m ** 3, n_waters, replace=False))]
+    centers = (sites + 0.5) * (L / m) + rng.uniform(-0.3, 0.3, size=(n_waters, 3))
+    r, th = 0.9572, math.radians(104.52)
+    body = np.array([[0.0, 0.0, 0.0],
+                     [r * math.sin(th / 2), 0.0, r * math.cos(th / 2)],
+                     [-r * math.sin(th / 2), 0.0, r * math.cos(th / 2)]])
+    R = _random_rotations(rng, n_waters)
+    pos = centers[:, None, :] + np.einsum("nij,aj->nai", R, body)
+    return pos.reshape(-1, 3)
+
+
+def water_topology(n_waters):
+    n = 3 * n_waters
+    o = np.arange(n_waters) * 3
+    types = np.tile([0, 1, 1], n_waters)
+    axis_types = np.tile([BISECTOR, ZTHENX, ZTHENX], n_waters).astype(np.int32)
+    axis_indices = np.full((n, 3), -1, dtype=np.int32)
+    axis_indices[o, 0], axis_indices[o, 1] = o + 1, o + 2
+    axis_indices[o + 1, 0], axis_indices[o + 1, 1] = o, o + 2
+    axis_indices[o + 2, 0], axis_indices[o + 2, 1] = o, o + 1
+    cov = np.concatenate([np.stack([o, o + 1, np.ones_like(o)], 1), np.stack([o, o + 2, np.ones_like(o)], 1),
+                          np.stack([o + 1, o + 2, 2 * np.ones_like(o)], 1)])
+    cov = cov[np.lexsort((cov[:, 1], cov[:, 0]))].astype(np.int32)
+    return types, axis_types, axis_indices, cov
+
+
+def type_multipoles(rng, charges=(-0.8, 0.4), sd_dip=0.1, sd_quad=0.1):
+    rows = []
+    for q in charges:
+        d = rng.normal(0.0, sd_dip, size=3)
+        qxx, qyy, qxy, qxz, qyz = rng.normal(0.0, sd_quad, size=5)
+        rows.append([q, d[0], d[1], d[2], qxx, qyy, -qxx - qyy, qxy, qxz, qyz])
+    return cart2harm(np.array(rows))
+
+
+def water_box(n_waters, L, seed, lmax=2, pol=False, rc=6.0, ethresh=5e-4, pol_O=1.0, pol_H=0.5, thole=0.33):
+    """System dict for an ADMP water box (positions / box in Angstrom)."""
+    rng = np.random.default_rng(seed)
+    pos = water_positions(n_waters, L, rng)
+    types, axis_types, axis_indices, cov = water_topology(n_waters)
+    Qt = type_multipoles(rng)
+    if lmax < 2:
+        Qt[:, 4:] = 0.0
+    if lmax < 1:
+        Qt[:, 1:4] = 0.0
+    kappa = math.sqrt(-math.log(2 * ethresh)) / rc
+    K = int(math.ceil(2 * kappa * L / 3 / ethresh ** 0.2))
+    sysd = dict(
+        n_atoms=3 * n_waters, pos=pos, box=np.eye(3) * L, types=types, axis_types=axis_types,
+        axis_indices=axis_indices, cov_rows=cov, Q_type=Qt, Q_local=Qt[types], lmax=lmax, lpol=pol, rc=rc,
+        ethresh=ethresh, kappa=kappa, K=(K, K, K),
+        mscales=np.array([0.0, 0.0, 1.0, 1.0, 1.0, 1.0]),
+        pscales=np.array([0.0, 0.0, 1.0, 1.0, 1.0, 1.0]),
+        dscales=np.array([1.0, 1.0, 1.0, 1.0, 1.0, 1.0]),
+    )
+    if pol:
+        sysd["pol"] = np.where(types == 0, pol_O, pol_H).astype(np.float64)
+        sysd["thole"] = np.full(3 * n_waters, thole, dtype=np.float64)
+    return sysd
+
+
+def workload(name):
+    """The named benchmark workloads."""
+    if name == "c0":
+        return water_box(216, 18.6, seed=0, lmax=2, pol=False, rc=6.0)
+    if name == "c1":
+        return water_box(4096, 49.7, seed=1, lmax=2, pol=True, rc=8.0)
+    if name == "c2":
+        return water_box(2048, 40.0, seed=2, lmax=2, pol=True, rc=8.0)
+    raise KeyError(name)
+
+
+def serving_sizes(n_requests=2000, seed=3, lo=100, hi=10000):
+    """Log-uniform molecule counts of the serving stream."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(lo), np.log(hi), size=n_requests)).astype(int)
+
+
+def pairs_nbond(pairs, cov_rows, n_atoms):
+    """Fill the third column of (i, j) rows from sparse covalent rows (i < j, nbond)."""
+    key = cov_rows[:, 0].astype(np.int64) * n_atoms + cov_rows[:, 1]
+    order = np.argsort(key)
+    key, nb = key[order], cov_rows[order, 2]
+    q = pairs[:, 0].astype(np.int64) * n_atoms + pairs[:, 1]
+    pos = np.clip(np.searchsorted(key, q), 0, max(len(key) - 1, 0))
+    out = np.zeros(len(pairs), dtype=np.int64)
+    if len(key):
+        hit = key[pos] == q
+        out[hit] = nb[pos[hit]]
+    return out

@@ -1,0 +1,134 @@
+/*
+ * dmffb200.h — C ABI of the B200 ADMP / PME energy-force engine (libdmffb200.so).
+ *
+ * Plain pointers and sizes only; no C++ or torch types cross this boundary.  Every call
+ * returns a status (DMFFB_OK == 0); on failure `dmffb_last_error(h)` holds a message.
+ * Units follow the reference backend: Angstrom, elementary charge, kJ/mol.
+ *
+ * The reference (deepmodeling/DMFF) has no C ABI (backend/c_api/CMakeLists.txt is empty);
+ * each entry point below names the Python interface it replaces.
+ */
+#ifndef DMFFB200_H
+#define DMFFB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    DMFFB_OK = 0,
+    DMFFB_BAD_ARG = 1,
+    DMFFB_OOM = 2,
+    DMFFB_CUDA_ERROR = 3,
+    DMFFB_NOT_CONVERGED = 4,      /* warning: results written, induced dipoles not converged */
+    DMFFB_NEIGHBOR_OVERFLOW = 5,  /* pair capacity too small; *npairs_out holds the count needed */
+    DMFFB_NONFINITE = 6,
+    DMFFB_CUFFT_ERROR = 7
+};
+
+/* local-axis types, dmff/admp/spatial.py:59-65 */
+enum { DMFFB_ZTHENX = 0, DMFFB_BISECTOR = 1, DMFFB_ZBISECT = 2, DMFFB_THREEFOLD = 3,
+       DMFFB_ZONLY = 4, DMFFB_NOAXISTYPE = 5 };
+
+/* arithmetic of the pair / mesh kernels (energies, virials and CG norms are always FP64) */
+enum { DMFFB_FP32 = 0, DMFFB_FP64 = 1 };
+
+/* induced-dipole solver */
+enum { DMFFB_SOLVER_CG = 0,          /* Jacobi-preconditioned CG to RMS(dE/dU) < cg_tol */
+       DMFFB_SOLVER_REFERENCE = 1 }; /* U <- U - (dE/dU) pol / DIELECTRIC, dmff/admp/pme.py:342-423 */
+
+typedef struct dmffb_engine dmffb_engine;
+
+/* Static description of one ADMP multipolar PME system.
+ * Replaces ADMPPmeForce.__init__ (dmff/admp/pme.py:43-114) plus the covalent map that
+ * ADMPPmeGenerator.createPotential builds (dmff/generators/admp.py:1203-1336). */
+typedef struct {
+    int32_t n_atoms;
+    int32_t lmax;             /* 0, 1, 2 */
+    int32_t lpol;             /* induced dipoles on/off */
+    int32_t lpme;             /* 0: kappa = 0 and no reciprocal part (CutoffPeriodic) */
+    int32_t precision;        /* DMFFB_FP32 | DMFFB_FP64 */
+    double rc;                /* cutoff, Angstrom (used by the internal neighbour build) */
+    double kappa;             /* Ewald kappa, 1/Angstrom (setup_ewald_parameters, pme.py:426-466) */
+    int32_t K[3];             /* PME mesh */
+    const int32_t* axis_types;   /* [n_atoms] host, DMFFB_* axis type */
+    const int32_t* axis_indices; /* [n_atoms*3] host, (z, x, y) atoms, -1 = unused */
+    int64_t n_cov;               /* sparse covalent map rows */
+    const int32_t* cov_rows;     /* [n_cov*3] host (i, j, nbond) with i < j, 1 <= nbond <= 6 */
+    double mscales[6];        /* indexed nbond-1, [5] = 1.0 (trailing entry, admp.py:912-918) */
+    double pscales[6];
+    double dscales[6];
+    int32_t solver;           /* DMFFB_SOLVER_* */
+    double cg_tol;            /* CG: stop when RMS(dE/dU) <= cg_tol * RMS(dE/dU at U = 0);
+                                 REFERENCE: POL_CONV, stop when max|dE/dU| < cg_tol (pme.py:394) */
+    int32_t max_iter;         /* CG / reference iteration cap */
+    int32_t steps_pol;        /* REFERENCE solver: >0 runs exactly this many steps (pme.py:404-422) */
+} dmffb_admp_desc;
+
+typedef struct {
+    double energy;            /* total, kJ/mol */
+    double e_real, e_recip, e_self, e_pol;
+    double box_grad[9];       /* dE/dbox (rows = lattice vectors), kJ/mol/A, fixed Cartesian positions */
+    int32_t n_iter;           /* dipole iterations used */
+    int32_t converged;
+    double residual_rms;      /* final RMS dE/dU */
+    int64_t n_pairs;          /* pair rows processed */
+} dmffb_admp_result;
+
+/* ADMPPmeForce(...) — pme.py:43-114 */
+int dmffb_admp_create(const dmffb_admp_desc* desc, dmffb_engine** out);
+void dmffb_destroy(dmffb_engine* h);
+const char* dmffb_last_error(const dmffb_engine* h);
+
+/* Per-atom parameters, host arrays: Q_local [n*9] harmonic local-frame multipoles in the
+ * reference's units (params["ADMPPmeForce"]["Q_local"][map_atomtype], admp.py:1373),
+ * zero-padded to 9 components; pol [n] (A^3) and thole [n] (may be NULL when lpol == 0). */
+int dmffb_admp_set_params(dmffb_engine* h, const double* Q_local, const double* pol, const double* thole);
+
+/* Energy + forces + box gradient: ADMPPmeForce.get_energy (pme.py:186-232) with
+ * jax.value_and_grad over (positions, box).  Device pointers: pos [n*3] A, U_inout [n*3]
+ * (Cartesian induced dipoles e*A; read as the initial guess, overwritten with the solution;
+ * may be NULL when lpol == 0), forces_out [n*3] (= -dE/dpos, may be NULL).  pairs is a
+ * device array of npairs rows (i, j, nbond) with the reference's padding semantics (rows with
+ * i >= j are skipped, utils.py:67-85); pairs == NULL uses the engine's own neighbour list
+ * (built on the first call and by dmffb_admp_build_neighbors).  box [9] is a host array.
+ * stream: a cudaStream_t (NULL = legacy default stream). */
+int dmffb_admp_compute(dmffb_engine* h, void* stream, const double* pos, const double* box,
+                       const int32_t* pairs, int64_t npairs, double* U_inout, double* forces_out,
+                       dmffb_admp_result* result);
+
+/* Same call with HOST buffers: the engine copies pos/pairs/U in and forces/U out
+ * (the path an OpenMM plugin or a ctypes caller without device memory uses). */
+int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* box,
+                            const int32_t* pairs, int64_t npairs, double* U_inout, double* forces_out,
+                            dmffb_admp_result* result);
+
+/* dE/dU at the given dipoles (the "field" of optimize_Uind, pme.py:381-392), device arrays. */
+int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const double* box,
+                     const int32_t* pairs, int64_t npairs, const double* U, double* field_out);
+
+/* Per-atom dE/dQ_global (harmonic, [n*9]) and dE/dQ_local ([n*9]) at the last compute(),
+ * for parameter gradients; device arrays. */
+int dmffb_admp_multipole_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal);
+
+/* Cell-list neighbour build: NeighborList.allocate (dmff/common/nblist.py:27-55) semantics —
+ * all i < j with minimum-image distance < rc (FP64 test), nbond from the covalent map.
+ * pos device [n*3]; box host [9]; rows written to pairs_out (device, capacity rows), sorted by i.
+ * Returns DMFFB_NEIGHBOR_OVERFLOW with *npairs_out = needed count when capacity is short. */
+int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box, double rc,
+                          int32_t* pairs_out, int64_t capacity, int64_t* npairs_out);
+
+/* Rebuild the engine-owned pair list used when compute() gets pairs == NULL. */
+int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box);
+
+/* Per-stage device times of the last compute() in milliseconds (CUDA events):
+ * [0] frames, [1] pol solve, [2] real FULL, [3] recip FULL, [4] self+frames, [5] total. */
+int dmffb_get_timings(const dmffb_engine* h, double* ms_out, int32_t n);
+int dmffb_set_timing(dmffb_engine* h, int32_t enabled);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

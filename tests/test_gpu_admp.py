@@ -1,0 +1,133 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the float64 oracle."""
+import numpy as np
+import pytest
+import torch
+
+from dmff_b200.synthetic import water_box
+from tests.helpers import make_engine, oracle_pairs, oracle_reference, rel_force_rms
+
+pytestmark = pytest.mark.gpu
+
+# tolerances of the FP32 path and of the FP64 instantiation
+TOL = {"fp32": dict(e=1e-5, f=1e-4, b=1e-4), "fp64": dict(e=1e-10, f=1e-8, b=1e-8)}
+
+
+def _run(eng, sysd, pairs):
+    dev = torch.device("cuda")
+    pos = torch.tensor(sysd["pos"], dtype=torch.float64, device=dev)
+    pr = torch.tensor(pairs, dtype=torch.int32, device=dev)
+    res, F, U = eng.compute(pos, sysd["box"], pairs=pr)
+    return res, F.cpu().numpy(), U.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def c0_small():
+    s = water_box(64, 12.4, seed=10, lmax=2, pol=False, rc=6.0)
+    pr = oracle_pairs(s)
+    return s, pr, oracle_reference(s, pr)
+
+
+@pytest.fixture(scope="module")
+def pol_small():
+    s = water_box(64, 12.4, seed=11, lmax=2, pol=True, rc=6.0)
+    pr = oracle_pairs(s)
+    return s, pr, oracle_reference(s, pr, solver="cg", tol=1e-9)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_nonpol_energy_forces_boxgrad(c0_small, prec):
+    s, pr, ref = c0_small
+    eng = make_engine(s, precision=prec)
+    res, F, _ = _run(eng, s, pr)
+    t = TOL[prec]
+    assert abs(res.energy - ref["E"]) <= t["e"] * abs(ref["E"])
+    assert rel_force_rms(F, ref["F"]) <= t["f"]
+    bg = np.array(res.box_grad).reshape(3, 3)
+    assert np.abs(bg - ref["box_grad"]).max() <= t["b"] * np.abs(ref["box_grad"]).max()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_pol_energy_forces_dipoles(pol_small, prec):
+    s, pr, ref = pol_small
+    eng = make_engine(s, precision=prec, cg_tol=1e-6 if prec == "fp32" else 1e-11)
+    res, F, U = _run(eng, s, pr)
+    t = TOL[prec]
+    assert res.converged == 1
+    assert abs(res.energy - ref["E"]) <= t["e"] * abs(ref["E"])
+    assert rel_force_rms(F, ref["F"]) <= t["f"]
+    assert np.abs(U - ref["U"]).max() <= (1e-4 if prec == "fp32" else 1e-8) * np.abs(ref["U"]).max()
+    bg = np.array(res.box_grad).reshape(3, 3)
+    assert np.abs(bg - ref["box_grad"]).max() <= t["b"] * np.abs(ref["box_grad"]).max()
+
+
+def test_reference_solver_matches_fixed_step_oracle():
+    s = water_box(27, 9.3, seed=12, lmax=2, pol=True, rc=4.5)
+    pr = oracle_pairs(s)
+    ref = oracle_reference(s, pr, solver="reference", steps_pol=5)
+    eng = make_engine(s, precision="fp64", solver="reference", steps_pol=5)
+    res, F, U = _run(eng, s, pr)
+    assert res.n_iter == 5
+    assert abs(res.energy - ref["E"]) <= 1e-9 * abs(ref["E"])
+    assert rel_force_rms(F, ref["F"]) <= 1e-8
+
+
+def test_host_buffer_path_matches_device_path(pol_small):
+    s, pr, ref = pol_small
+    eng = make_engine(s, precision="fp32", cg_tol=1e-6)
+    res_d, F_d, U_d = _run(eng, s, pr)
+    res_h, F_h, U_h = eng.compute_host(s["pos"], s["box"], pairs=pr)
+    assert abs(res_h.energy - res_d.energy) <= 1e-6 * abs(res_d.energy)
+    assert rel_force_rms(F_h, F_d) <= 1e-5
+
+
+@pytest.mark.parametrize("name,L,n,rc", [("tiny", 9.3, 27, 4.5), ("c0", 18.6, 216, 6.0), ("mid", 31.0, 1000, 8.0)])
+def test_neighbor_set_bit_exact(name, L, n, rc):
+    import oracle.admp_ref as R
+    s = water_box(n, L, seed=20, lmax=2, pol=False, rc=rc)
+    pr_o = oracle_pairs(s)
+    eng = make_engine(s, precision="fp64")
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
+    rows = eng.build_neighbors(pos, s["box"], rc).cpu().numpy()
+    assert rows.shape[0] == pr_o.shape[0]
+    assert np.all(rows[:, 0] < rows[:, 1])
+    assert np.all(np.diff(rows[:, 0]) >= 0)  # sorted by i
+    got = set(map(tuple, rows.tolist()))
+    want = set(map(tuple, pr_o.tolist()))
+    assert got == want
+
+
+def test_internal_pairs_equal_given_pairs(c0_small):
+    s, pr, ref = c0_small
+    eng = make_engine(s, precision="fp64")
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
+    res, F, _ = eng.compute(pos, s["box"])  # engine-built cell list
+    assert res.n_pairs == len(pr)
+    assert abs(res.energy - ref["E"]) <= 1e-10 * abs(ref["E"])
+    assert rel_force_rms(F.cpu().numpy(), ref["F"]) <= 1e-8
+
+
+@pytest.mark.parametrize("xml,key,dec", [("admp.xml", "dimer_pol_lmax2_steppol5", 1),
+                                         ("admp_mono.xml", "dimer_pol_lmax0_steppol5", 2),
+                                         ("admp_nonpol.xml", "dimer_nonpol_lmax2", 2)])
+def test_dropin_api_water_dimer_goldens(xml, key, dec):
+    """tests/test_admp/test_compute.py:36-145 through Hamiltonian / NeighborList / potential_fn."""
+    import json
+    import os
+    from dmff_b200 import Hamiltonian, NeighborList, PDBFile
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    gold = json.load(open(os.path.join(here, "energies.json")))[key]["value"]
+    H = Hamiltonian(os.path.join(here, "data", xml))
+    pdb = PDBFile(os.path.join(here, "data", "water_dimer.pdb"))
+    pot = H.createPotential(pdb.topology, nonbondedMethod="CutoffPeriodic", nonbondedCutoff=0.4, ethresh=5e-4,
+                            step_pol=5, precision="fp64")
+    box = pdb.topology.getPeriodicBoxVectors()
+    nbl = NeighborList(box, 0.4, pot.meta["cov_map"])
+    nbl.allocate(pdb.positions)
+    assert int((nbl.pairs[:, 0] < nbl.pairs[:, 1]).sum()) == 15
+    assert nbl.pairs.shape[0] == int(15 * 1.3)
+    efunc = pot.getPotentialFunc(names=["ADMPPmeForce"])
+    pos = torch.tensor(pdb.positions, requires_grad=True)
+    E = efunc(pos, box, nbl.pairs, H.paramset)
+    np.testing.assert_almost_equal(E.item(), gold, decimal=dec)
+    (g,) = torch.autograd.grad(E, pos)
+    assert torch.isfinite(g).all()
