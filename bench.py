@@ -1,0 +1,326 @@
+"""Benchmark of the ADMP polarizable PME energy/force/virial step on B200.
+
+Workload (default): 4096 rigid waters (12288 atoms) in a 49.7 A box, lmax=2 multipoles with
+local frames, isotropic polarizabilities (O 1.0, H 0.5 A^3), Thole 0.33, rc = 8 A,
+ethresh = 5e-4 (kappa 0.3285/A, 50^3 mesh); seeded synthetic coordinates and parameters.
+One step = cell-list neighbour rebuild + induced-dipole CG solve (from U = 0) + energy,
+forces and box gradient, FP32 pair / mesh arithmetic with FP64 accumulation.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Multi-GPU runs (torchrun) evaluate one independent replica
+per GPU (the path has no data exchange); value = all atom-evaluations / max-over-ranks time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atom-evals/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="c1")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(name, s, K):
+    return {"workload": {"c1": "polarizable ADMP water box, 4096 waters / 12288 atoms, 49.7 A, rc 8 A",
+                         "c0": "ADMP water box, 216 waters / 648 atoms, 18.6 A, rc 6 A, no polarization",
+                         "c2": "polarizable ADMP water box, 2048 waters / 6144 atoms, 40 A, rc 8 A"}[name],
+            "n_atoms": int(s["n_atoms"]), "lmax": int(s["lmax"]), "polarizable": bool(s["lpol"]),
+            "rc_A": s["rc"], "ethresh": s["ethresh"], "pme_mesh": list(s["K"]),
+            "cg_tol_rel": 1e-6, "l2": "flushed between timed steps (256 MiB write)",
+            "step": "cell-list rebuild + CG dipole solve from U=0 + energy/forces/box gradient"}
+
+
+# ---------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------- roofline
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def roofline(stats, s, npairs, peaks, peak_src, traffic_per_launch=None):
+    """Roofline entry for the kernel class with the largest device time.  Algorithmic work per
+    launch (fixed convention): pair FULL polarizable 1900 flop/pair; pair MATVEC 200 flop/pair;
+    spread N(12 + 4(l+1)^2) + 4K^3 B; gather 4K^3 + N(12 + 4(l+1)^2 + 24) B; convolution 16 K^3 B."""
+    n = s["n_atoms"]
+    K3 = float(np.prod(s["K"]))
+    cls = max((k for k in stats if stats[k][1] > 0 and k != "fft"), key=lambda k: stats[k][0])
+    ms, launches = stats[cls]
+    per_launch_s = ms / 1e3 / launches
+    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12  # TFLOP/s, nominal at max clock
+    if cls in ("pair_full", "pair_matvec", "pair_field"):
+        flop = {"pair_full": 1900, "pair_matvec": 200, "pair_field": 600}[cls] * npairs
+        ach = flop / per_launch_s / 1e12
+        return {"kernel": cls, "bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": ach / fp32_peak, "traffic": traffic_per_launch, "launches": launches,
+                "avg_launch_us": per_launch_s * 1e6,
+                "peak_source": "nominal FP32 CUDA-core peak: 148 SM x 128 lanes x 2 x max SM clock"}
+    lmap = {"spread": 2, "gather_full": 2, "gather_field": 1}
+    if cls == "spread":
+        byts = n * (12 + 4 * 9) + 4 * K3
+    elif cls in ("gather_full", "gather_field"):
+        l = lmap[cls]
+        byts = 4 * K3 + n * (12 + 4 * (l + 1) ** 2 + 24)
+    elif cls == "conv":
+        byts = 16 * K3
+    elif cls == "vector":
+        byts = 5 * 3 * n * 8
+    elif cls == "neighbors":
+        byts = 12 * n + 12 * npairs
+    else:
+        byts = 12 * n
+    ach = byts / per_launch_s / 1e9
+    return {"kernel": cls, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": ach / peaks["hbm_gbs"], "traffic": traffic_per_launch, "launches": launches,
+            "avg_launch_us": per_launch_s * 1e6, "peak_source": f"hbm_gbs ({peak_src})"}
+
+
+# ---------------------------------------------------------------------------------- CPU side
+def cpu_reference_timing(s, n_ref_iter, want_ef=True):
+    """Float64 CPU restatement of the reference path (the oracle) on all host threads: one dE/dU
+    pass (the unit of the dipole solve) and one energy+forces pass of the same workload."""
+    import torch
+    import oracle.admp_ref as R
+    from dmff_b200.synthetic import pairs_nbond
+    torch.set_num_threads(os.cpu_count())
+    pr = R.brute_force_pairs(s["pos"], s["box"], s["rc"])
+    pr[:, 2] = pairs_nbond(pr, s["cov_rows"], s["n_atoms"])
+    f = R.ADMPPmeForce(s["box"], s["axis_types"], s["axis_indices"], s["rc"], s["ethresh"], s["lmax"], s["lpol"],
+                       kappa=s["kappa"], K=s["K"])
+    Ql = torch.tensor(s["Q_local"])
+    rest = (torch.tensor(s["pol"]), torch.tensor(s["thole"]), torch.tensor(s["mscales"]),
+            torch.tensor(s["pscales"]), torch.tensor(s["dscales"]))
+    pos = torch.tensor(s["pos"])
+    box = torch.tensor(s["box"])
+    U0 = torch.zeros((s["n_atoms"], 3), dtype=torch.float64)
+    t0 = time.perf_counter()
+    f.grad_U(pos, box, pr, Ql, U0, *rest)
+    t_g = time.perf_counter() - t0
+    t_ef = None
+    if want_ef:
+        p = pos.clone().requires_grad_(True)
+        b = box.clone().requires_grad_(True)
+        t0 = time.perf_counter()
+        E = f.energy_fn(p, b, pr, Ql, U0, *rest)
+        torch.autograd.grad(E, (p, b))
+        t_ef = time.perf_counter() - t0
+    return t_g, t_ef, torch.get_num_threads()
+
+
+def run_reference(args, s, rank):
+    """--impl reference: the reference's own CPU path (float64 oracle restatement; the JAX
+    reference cannot be installed here) on the host cores, same workload/metric/unit."""
+    if rank != 0:
+        return
+    n_ref_iter = 30  # the reference's MAX_N_POL (dmff/admp/settings.py:3)
+    warm = min(args.warmup, 1)
+    steps = min(args.steps, 3)
+    t_ef = None
+    for _ in range(max(warm, 1)):
+        _, t_ef, cores = cpu_reference_timing(s, n_ref_iter, want_ef=True)
+    tg = []
+    for _ in range(steps):
+        g, _, cores = cpu_reference_timing(s, n_ref_iter, want_ef=False)
+        tg.append(g)
+    t_eval = t_ef + n_ref_iter * statistics.median(tg)
+    value = s["n_atoms"] / t_eval
+    sample = (f"per step: one dE/dU pass of the {s['n_atoms']}-atom box (median of {steps}); one energy+forces "
+              f"pass timed in warm-up ({t_ef:.2f} s); evaluation = E+F + {n_ref_iter} dE/dU passes "
+              f"(the reference's MAX_N_POL)")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": args.gpus,
+           "steps": steps, "warmup": warm, "ms_per_step": t_eval * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": workload_config(args.workload, s, s["K"]),
+           "cpu_baseline": {"value": value, "unit": "atom-evals/s", "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": "atom-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from dmff_b200.synthetic import workload
+    s = workload(args.workload)
+    if args.impl == "reference":
+        run_reference(args, s, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    from dmff_b200.engine import AdmpEngine
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    eng = AdmpEngine(s["n_atoms"], s["lmax"], s["lpol"], True, s["rc"], s["kappa"], s["K"], s["axis_types"],
+                     s["axis_indices"], s["cov_rows"], s["mscales"], s["pscales"], s["dscales"], precision="fp32",
+                     solver="cg", cg_tol=1e-6, max_iter=1000, device=dev)
+    eng.set_params(s["Q_local"], s.get("pol"), s.get("thole"))
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
+    box = s["box"]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        eng.rebuild_internal_pairs(pos, box)
+        eng.U.zero_()
+        return eng.compute(pos, box)
+
+    for _ in range(args.warmup):
+        res, F, U = step()
+    torch.cuda.synchronize()
+    launches0 = eng.counters()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    iters = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            res, F, U = step()
+            evs[k][1].record(stream)
+            iters.append(res.n_iter)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    launches1 = eng.counters()
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * s["n_atoms"] / (total_ms / 1e3)
+
+    # e2e through the host-buffer C-ABI entry (pinned positions in, forces + dipoles out)
+    pos_h = torch.tensor(s["pos"], dtype=torch.float64).pin_memory().numpy()
+    e2e_ms = []
+    for k in range(args.warmup):
+        eng.compute_host(pos_h, box)
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r_h, F_h, U_h = eng.compute_host(pos_h, box)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = sum(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * args.steps * s["n_atoms"] / (e2e_total / 1e3)
+
+    # per-kernel device times over K instrumented steps (events around every launch)
+    eng.set_profiling(True)
+    for k in range(args.steps):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    stats = eng.kernel_stats()
+    eng.set_profiling(False)
+    peaks, src = measured_peaks()
+    roof = roofline(stats, s, int(res.n_pairs), peaks, src)
+
+    out = None
+    if rank == 0:
+        n_iter = int(statistics.median(iters))
+        out = {"metric": METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pairs/mesh, fp64 accumulation",
+               "data": "synthetic", "config": dict(workload_config(args.workload, s, s["K"]),
+                                                   parallelism=f"replicas x{world}"),
+               "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                              "e2e_p50": float(np.percentile(e2e_ms, 50)), "e2e_p99": float(np.percentile(e2e_ms, 99))},
+               "e2e": {"value": e2e_value, "unit": "atom-evals/s", "h2d_bytes_per_step": 2 * 3 * 8 * s["n_atoms"],
+                       "d2h_bytes_per_step": 2 * 3 * 8 * s["n_atoms"],
+                       "path": "dmffb_admp_compute_host (C ABI, host buffers)"},
+               "roofline": roof, "clocks": clk.summary(),
+               "gpu_launches": int(launches1["launches"] - launches0["launches"]),
+               "library_launches": {"cufft_execs": int(launches1["fft_execs"] - launches0["fft_execs"])},
+               "result": {"energy_kJmol": res.energy, "cg_iters": n_iter, "converged": int(res.converged),
+                          "n_pairs": int(res.n_pairs)},
+               "kernel_ms_per_step": {k: v[0] / args.steps for k, v in stats.items() if v[1]}}
+        if world == 1 and not args.no_cpu_baseline:
+            t_g, t_ef, cores = cpu_reference_timing(s, n_iter)
+            t_eval = t_ef + n_iter * t_g
+            out["cpu_baseline"] = {
+                "value": s["n_atoms"] / t_eval, "unit": "atom-evals/s", "cores": cores, "kind": "port",
+                "sample": (f"one dE/dU pass ({t_g:.2f} s) and one energy+forces pass ({t_ef:.2f} s) of the same "
+                           f"box with the float64 oracle; evaluation = E+F + {n_iter} dE/dU passes (the GPU's CG "
+                           f"iteration count)")}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -28,7 +28,11 @@ EXPORTED = [
     "dmffb_admp_create", "dmffb_destroy", "dmffb_last_error", "dmffb_admp_set_params",
     "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
     "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
+    "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters",
 ]
+
+KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
+                  "gather_field", "self_frames", "vector", "neighbors"]
 
 
 class AdmpDesc(ctypes.Structure):
@@ -98,6 +102,9 @@ def load():
     lib.dmffb_admp_build_neighbors.argtypes = [vp, vp, vp, vp]
     lib.dmffb_get_timings.argtypes = [vp, P(dbl), i32]
     lib.dmffb_set_timing.argtypes = [vp, i32]
+    lib.dmffb_set_profiling.argtypes = [vp, i32]
+    lib.dmffb_get_kernel_stats.argtypes = [vp, P(dbl), P(i64), i32]
+    lib.dmffb_get_counters.argtypes = [vp, P(i64), i32]
     for name in EXPORTED:
         if name not in ("dmffb_destroy", "dmffb_last_error"):
             getattr(lib, name).restype = ctypes.c_int

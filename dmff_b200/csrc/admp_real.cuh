@@ -457,4 +457,108 @@ __global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
     }
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Induced-dipole matrix-vector product for the CG solve, atomics-free: a full (both-direction)
+// CSR neighbour list, one warp per atom, FP32 pair tensors accumulated in FP64 registers.
+//   dE/dU_i += sum_j [udud1 I + (udud0 - udud1) z z^T] U_j      (pme.py:872-878)
+// CSR entries pack j in bits 0..27 and the scale index (nbond-1, wrapped) in bits 28..30.
+struct CsrArgs {
+    int n;
+    const int64_t* off;   // [n+1]
+    const int32_t* ent;   // packed (j, scale index)
+};
+
+__device__ __forceinline__ int scale_index(int nb) {
+    int sidx = nb - 1;
+    if (sidx < 0) sidx += 6;
+    return sidx < 0 ? 0 : (sidx > 5 ? 5 : sidx);
+}
+
+__global__ void k_csr_count(int64_t npairs, const int32_t* pairs, int n, int32_t* deg) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= npairs) return;
+    const int i = pairs[3 * r], j = pairs[3 * r + 1];
+    if (i < 0 || i >= j || j >= n) return;
+    atomicAdd(deg + i, 1);
+    atomicAdd(deg + j, 1);
+}
+
+__global__ void k_csr_fill(int64_t npairs, const int32_t* pairs, int n, const int64_t* off, int32_t* cursor,
+                           int32_t* ent) {
+    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= npairs) return;
+    const int i = pairs[3 * r], j = pairs[3 * r + 1];
+    if (i < 0 || i >= j || j >= n) return;
+    const int s = scale_index(pairs[3 * r + 2]);
+    const int ki = atomicAdd(cursor + i, 1);
+    const int kj = atomicAdd(cursor + j, 1);
+    ent[off[i] + ki] = j | (s << 28);
+    ent[off[j] + kj] = i | (s << 28);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_matvec_csr(PairArgs<T> a, CsrArgs c, double* out) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= c.n) return;
+    const int i = w;
+    const T D = T(DMFFB_DIELECTRIC);
+    BoxT<T> bx;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { bx.h[k] = (T)a.boxd.h[k]; bx.hinv[k] = (T)a.boxd.hinv[k]; }
+    const T xi = a.pos[4 * i], yi = a.pos[4 * i + 1], zi = a.pos[4 * i + 2];
+    const T thi = a.thole[i], psi = a.polsix[i];
+    const T kap = a.kappa;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    const int64_t beg = c.off[i], end = c.off[i + 1];
+    for (int64_t k = beg + lane; k < end; k += 32) {
+        const int e = c.ent[k];
+        const int j = e & 0x0FFFFFFF;
+        const int sidx = (e >> 28) & 7;
+        T dx = xi - a.pos[4 * j], dy = yi - a.pos[4 * j + 1], dz = zi - a.pos[4 * j + 2];
+        pbc_shift(bx, dx, dy, dz, (T*)nullptr);
+        const T r2 = dx * dx + dy * dy + dz * dz;
+        const T rinv = d_rsqrt(r2);
+        const T r = r2 * rinv;
+        const T ez0 = dx * rinv, ez1 = dy * rinv, ez2 = dz * rinv;
+        const T av = kap * r;
+        const T a2 = av * av;
+        const T X = T(DMFFB_TWO_OVER_SQRTPI) * d_exp(-a2);
+        const T t2 = av * X;
+        const T a3X = a2 * t2;
+        const T base = d_erfc(av) + t2 + T(2.0 / 3.0) * a3X;
+        const T pp = a.ps[sidx], dsv = a.dsc[sidx];
+        const T Ath = pp > T(0) ? T(5.0) : thi + a.thole[j];
+        T dmp = psi * a.polsix[j];
+        dmp = dmp < T(1e-8) ? T(1e-8) : dmp;
+        T u = r / dmp;
+        u = u < T(1e8) ? u : T(1e8);
+        const T au = Ath * u;
+        const T ev = au < T(50) ? d_exp(-au) : T(0);
+        const T Pc = T(1) + au + T(0.5) * au * au;
+        const T Pd0 = Pc + au * au * au * T(0.25);
+        const T bd0 = (dsv - T(1)) - dsv * ev * Pd0 + base;
+        const T bd1 = (dsv - T(1)) - dsv * ev * Pc + base;
+        const T r3 = rinv * rinv * rinv;
+        const T udud0 = T(-2.0 / 3.0) * D * r3 * (T(3) * bd0 + a3X);
+        const T udud1 = D * r3 * (bd1 - T(2.0 / 3.0) * a3X);
+        const double* U = a.U + 3 * j;
+        const T u0 = (T)U[0], u1 = (T)U[1], u2 = (T)U[2];
+        const T zu = ez0 * u0 + ez1 * u1 + ez2 * u2;
+        const T dd = (udud0 - udud1) * zu;
+        acc0 += (double)(udud1 * u0 + dd * ez0);
+        acc1 += (double)(udud1 * u1 + dd * ez1);
+        acc2 += (double)(udud1 * u2 + dd * ez2);
+    }
+    acc0 = warp_sum(acc0);
+    acc1 = warp_sum(acc1);
+    acc2 = warp_sum(acc2);
+    if (lane == 0) {
+        out[3 * i] = acc0;
+        out[3 * i + 1] = acc1;
+        out[3 * i + 2] = acc2;
+    }
+}
+
 }  // namespace dmffb

@@ -112,6 +112,7 @@ struct SpreadArgs {
     int lmax;           // 0: charge only, 1: up to dipole, 2: up to quadrupole
     MeshGeom g;
     T* grid;
+    int perm_mul;  // warps visit atoms in the order (w * perm_mul) mod n, gcd(perm_mul, n) = 1
 };
 
 template <typename T>
@@ -156,7 +157,9 @@ __global__ void __launch_bounds__(256) k_spread(SpreadArgs<T> a) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= a.n) return;
-    const int at = warp;
+    // concurrently running warps take atoms far apart in the box, which keeps them off the same
+    // mesh addresses (atoms are usually stored in spatial order)
+    const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
     int m0[3];
     T Mx[4][6], My[4][6], Mz[4][6];
     stencil_setup<T>(a.g, a.pos, at, m0, Mx, My, Mz);
@@ -370,8 +373,14 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs<T> a) {
             }
         }
     }
+    // reduce only the sums this mode uses (field: first derivatives; full: all 20)
+    if (maxo == 2) {
 #pragma unroll
-    for (int k = 0; k < 20; ++k) P[k] = warp_sum(P[k]);
+        for (int k = 1; k < 4; ++k) P[k] = warp_sum(P[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 20; ++k) P[k] = warp_sum(P[k]);
+    }
 
     double red[10];
 #pragma unroll

@@ -65,6 +65,12 @@ struct dmffb_engine {
     double* d_scal = nullptr;
     double *d_b = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_Ap = nullptr, *d_fr = nullptr;
     double* d_gQ = nullptr;
+    double* d_fmv = nullptr;  // CSR matvec output [3n]
+    int64_t* d_csr_off = nullptr;
+    int32_t *d_csr_ent = nullptr, *d_csr_deg = nullptr;
+    int64_t csr_cap = 0;
+    void* d_cub2 = nullptr;
+    size_t cub2_bytes = 0;
     void* d_grid = nullptr;
     void* d_cgrid = nullptr;
     double* d_bmod = nullptr;
@@ -85,9 +91,23 @@ struct dmffb_engine {
     bool timing = false;
     cudaEvent_t ev[8];
     double t_ms[6] = {0, 0, 0, 0, 0, 0};
+    // ---- per-kernel-class instrumentation (events around every launch when enabled)
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, int>> prof_marks;  // (class, event index of start)
+    double kstat_ms[16] = {0};
+    int64_t kstat_n[16] = {0};
+    int64_t n_launch = 0, n_fft = 0;
     // ---- last result book-keeping
     Box last_box;
     const double* cur_pos = nullptr;  // FP64 positions of the evaluation in flight
+    int perm_mul = 1;
+    // ---- CG iteration graph (two iterations per launch) and the side stream of the matvec
+    cudaStream_t s1 = nullptr, s2 = nullptr;  // engine work stream (capturable) and matvec side stream
+    cudaEvent_t e_fork = nullptr, e_join = nullptr, e_in = nullptr, e_out = nullptr;
+    cudaGraphExec_t cg_exec = nullptr;
+    std::vector<double> cg_key;
+    bool use_graphs = true;
 };
 
 namespace {
@@ -170,16 +190,64 @@ MeshGeom mesh_geom(const Box& b, const int K[3]) {
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// kernel classes for dmffb_get_kernel_stats
+enum { KC_PREP = 0, KC_PAIR_FULL, KC_PAIR_FIELD, KC_PAIR_MATVEC, KC_SPREAD, KC_FFT, KC_CONV, KC_GATHER_FULL,
+       KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_COUNT };
+
+inline void prof_begin(dmffb_engine* h, cudaStream_t s, int cls) {
+    if (!h->prof) return;
+    const size_t k = h->prof_marks.size() * 2;
+    while (h->ev_pool.size() < k + 2) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->ev_pool.push_back(e);
+    }
+    cudaEventRecord(h->ev_pool[k], s);
+    h->prof_marks.push_back({cls, (int)k});
+}
+inline void prof_end(dmffb_engine* h, cudaStream_t s) {
+    if (!h->prof) return;
+    cudaEventRecord(h->ev_pool[h->prof_marks.back().second + 1], s);
+}
+inline void prof_collect(dmffb_engine* h) {
+    if (!h->prof) return;
+    for (auto& m : h->prof_marks) {
+        float ms = 0.f;
+        cudaEventSynchronize(h->ev_pool[m.second + 1]);
+        cudaEventElapsedTime(&ms, h->ev_pool[m.second], h->ev_pool[m.second + 1]);
+        h->kstat_ms[m.first] += ms;
+        h->kstat_n[m.first] += 1;
+    }
+    h->prof_marks.clear();
+}
+// launch one of our kernels with accounting: LAUNCH(h, stream, class, kernel<<<...>>>(args))
+#define LAUNCH(H, S, CLS, ...)   \
+    do {                         \
+        prof_begin(H, S, CLS);   \
+        __VA_ARGS__;             \
+        prof_end(H, S);          \
+        (H)->n_launch++;         \
+    } while (0)
+#define FFTCALL(H, S, ...)        \
+    do {                          \
+        prof_begin(H, S, KC_FFT); \
+        CKFFT(__VA_ARGS__);       \
+        prof_end(H, S);           \
+        (H)->n_fft++;             \
+    } while (0)
+
 // ------------------------------------------------------------------ small vector kernels
 template <typename T>
-__global__ void k_field_combine(int n, const double* recip, const T* fT, const double* U, const double* Qg,
-                                const double* pol, double self1, int include_perm, double* out) {
+__global__ void k_field_combine(int n, const double* recip, const T* fT, const double* mv, const double* U,
+                                const double* Qg, const double* pol, double self1, int include_perm, double* out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= 3 * n) return;
     const int a = k / 3, c = k % 3;
     double p = pol[a];
     p = p < 1e-8 ? 1e-8 : p;
-    double v = (recip ? recip[k] : 0.0) + (double)fT[k];
+    double v = recip ? recip[k] : 0.0;
+    if (fT) v += (double)fT[k];
+    if (mv) v += mv[k];
     if (U) v += (DMFFB_DIELECTRIC / p + self1) * U[k];
     if (include_perm) {
         const int hidx = c == 0 ? 2 : (c == 1 ? 3 : 1);
@@ -216,7 +284,7 @@ __global__ void k_cg_init(int n, const double* b, const double* Ax, const double
 __global__ void k_cg_update(int n, const double* s, int slot, double* x, double* r, double* z, const double* p,
                             const double* Ap, const double* pol, double* rz_new, double* rr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const double alpha = s[slot] / s[2];
+    const double alpha = s[2] != 0.0 ? s[slot] / s[2] : 0.0;
     double v[1] = {0.0}, w[1] = {0.0};
     if (k < 3 * n) {
         double pp = pol[k / 3];
@@ -236,7 +304,7 @@ __global__ void k_cg_update(int n, const double* s, int slot, double* x, double*
 __global__ void k_cg_p(int n, const double* s, int slot_old, int slot_new, const double* z, double* p) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= 3 * n) return;
-    const double beta = s[slot_new] / s[slot_old];
+    const double beta = s[slot_old] != 0.0 ? s[slot_new] / s[slot_old] : 0.0;
     p[k] = z[k] + beta * p[k];
 }
 
@@ -312,13 +380,14 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     sa.lmax = lmax_eff(h);
     sa.g = g;
     sa.grid = (T*)h->d_grid;
-    k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa);
+    sa.perm_mul = h->perm_mul;
+    LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
     CKFFT(cufftSetStream(h->plan_f, s));
     CKFFT(cufftSetStream(h->plan_b, s));
     if (sizeof(T) == 4) {
-        CKFFT(cufftExecR2C(h->plan_f, (cufftReal*)h->d_grid, (cufftComplex*)h->d_cgrid));
+        FFTCALL(h, s, cufftExecR2C(h->plan_f, (cufftReal*)h->d_grid, (cufftComplex*)h->d_cgrid));
     } else {
-        CKFFT(cufftExecD2Z(h->plan_f, (cufftDoubleReal*)h->d_grid, (cufftDoubleComplex*)h->d_cgrid));
+        FFTCALL(h, s, cufftExecD2Z(h->plan_f, (cufftDoubleReal*)h->d_grid, (cufftDoubleComplex*)h->d_cgrid));
     }
     ConvArgs<T> ca;
     for (int k = 0; k < 3; ++k) ca.K[k] = h->K[k];
@@ -333,11 +402,11 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     ca.scal = h->d_scal + S_RECIP;
     ca.want_energy = (mode == GATHER_FULL) ? 1 : 0;
     const int64_t nk = (int64_t)h->K[0] * h->K[1] * ca.Kh;
-    k_conv<T><<<nblk(nk, 256), 256, 0, s>>>(ca);
+    LAUNCH(h, s, KC_CONV, k_conv<T><<<nblk(nk, 256), 256, 0, s>>>(ca));
     if (sizeof(T) == 4) {
-        CKFFT(cufftExecC2R(h->plan_b, (cufftComplex*)h->d_cgrid, (cufftReal*)h->d_grid));
+        FFTCALL(h, s, cufftExecC2R(h->plan_b, (cufftComplex*)h->d_cgrid, (cufftReal*)h->d_grid));
     } else {
-        CKFFT(cufftExecZ2D(h->plan_b, (cufftDoubleComplex*)h->d_cgrid, (cufftDoubleReal*)h->d_grid));
+        FFTCALL(h, s, cufftExecZ2D(h->plan_b, (cufftDoubleComplex*)h->d_cgrid, (cufftDoubleReal*)h->d_grid));
     }
     GatherArgs<T> ga;
     ga.n = h->n;
@@ -358,7 +427,38 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     ga.scal = h->d_scal + S_GATHER;
     ga.want_box = 1;
     ga.mode = mode;
-    k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga);
+    LAUNCH(h, s, (mode == GATHER_FULL ? KC_GATHER_FULL : KC_GATHER_FIELD), k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga));
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
+// dE/dU at U (include_perm) or its linear part A U (!include_perm), into out
+// full both-direction CSR of the half-list rows (for the atomics-free CG matvec)
+int build_csr(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npairs) {
+    const int n = h->n;
+    int st;
+    if (!h->d_csr_off) {
+        if ((st = dalloc(h, &h->d_csr_off, (n + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_csr_deg, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_fmv, 3 * n * sizeof(double)))) return st;
+        size_t need = 0;
+        cub::DeviceScan::InclusiveSum(nullptr, need, (int32_t*)nullptr, (int64_t*)nullptr, n);
+        h->cub2_bytes = need;
+        if ((st = dalloc(h, &h->d_cub2, need))) return st;
+    }
+    if (2 * npairs > h->csr_cap) {
+        if (h->d_csr_ent) cudaFree(h->d_csr_ent);
+        h->csr_cap = 2 * npairs + 1024;
+        if ((st = dalloc(h, &h->d_csr_ent, h->csr_cap * sizeof(int32_t)))) return st;
+    }
+    CK(cudaMemsetAsync(h->d_csr_deg, 0, n * sizeof(int32_t), s));
+    LAUNCH(h, s, KC_VEC, k_csr_count<<<nblk(npairs, 256), 256, 0, s>>>(npairs, pairs, n, h->d_csr_deg));
+    CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
+    size_t tb = h->cub2_bytes;
+    LAUNCH(h, s, KC_VEC, cub::DeviceScan::InclusiveSum(h->d_cub2, tb, h->d_csr_deg, h->d_csr_off + 1, n, s));
+    CK(cudaMemsetAsync(h->d_csr_deg, 0, n * sizeof(int32_t), s));
+    LAUNCH(h, s, KC_VEC, k_csr_fill<<<nblk(npairs, 256), 256, 0, s>>>(npairs, pairs, n, h->d_csr_off, h->d_csr_deg,
+                                                                      h->d_csr_ent));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
@@ -367,15 +467,27 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
 template <typename T>
 int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
                int64_t npairs, const double* U, bool include_perm, double* out) {
-    CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
-    const unsigned nb = nblk(npairs, 128);
+    if (include_perm) CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
     if (include_perm && npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
-        k_admp_pair<T, true, PAIR_FIELD><<<nb, 128, 0, s>>>(a);
+        LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, s>>>(a));
     }
-    if (U && npairs > 0) {
+    // the real-space matvec runs on a side stream, overlapping the reciprocal pass
+    const bool fork = U && h->s2 && !h->prof;
+    if (U) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, U);
-        k_admp_pair<T, true, PAIR_MATVEC><<<nb, 128, 0, s>>>(a);
+        CsrArgs c;
+        c.n = h->n;
+        c.off = h->d_csr_off;
+        c.ent = h->d_csr_ent;
+        cudaStream_t sm = s;
+        if (fork) {
+            CK(cudaEventRecord(h->e_fork, s));
+            CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
+            sm = h->s2;
+        }
+        LAUNCH(h, sm, KC_PAIR_MATVEC, k_matvec_csr<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, sm>>>(a, c, h->d_fmv));
+        if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
     const double* recip = nullptr;
     if (h->lpme && h->have_plans) {
@@ -383,10 +495,12 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
         if (st) return st;
         recip = h->d_fr;
     }
+    if (fork) CK(cudaStreamWaitEvent(s, h->e_join, 0));
     const double k = h->kappa;
     const double self1 = h->lpme ? -2.0 * DMFFB_DIELECTRIC * (k / 1.7724538509055159) * 2.0 * k * k / 3.0 : 0.0;
-    k_field_combine<T><<<nblk(3 * h->n, 256), 256, 0, s>>>(h->n, recip, (const T*)h->d_fieldT, U, h->d_Qg, h->d_pol,
-                                                           self1, include_perm ? 1 : 0, out);
+    LAUNCH(h, s, KC_VEC, k_field_combine<T><<<nblk(3 * h->n, 256), 256, 0, s>>>(
+                             h->n, recip, include_perm ? (const T*)h->d_fieldT : nullptr, U ? h->d_fmv : nullptr, U,
+                             h->d_Qg, h->d_pol, self1, include_perm ? 1 : 0, out));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
@@ -398,6 +512,7 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     const unsigned nb3 = nblk(3 * n, 256);
     double* sc = h->d_scal + S_CG;
     int st;
+    if ((st = build_csr(h, s, pairs, npairs))) return st;
     if (h->solver == DMFFB_SOLVER_REFERENCE) {
         int it = 0;
         bool conv = false;
@@ -406,7 +521,7 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
             if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, h->d_b))) return st;
             if (h->steps_pol <= 0) {
                 CK(cudaMemsetAsync(sc + 8, 0, sizeof(double), s));
-                k_absmax<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_pol, 0.001, (unsigned long long*)(sc + 8));
+                LAUNCH(h, s, KC_VEC, k_absmax<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_pol, 0.001, (unsigned long long*)(sc + 8)));
                 CK(cudaMemcpyAsync(h->h_scal, sc + 8, sizeof(double), cudaMemcpyDeviceToHost, s));
                 CK(cudaStreamSynchronize(s));
                 if (h->h_scal[0] < h->cg_tol) {
@@ -414,7 +529,7 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
                     break;
                 }
             }
-            k_ref_step<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_pol, U, nullptr);
+            LAUNCH(h, s, KC_VEC, k_ref_step<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_pol, U, nullptr));
         }
         if (h->steps_pol > 0) {
             conv = true;
@@ -428,15 +543,49 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     // CG on A U = -b
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b))) return st;
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
-    k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_Ap, h->d_pol, h->d_r, h->d_z, h->d_p);
+    LAUNCH(h, s, KC_VEC, k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_Ap, h->d_pol, h->d_r, h->d_z, h->d_p));
     CK(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
-    k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_r, h->d_z, h->d_r, h->d_r, sc + 0, sc + 3);
-    k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_b, h->d_b, nullptr, nullptr, sc + 4, nullptr);
+    LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_r, h->d_z, h->d_r, h->d_r, sc + 0, sc + 3));
+    LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_b, h->d_b, nullptr, nullptr, sc + 4, nullptr));
     int it = 0;
     bool conv = false;
     double rms = 0.0, rms_b = 0.0;
-    int slot = 0;
-    for (it = 0; it <= h->max_iter; ++it) {
+    // one CG iteration; slot = parity of the r.z scalar it reads
+    auto iteration = [&](int slot) -> int {
+        int st2;
+        if ((st2 = field_eval<T>(h, s, pos, bx, pairs, npairs, h->d_p, false, h->d_Ap))) return st2;
+        CK(cudaMemsetAsync(sc + 2, 0, 2 * sizeof(double), s));  // pAp, rr
+        CK(cudaMemsetAsync(sc + (1 - slot), 0, sizeof(double), s));
+        LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_p, h->d_Ap, nullptr, nullptr, sc + 2, nullptr));
+        LAUNCH(h, s, KC_VEC, k_cg_update<<<nb3, 256, 0, s>>>(n, sc, slot, U, h->d_r, h->d_z, h->d_p, h->d_Ap,
+                                                           h->d_pol, sc + (1 - slot), sc + 3));
+        LAUNCH(h, s, KC_VEC, k_cg_p<<<nb3, 256, 0, s>>>(n, sc, slot, 1 - slot, h->d_z, h->d_p));
+        return DMFFB_OK;
+    };
+    // two iterations (slot 0 then 1) are captured once into a CUDA graph and replayed; the graph
+    // is recaptured when any pointer or the box it bakes in changes
+    const bool graphs = h->use_graphs && !h->prof;
+    if (graphs) {
+        std::vector<double> key = {(double)(uintptr_t)pos, (double)(uintptr_t)pairs, (double)npairs,
+                                   (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T)};
+        for (int k = 0; k < 9; ++k) key.push_back(bx.h[k]);
+        if (!h->cg_exec || key != h->cg_key) {
+            if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            int st0 = iteration(0);
+            int st1 = st0 ? st0 : iteration(1);
+            cudaError_t ce = cudaStreamEndCapture(s, &g);
+            if (st1) return st1;
+            if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&h->cg_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+            h->cg_key = key;
+        }
+    }
+    const int check_every = 4;  // host reads the residual every few iterations (no per-iteration sync)
+    while (true) {
         CK(cudaMemcpyAsync(h->h_scal, sc + 3, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         rms = sqrt(h->h_scal[0] / (3.0 * n));
@@ -447,15 +596,18 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
             conv = true;
             break;
         }
-        if (it == h->max_iter) break;
-        if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, h->d_p, false, h->d_Ap))) return st;
-        CK(cudaMemsetAsync(sc + 2, 0, 2 * sizeof(double), s));  // pAp, rr
-        CK(cudaMemsetAsync(sc + (1 - slot), 0, sizeof(double), s));
-        k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_p, h->d_Ap, nullptr, nullptr, sc + 2, nullptr);
-        k_cg_update<<<nb3, 256, 0, s>>>(n, sc, slot, U, h->d_r, h->d_z, h->d_p, h->d_Ap, h->d_pol, sc + (1 - slot),
-                                        sc + 3);
-        k_cg_p<<<nb3, 256, 0, s>>>(n, sc, slot, 1 - slot, h->d_z, h->d_p);
-        slot = 1 - slot;
+        if (it >= h->max_iter) break;
+        for (int k = 0; k < check_every; k += 2) {
+            if (graphs) {
+                CK(cudaGraphLaunch(h->cg_exec, s));
+                h->n_launch += 2 * 8;
+                h->n_fft += 4;
+            } else {
+                if ((st = iteration(0))) return st;
+                if ((st = iteration(1))) return st;
+            }
+            it += 2;
+        }
     }
     res->n_iter = it;
     res->converged = conv ? 1 : 0;
@@ -503,7 +655,7 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     pa.posT = (T*)h->d_posT;
     pa.QgT = (T*)h->d_QgT;
     pa.Qg = h->d_Qg;
-    k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa);
+    LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
     CK(cudaGetLastError());
     if (h->timing) CK(cudaEventRecord(h->ev[1], s));
     if (h->lpol) {
@@ -514,8 +666,8 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     if (h->timing) CK(cudaEventRecord(h->ev[2], s));
     if (npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, h->lpol ? U : nullptr);
-        if (h->lpol) k_admp_pair<T, true, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a);
-        else k_admp_pair<T, false, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a);
+        if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a));
+        else LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a));
         CK(cudaGetLastError());
     }
     if (h->timing) CK(cudaEventRecord(h->ev[3], s));
@@ -537,12 +689,13 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     sa.scal = h->d_scal + S_SELF;
     sa.tau_out = nullptr;
     if (h->lmax == 0) sa.f.axis_idx = nullptr;
-    k_self_frames<T><<<nblk(n, 128), 128, 0, s>>>(sa);
-    if (forces) k_finalize_forces<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_gpair, h->d_grad, forces);
+    LAUNCH(h, s, KC_SELF, k_self_frames<T><<<nblk(n, 128), 128, 0, s>>>(sa));
+    if (forces) LAUNCH(h, s, KC_VEC, k_finalize_forces<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_gpair, h->d_grad, forces));
     CK(cudaGetLastError());
     if (h->timing) CK(cudaEventRecord(h->ev[5], s));
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    prof_collect(h);
     const double* sc = h->h_scal;
     res->e_real = sc[S_EREAL];
     res->e_recip = sc[S_RECIP];
@@ -619,6 +772,13 @@ int dmffb_admp_create(const dmffb_admp_desc* d, dmffb_engine** out) {
         h->dsc[k] = d->dscales[k];
     }
     h->solver = d->solver;
+    {  // a multiplier coprime with n near n / 148 (one stride per SM) for the spread order
+        auto gcd = [](int64_t a, int64_t b) { while (b) { int64_t t = a % b; a = b; b = t; } return a; };
+        int64_t m = std::max<int64_t>(1, d->n_atoms / 148) | 1;
+        while (gcd(m, d->n_atoms) != 1) m += 2;
+        h->perm_mul = (int)(m % std::max(1, d->n_atoms));
+        if (h->perm_mul == 0) h->perm_mul = 1;
+    }
     h->cg_tol = d->cg_tol > 0 ? d->cg_tol : 1e-6;
     h->max_iter = d->max_iter > 0 ? d->max_iter : 500;
     h->steps_pol = d->steps_pol;
@@ -727,6 +887,12 @@ int dmffb_admp_create(const dmffb_admp_desc* d, dmffb_engine** out) {
         h->have_plans = true;
     }
     for (int k = 0; k < 8; ++k) cudaEventCreate(&h->ev[k]);
+    cudaStreamCreateWithFlags(&h->s1, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&h->e_in, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->e_out, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->e_fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->e_join, cudaEventDisableTiming);
 #undef AL
     cudaError_t e = cudaDeviceSynchronize();
     *out = h;
@@ -739,7 +905,7 @@ void dmffb_destroy(dmffb_engine* h) {
     void* ptrs[] = {h->d_axis_type, h->d_axis_idx, h->d_cov_ptr, h->d_cov_j, h->d_cov_nb, h->d_Qloc, h->d_pol,
                     h->d_thole, h->d_polsix, h->d_pos, h->d_U, h->d_forces, h->d_posT, h->d_Qg, h->d_QgT,
                     h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
-                    h->d_Ap, h->d_fr, h->d_gQ, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
+                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
                     h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
                     h->d_cub};
     for (void* p : ptrs)
@@ -750,6 +916,14 @@ void dmffb_destroy(dmffb_engine* h) {
         cufftDestroy(h->plan_b);
     }
     for (int k = 0; k < 8; ++k) cudaEventDestroy(h->ev[k]);
+    for (auto e : h->ev_pool) cudaEventDestroy(e);
+    if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
+    if (h->s2) cudaStreamDestroy(h->s2);
+    if (h->s1) cudaStreamDestroy(h->s1);
+    if (h->e_in) cudaEventDestroy(h->e_in);
+    if (h->e_out) cudaEventDestroy(h->e_out);
+    if (h->e_fork) cudaEventDestroy(h->e_fork);
+    if (h->e_join) cudaEventDestroy(h->e_join);
     delete h;
 }
 
@@ -779,9 +953,17 @@ int dmffb_admp_compute(dmffb_engine* h, void* stream, const double* pos, const d
                        int64_t npairs, double* U_inout, double* forces_out, dmffb_admp_result* result) {
     if (!h) return DMFFB_BAD_ARG;
     if (pairs && npairs < 0) return fail(h, DMFFB_BAD_ARG, "negative npairs");
-    cudaStream_t s = (cudaStream_t)stream;
-    if (h->prec == DMFFB_FP32) return compute_impl<float>(h, s, pos, box, pairs, npairs, U_inout, forces_out, result);
-    return compute_impl<double>(h, s, pos, box, pairs, npairs, U_inout, forces_out, result);
+    // the evaluation runs on the engine's own stream (capturable into CUDA graphs), ordered
+    // after the caller's prior work on `stream` and before the caller's later work
+    cudaStream_t caller = (cudaStream_t)stream;
+    CK(cudaEventRecord(h->e_in, caller));
+    CK(cudaStreamWaitEvent(h->s1, h->e_in, 0));
+    int st = h->prec == DMFFB_FP32
+                 ? compute_impl<float>(h, h->s1, pos, box, pairs, npairs, U_inout, forces_out, result)
+                 : compute_impl<double>(h, h->s1, pos, box, pairs, npairs, U_inout, forces_out, result);
+    cudaEventRecord(h->e_out, h->s1);
+    cudaStreamWaitEvent(caller, h->e_out, 0);
+    return st;
 }
 
 int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* box, const int32_t* pairs,
@@ -798,6 +980,10 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
     if (h->lpol) {
         if (U_inout) CK(cudaMemcpyAsync(h->d_U, U_inout, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
         else CK(cudaMemsetAsync(h->d_U, 0, 3 * n * sizeof(double), s));
+    }
+    if (!pairs) {  // host callers hold no device pair list: rebuild for these positions
+        int sb = dmffb_admp_build_neighbors(h, (void*)s, h->d_pos, box);
+        if (sb) return sb;
     }
     int st = dmffb_admp_compute(h, s, h->d_pos, box, dp, npairs, h->lpol ? h->d_U : nullptr, h->d_forces, result);
     if (dp) cudaFree(dp);
@@ -837,7 +1023,7 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
         pa.posT = (T*)h->d_posT;
         pa.QgT = (T*)h->d_QgT;
         pa.Qg = h->d_Qg;
-        k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa);
+        LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
         int st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out);
         if (st) return st;
         CK(cudaStreamSynchronize(s));
@@ -917,20 +1103,20 @@ int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, cons
     if (cells) {
         CK(cudaMemsetAsync(h->d_cell_count, 0, (ncell + 1) * sizeof(int32_t), s));
         CK(cudaMemsetAsync(h->d_cell_cursor, 0, (ncell + 1) * sizeof(int32_t), s));
-        k_cell_count<<<nblk(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], h->d_atom_cell, h->d_cell_count);
+        LAUNCH(h, s, KC_NBLIST, k_cell_count<<<nblk(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], h->d_atom_cell, h->d_cell_count));
         size_t tb = h->cub_bytes;
-        cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_cell_count, h->d_cell_start, ncell + 1, s);
-        k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(n, h->d_atom_cell, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms);
+        LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_cell_count, h->d_cell_start, ncell + 1, s));
+        LAUNCH(h, s, KC_NBLIST, k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(n, h->d_atom_cell, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms));
         a.cell_start = h->d_cell_start;
         a.cell_atoms = h->d_cell_atoms;
-        k_pairs<0><<<nblk(n, 128), 128, 0, s>>>(a);
+        LAUNCH(h, s, KC_NBLIST, k_pairs_warp<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(a));
     } else {
-        k_pairs_all<0><<<nblk(n, 128), 128, 0, s>>>(a);
+        LAUNCH(h, s, KC_NBLIST, k_pairs_all<0><<<nblk(n, 128), 128, 0, s>>>(a));
     }
     {
         size_t tb = h->cub_bytes;
         CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
-        cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount, h->d_poff + 1, n, s);
+        LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount, h->d_poff + 1, n, s));
     }
     int64_t total = 0;
     CK(cudaMemcpyAsync(&total, h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -940,10 +1126,11 @@ int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, cons
         h->err = "neighbour capacity too small";
         return DMFFB_NEIGHBOR_OVERFLOW;
     }
-    if (cells) k_pairs<1><<<nblk(n, 128), 128, 0, s>>>(a);
-    else k_pairs_all<1><<<nblk(n, 128), 128, 0, s>>>(a);
+    if (cells) LAUNCH(h, s, KC_NBLIST, k_pairs_warp<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(a));
+    else LAUNCH(h, s, KC_NBLIST, k_pairs_all<1><<<nblk(n, 128), 128, 0, s>>>(a));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
+    prof_collect(h);
     return DMFFB_OK;
 }
 
@@ -966,6 +1153,29 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
 int dmffb_get_timings(const dmffb_engine* h, double* ms_out, int32_t n) {
     if (!h || !ms_out) return DMFFB_BAD_ARG;
     for (int k = 0; k < n && k < 6; ++k) ms_out[k] = h->t_ms[k];
+    return DMFFB_OK;
+}
+
+int dmffb_set_profiling(dmffb_engine* h, int32_t enabled) {
+    if (!h) return DMFFB_BAD_ARG;
+    h->prof = enabled != 0;
+    for (int k = 0; k < 16; ++k) { h->kstat_ms[k] = 0; h->kstat_n[k] = 0; }
+    return DMFFB_OK;
+}
+
+int dmffb_get_kernel_stats(const dmffb_engine* h, double* ms_out, int64_t* launches_out, int32_t n) {
+    if (!h) return DMFFB_BAD_ARG;
+    for (int k = 0; k < n && k < KC_COUNT; ++k) {
+        if (ms_out) ms_out[k] = h->kstat_ms[k];
+        if (launches_out) launches_out[k] = h->kstat_n[k];
+    }
+    return DMFFB_OK;
+}
+
+int dmffb_get_counters(const dmffb_engine* h, int64_t* out, int32_t n) {
+    if (!h || !out) return DMFFB_BAD_ARG;
+    if (n > 0) out[0] = h->n_launch;
+    if (n > 1) out[1] = h->n_fft;
     return DMFFB_OK;
 }
 

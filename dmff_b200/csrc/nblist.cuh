@@ -151,4 +151,82 @@ __global__ void __launch_bounds__(128) k_pairs_all(NbArgs a) {
     if (PASS == 0) a.count[i] = cnt;
 }
 
+
+// Warp-per-atom variant: lanes stride over the candidates of each of the 27 cells; a FP32
+// distance decides every candidate farther than 1e-3 A from the cutoff (and away from a
+// half-box image ambiguity), the exact FP64 test decides the rest, so the pair set is the one
+// of within_rc.  Output order: ballot prefix within each chunk keeps rows sorted by i.
+template <int PASS>
+__global__ void __launch_bounds__(256) k_pairs_warp(NbArgs a) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= a.n) return;
+    const double* pi = a.pos + 3 * i;
+    const double pix = pi[0], piy = pi[1], piz = pi[2];
+    float hf[9], hif[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { hf[k] = (float)a.box.h[k]; hif[k] = (float)a.box.hinv[k]; }
+    const float rlo = (float)(a.rc - 1e-3), rhi = (float)(a.rc + 1e-3);
+    const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
+    int c3[3];
+    cell_of(a.box, a.nc, pi, c3);
+    int64_t out = (PASS == 1) ? a.offset[i] : 0;
+    int cnt = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
+                const int c = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+                const int cs = a.cell_start[c], ce = a.cell_start[c + 1];
+                for (int base = cs; base < ce; base += 32) {
+                    const int k = base + lane;
+                    bool keep = false;
+                    int j = -1;
+                    if (k < ce) {
+                        j = a.cell_atoms[k];
+                        if (j > i) {
+                            const double* pj = a.pos + 3 * j;
+                            const float d0 = (float)(pj[0] - pix), d1 = (float)(pj[1] - piy), d2 = (float)(pj[2] - piz);
+                            bool amb = false;
+                            float sf[3];
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) {
+                                float t = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
+                                float nn = floorf(t + 0.5f);
+                                sf[q] = t - nn;
+                                amb |= fabsf(sf[q]) > 0.4999f;
+                            }
+                            const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
+                            const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
+                            const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
+                            const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
+                            if (!amb && r2 < rlo2) keep = true;
+                            else if (!amb && r2 > rhi2) keep = false;
+                            else keep = within_rc(a.box, pi, pj, a.rc);
+                        }
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (PASS == 1) {
+                        if (keep) {
+                            const int64_t slot = out + __popc(m & lt);
+                            if (slot < a.cap) {
+                                a.pairs[3 * slot] = i;
+                                a.pairs[3 * slot + 1] = j;
+                                a.pairs[3 * slot + 2] = lookup_nbond(a, i, j);
+                            }
+                        }
+                        out += __popc(m);
+                    } else {
+                        cnt += __popc(m);
+                    }
+                }
+            }
+        }
+    }
+    if (PASS == 0 && lane == 0) a.count[i] = cnt;
+}
+
 }  // namespace dmffb

@@ -200,6 +200,22 @@ class AdmpEngine:
     def set_timing(self, on=True):
         self.lib.dmffb_set_timing(self.h, int(on))
 
+    def set_profiling(self, on=True):
+        self.lib.dmffb_set_profiling(self.h, int(on))
+
+    def kernel_stats(self):
+        """{class: (total ms, launches)} accumulated while profiling was on."""
+        n = len(L.KERNEL_CLASSES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        self.lib.dmffb_get_kernel_stats(self.h, ms, cnt, n)
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(L.KERNEL_CLASSES)}
+
+    def counters(self):
+        out = (ctypes.c_int64 * 2)()
+        self.lib.dmffb_get_counters(self.h, out, 2)
+        return {"launches": out[0], "fft_execs": out[1]}
+
     def timings(self):
         arr = (ctypes.c_double * 6)()
         self.lib.dmffb_get_timings(self.h, arr, 6)
