@@ -390,7 +390,12 @@ __device__ __forceinline__ void pair_row(const PairArgs<T>& a, int i, int j, int
 // One thread per pair row.  Rows with a topological scale (nbond != 0: excluded / scaled
 // intramolecular pairs, which carry the large Ewald corrections that cancel the self energy)
 // are evaluated in FP64 even in the FP32 instantiation.
-template <typename T, bool POL, int MODE>
+enum { ROWS_ALL = 0, ROWS_UNSCALED = 1, ROWS_SCALED = 2 };
+
+// ROWS selects which rows this launch evaluates: all of them, only nbond == 0 rows (FP32
+// arithmetic) or only nbond != 0 rows (always FP64); the FP32 engine launches the last two so
+// that no warp mixes the two arithmetic paths.
+template <typename T, bool POL, int MODE, int ROWS = ROWS_ALL>
 __global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
     const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     int i = -1, j = -1, nb = 0;
@@ -399,7 +404,8 @@ __global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
         j = a.pairs[3 * row + 1];
         nb = a.pairs[3 * row + 2];
     }
-    const bool valid = (row < a.npairs) && i >= 0 && i < j && j < a.n;
+    const bool valid = (row < a.npairs) && i >= 0 && i < j && j < a.n &&
+                       (ROWS == ROWS_ALL || (ROWS == ROWS_UNSCALED) == (nb == 0));
     const int key = valid ? i : -1;
 
     T oi[6], oj[6];  // FULL: grad(3) + torque(3); FIELD/MATVEC: field(3)
@@ -429,10 +435,11 @@ __global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
     const int nout = (MODE == PAIR_FULL) ? 6 : 3;
     T* outp = (MODE == PAIR_FULL) ? a.grad : a.field;
     const bool head = seg_head(key);
+    const int run = seg_run_id(key);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
         if (k >= nout) break;
-        T s = seg_sum(oi[k], key);
+        T s = seg_sum(oi[k], run);
         if (head && key >= 0) {
             T* dst = (k < 3) ? (outp + 3 * key + k) : (a.torque + 3 * key + (k - 3));
             atomicAdd(dst, s);
@@ -550,6 +557,99 @@ __global__ void __launch_bounds__(256) k_matvec_csr(PairArgs<T> a, CsrArgs c, do
         acc0 += (double)(udud1 * u0 + dd * ez0);
         acc1 += (double)(udud1 * u1 + dd * ez1);
         acc2 += (double)(udud1 * u2 + dd * ez2);
+    }
+    acc0 = warp_sum(acc0);
+    acc1 = warp_sum(acc1);
+    acc2 = warp_sum(acc2);
+    if (lane == 0) {
+        out[3 * i] = acc0;
+        out[3 * i + 1] = acc1;
+        out[3 * i + 2] = acc2;
+    }
+}
+
+
+// Matvec split in two: the pair tensors [udud1, udud0 - udud1, z] of every CSR entry are fixed
+// during one dipole solve, so they are evaluated once (k_matvec_coef) and each CG iteration only
+// streams them (k_matvec_apply).
+template <typename T>
+struct MvCoef {
+    T c[4];  // udud1, udud0 - udud1, z_x, z_y
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_matvec_coef(PairArgs<T> a, CsrArgs c, MvCoef<T>* coef, T* coefz) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= c.n) return;
+    const int i = w;
+    const T D = T(DMFFB_DIELECTRIC);
+    BoxT<T> bx;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { bx.h[k] = (T)a.boxd.h[k]; bx.hinv[k] = (T)a.boxd.hinv[k]; }
+    const T xi = a.pos[4 * i], yi = a.pos[4 * i + 1], zi = a.pos[4 * i + 2];
+    const T thi = a.thole[i], psi = a.polsix[i];
+    const T kap = a.kappa;
+    const int64_t beg = c.off[i], end = c.off[i + 1];
+    for (int64_t k = beg + lane; k < end; k += 32) {
+        const int e = c.ent[k];
+        const int j = e & 0x0FFFFFFF;
+        const int sidx = (e >> 28) & 7;
+        T dx = xi - a.pos[4 * j], dy = yi - a.pos[4 * j + 1], dz = zi - a.pos[4 * j + 2];
+        pbc_shift(bx, dx, dy, dz, (T*)nullptr);
+        const T r2 = dx * dx + dy * dy + dz * dz;
+        const T rinv = d_rsqrt(r2);
+        const T r = r2 * rinv;
+        const T av = kap * r;
+        const T a2 = av * av;
+        const T X = T(DMFFB_TWO_OVER_SQRTPI) * d_exp(-a2);
+        const T t2 = av * X;
+        const T a3X = a2 * t2;
+        const T base = d_erfc(av) + t2 + T(2.0 / 3.0) * a3X;
+        const T pp = a.ps[sidx], dsv = a.dsc[sidx];
+        const T Ath = pp > T(0) ? T(5.0) : thi + a.thole[j];
+        T dmp = psi * a.polsix[j];
+        dmp = dmp < T(1e-8) ? T(1e-8) : dmp;
+        T u = r / dmp;
+        u = u < T(1e8) ? u : T(1e8);
+        const T au = Ath * u;
+        const T ev = au < T(50) ? d_exp(-au) : T(0);
+        const T Pc = T(1) + au + T(0.5) * au * au;
+        const T Pd0 = Pc + au * au * au * T(0.25);
+        const T bd0 = (dsv - T(1)) - dsv * ev * Pd0 + base;
+        const T bd1 = (dsv - T(1)) - dsv * ev * Pc + base;
+        const T r3 = rinv * rinv * rinv;
+        const T udud0 = T(-2.0 / 3.0) * D * r3 * (T(3) * bd0 + a3X);
+        const T udud1 = D * r3 * (bd1 - T(2.0 / 3.0) * a3X);
+        MvCoef<T> cf;
+        cf.c[0] = udud1;
+        cf.c[1] = udud0 - udud1;
+        cf.c[2] = dx * rinv;
+        cf.c[3] = dy * rinv;
+        coef[k] = cf;
+        coefz[k] = dz * rinv;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_matvec_apply(CsrArgs c, const MvCoef<T>* coef, const T* coefz,
+                                                      const double* U, double* out) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= c.n) return;
+    const int i = w;
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+    const int64_t beg = c.off[i], end = c.off[i + 1];
+    for (int64_t k = beg + lane; k < end; k += 32) {
+        const int j = c.ent[k] & 0x0FFFFFFF;
+        const MvCoef<T> cf = coef[k];
+        const T ez = coefz[k];
+        const double* Uj = U + 3 * j;
+        const T u0 = (T)Uj[0], u1 = (T)Uj[1], u2 = (T)Uj[2];
+        const T dd = cf.c[1] * (cf.c[2] * u0 + cf.c[3] * u1 + ez * u2);
+        acc0 += (double)(cf.c[0] * u0 + dd * cf.c[2]);
+        acc1 += (double)(cf.c[0] * u1 + dd * cf.c[3]);
+        acc2 += (double)(cf.c[0] * u2 + dd * ez);
     }
     acc0 = warp_sum(acc0);
     acc1 = warp_sum(acc1);

@@ -496,4 +496,115 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs<T> a) {
     if (a.mode == GATHER_FULL) block_reduce_add<10>(red, a.scal);
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Lean kernels for the CG loop, where only induced dipoles are spread and only the first
+// derivatives of the convolved mesh are gathered: value + first-derivative splines, 3 mesh
+// coefficients, 3 sums; small register footprint for occupancy.
+template <typename T>
+__device__ __forceinline__ void bspline6_01(T w, T M0[6], T M1[6]) {
+    T m2[2] = {w, T(1) - w};
+    T m3[3], m4[4], m5[5];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        m3[j] = ((w + T(j)) * (j < 2 ? m2[j] : T(0)) + (T(3) - w - T(j)) * (j > 0 ? m2[j - 1] : T(0))) * T(0.5);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        m4[j] = ((w + T(j)) * (j < 3 ? m3[j] : T(0)) + (T(4) - w - T(j)) * (j > 0 ? m3[j - 1] : T(0))) * T(1.0 / 3.0);
+#pragma unroll
+    for (int j = 0; j < 5; ++j)
+        m5[j] = ((w + T(j)) * (j < 4 ? m4[j] : T(0)) + (T(5) - w - T(j)) * (j > 0 ? m4[j - 1] : T(0))) * T(0.25);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const T a = j < 5 ? m5[j] : T(0), b = j > 0 ? m5[j - 1] : T(0);
+        M0[j] = ((w + T(j)) * a + (T(6) - w - T(j)) * b) * T(0.2);
+        M1[j] = a - b;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void stencil01(const MeshGeom& g, const double* pos, int at, int m0[3], T Mx[2][6],
+                                          T My[2][6], T Mz[2][6]) {
+    const double R0 = pos[3 * at], R1 = pos[3 * at + 1], R2 = pos[3 * at + 2];
+    T (*Ms[3])[6] = {Mx, My, Mz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double x = g.NA[3 * d] * R0 + g.NA[3 * d + 1] * R1 + g.NA[3 * d + 2] * R2;
+        const double c = ceil(x);
+        m0[d] = (int)c;
+        bspline6_01<T>((T)(c - x), Ms[d][0], Ms[d][1]);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_spread_dip(SpreadArgs<T> a) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.n) return;
+    const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
+    int m0[3];
+    T Mx[2][6], My[2][6], Mz[2][6];
+    stencil01<T>(a.g, a.pos, at, m0, Mx, My, Mz);
+    const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
+    const double* B = a.g.B;
+    const T c1 = -(T(B[0]) * mu0 + T(B[1]) * mu1 + T(B[2]) * mu2);
+    const T c2 = -(T(B[3]) * mu0 + T(B[4]) * mu1 + T(B[5]) * mu2);
+    const T c3 = -(T(B[6]) * mu0 + T(B[7]) * mu1 + T(B[8]) * mu2);
+    const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
+    for (int L = lane; L < 36; L += 32) {
+        const int ix = L / 6, iy = L % 6;
+        const T s0 = c1 * Mx[1][ix] * My[0][iy] + c2 * Mx[0][ix] * My[1][iy];
+        const T s1 = c3 * Mx[0][ix] * My[0][iy];
+        const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
+        T* line = a.grid + ((size_t)gx * K1 + gy) * K2;
+        int gz = wrapi(m0[2] - 3, K2);
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+            atomicAdd(line + gz, s0 * Mz[0][t] + s1 * Mz[1][t]);
+            gz = (gz + 1 == K2) ? 0 : gz + 1;
+        }
+    }
+}
+
+// dE/dmu (Cartesian) of every site from the convolved mesh: out = scale * (-B^T grad_u phi)
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather_field(int n, const double* pos, MeshGeom g, const T* phi, double scale,
+                                                      double* out) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int at = warp;
+    int m0[3];
+    T Mx[2][6], My[2][6], Mz[2][6];
+    stencil01<T>(g, pos, at, m0, Mx, My, Mz);
+    const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
+    T p1 = T(0), p2 = T(0), p3 = T(0);
+    for (int L = lane; L < 36; L += 32) {
+        const int ix = L / 6, iy = L % 6;
+        const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
+        const T* line = phi + ((size_t)gx * K1 + gy) * K2;
+        int gz = wrapi(m0[2] - 3, K2);
+        T s0 = T(0), s1 = T(0);
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+            const T v = line[gz];
+            s0 += v * Mz[0][t];
+            s1 += v * Mz[1][t];
+            gz = (gz + 1 == K2) ? 0 : gz + 1;
+        }
+        p1 += Mx[1][ix] * My[0][iy] * s0;
+        p2 += Mx[0][ix] * My[1][iy] * s0;
+        p3 += Mx[0][ix] * My[0][iy] * s1;
+    }
+    p1 = warp_sum(p1);
+    p2 = warp_sum(p2);
+    p3 = warp_sum(p3);
+    if (lane == 0) {
+        const double* B = g.B;
+        const double P1 = scale * (double)p1, P2 = scale * (double)p2, P3 = scale * (double)p3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[3 * at + c] = -(P1 * B[c] + P2 * B[3 + c] + P3 * B[6 + c]);
+    }
+}
+
 }  // namespace dmffb

@@ -49,23 +49,30 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
-// segmented suffix sum over runs of equal keys in a warp (keys of a run are contiguous lanes):
-// after the call, the first lane of each run holds the run total.
-template <typename T>
-__device__ __forceinline__ T seg_sum(T v, int key) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T ov = __shfl_down_sync(0xffffffffu, v, o);
-        int ok = __shfl_down_sync(0xffffffffu, key, o);
-        if (lane + o < 32 && ok == key) v += ov;
-    }
-    return v;
-}
+// Segmented sums over runs of equal keys in a warp.  A key may appear in several runs (rows
+// skipped by a launch sit between rows of the same atom), so runs are identified by a run id:
+// the number of run heads up to and including the lane.  After seg_sum, the head lane of each
+// run holds that run's total.
 __device__ __forceinline__ bool seg_head(int key) {
     const int lane = threadIdx.x & 31;
     int prev = __shfl_up_sync(0xffffffffu, key, 1);
     return lane == 0 || prev != key;
+}
+__device__ __forceinline__ int seg_run_id(int key) {
+    const int lane = threadIdx.x & 31;
+    const unsigned heads = __ballot_sync(0xffffffffu, seg_head(key));
+    return __popc(heads & (0xffffffffu >> (31 - lane)));
+}
+template <typename T>
+__device__ __forceinline__ T seg_sum(T v, int run) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T ov = __shfl_down_sync(0xffffffffu, v, o);
+        int orun = __shfl_down_sync(0xffffffffu, run, o);
+        if (lane + o < 32 && orun == run) v += ov;
+    }
+    return v;
 }
 
 // block-wide reduction of NV doubles into dst[] with one atomicAdd per value per block

@@ -6,6 +6,7 @@
 #include <cub/cub.cuh>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -69,6 +70,13 @@ struct dmffb_engine {
     int64_t* d_csr_off = nullptr;
     int32_t *d_csr_ent = nullptr, *d_csr_deg = nullptr;
     int64_t csr_cap = 0;
+    bool csr_from_build = false;     // CSR built together with the internal pair list
+    const int32_t* csr_pairs = nullptr;  // the half list the current CSR belongs to
+    float* d_posf = nullptr;
+    void* d_mvcoef = nullptr;  // [csr_cap] MvCoef<T>
+    void* d_mvz = nullptr;     // [csr_cap] T
+    int64_t mv_cap = 0;
+    int32_t* d_pcount_f = nullptr;
     void* d_cub2 = nullptr;
     size_t cub2_bytes = 0;
     void* d_grid = nullptr;
@@ -381,7 +389,10 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     sa.g = g;
     sa.grid = (T*)h->d_grid;
     sa.perm_mul = h->perm_mul;
-    LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
+    if (mode == GATHER_FIELD && !use_Qg && U)
+        LAUNCH(h, s, KC_SPREAD, k_spread_dip<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
+    else
+        LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
     CKFFT(cufftSetStream(h->plan_f, s));
     CKFFT(cufftSetStream(h->plan_b, s));
     if (sizeof(T) == 4) {
@@ -427,16 +438,42 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     ga.scal = h->d_scal + S_GATHER;
     ga.want_box = 1;
     ga.mode = mode;
-    LAUNCH(h, s, (mode == GATHER_FULL ? KC_GATHER_FULL : KC_GATHER_FIELD), k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga));
+    if (mode == GATHER_FIELD && !field_acc)
+        LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
+                                          h->n, pos, g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, field_out));
+    else
+        LAUNCH(h, s, (mode == GATHER_FULL ? KC_GATHER_FULL : KC_GATHER_FIELD), k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
 
-// dE/dU at U (include_perm) or its linear part A U (!include_perm), into out
+// pair tensors of every CSR entry for the solve at these positions
+template <typename T>
+int matvec_setup(dmffb_engine* h, cudaStream_t s, const Box& bx, const int32_t* pairs, int64_t npairs) {
+    int st;
+    if (h->csr_cap > h->mv_cap) {
+        if (h->d_mvcoef) { cudaFree(h->d_mvcoef); cudaFree(h->d_mvz); }
+        h->mv_cap = h->csr_cap;
+        if ((st = dalloc(h, &h->d_mvcoef, h->mv_cap * sizeof(MvCoef<T>)))) return st;
+        if ((st = dalloc(h, &h->d_mvz, h->mv_cap * sizeof(T)))) return st;
+    }
+    PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
+    CsrArgs c;
+    c.n = h->n;
+    c.off = h->d_csr_off;
+    c.ent = h->d_csr_ent;
+    LAUNCH(h, s, KC_PAIR_MATVEC, k_matvec_coef<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
+                                     a, c, (MvCoef<T>*)h->d_mvcoef, (T*)h->d_mvz));
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
 // full both-direction CSR of the half-list rows (for the atomics-free CG matvec)
 int build_csr(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npairs) {
     const int n = h->n;
     int st;
+    if (h->csr_from_build && pairs == h->d_pairs) return DMFFB_OK;  // made by the neighbour build
+    h->csr_from_build = false;
     if (!h->d_csr_off) {
         if ((st = dalloc(h, &h->d_csr_off, (n + 1) * sizeof(int64_t)))) return st;
         if ((st = dalloc(h, &h->d_csr_deg, n * sizeof(int32_t)))) return st;
@@ -470,7 +507,12 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     if (include_perm) CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
     if (include_perm && npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
-        LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, s>>>(a));
+        if (sizeof(T) == 4) {
+            LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_UNSCALED><<<nblk(npairs, 128), 128, 0, s>>>(a));
+            LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(npairs, 128), 128, 0, s>>>(a));
+        } else {
+            LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, s>>>(a));
+        }
     }
     // the real-space matvec runs on a side stream, overlapping the reciprocal pass
     const bool fork = U && h->s2 && !h->prof;
@@ -486,7 +528,8 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
             CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
             sm = h->s2;
         }
-        LAUNCH(h, sm, KC_PAIR_MATVEC, k_matvec_csr<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, sm>>>(a, c, h->d_fmv));
+        LAUNCH(h, sm, KC_PAIR_MATVEC, k_matvec_apply<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, sm>>>(
+                                          c, (const MvCoef<T>*)h->d_mvcoef, (const T*)h->d_mvz, U, h->d_fmv));
         if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
     const double* recip = nullptr;
@@ -513,6 +556,7 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     double* sc = h->d_scal + S_CG;
     int st;
     if ((st = build_csr(h, s, pairs, npairs))) return st;
+    if ((st = matvec_setup<T>(h, s, bx, pairs, npairs))) return st;
     if (h->solver == DMFFB_SOLVER_REFERENCE) {
         int it = 0;
         bool conv = false;
@@ -567,7 +611,8 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     const bool graphs = h->use_graphs && !h->prof;
     if (graphs) {
         std::vector<double> key = {(double)(uintptr_t)pos, (double)(uintptr_t)pairs, (double)npairs,
-                                   (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T)};
+                                   (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T),
+                                   (double)(uintptr_t)h->d_mvcoef, (double)(uintptr_t)h->d_csr_off};
         for (int k = 0; k < 9; ++k) key.push_back(bx.h[k]);
         if (!h->cg_exec || key != h->cg_key) {
             if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
@@ -666,8 +711,19 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     if (h->timing) CK(cudaEventRecord(h->ev[2], s));
     if (npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, h->lpol ? U : nullptr);
-        if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a));
-        else LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL><<<nblk(npairs, 128), 128, 0, s>>>(a));
+        const unsigned nbk = nblk(npairs, 128);
+        if (sizeof(T) == 4) {
+            if (h->lpol) {
+                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(a));
+                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbk, 128, 0, s>>>(a));
+            } else {
+                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(a));
+                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbk, 128, 0, s>>>(a));
+            }
+        } else {
+            if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nbk, 128, 0, s>>>(a));
+            else LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL><<<nbk, 128, 0, s>>>(a));
+        }
         CK(cudaGetLastError());
     }
     if (h->timing) CK(cudaEventRecord(h->ev[3], s));
@@ -689,7 +745,7 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     sa.scal = h->d_scal + S_SELF;
     sa.tau_out = nullptr;
     if (h->lmax == 0) sa.f.axis_idx = nullptr;
-    LAUNCH(h, s, KC_SELF, k_self_frames<T><<<nblk(n, 128), 128, 0, s>>>(sa));
+    LAUNCH(h, s, KC_SELF, k_self_frames<T><<<nblk(n, 32), 32, 0, s>>>(sa));
     if (forces) LAUNCH(h, s, KC_VEC, k_finalize_forces<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_gpair, h->d_grad, forces));
     CK(cudaGetLastError());
     if (h->timing) CK(cudaEventRecord(h->ev[5], s));
@@ -772,6 +828,7 @@ int dmffb_admp_create(const dmffb_admp_desc* d, dmffb_engine** out) {
         h->dsc[k] = d->dscales[k];
     }
     h->solver = d->solver;
+    if (getenv("DMFFB_DISABLE_GRAPHS")) h->use_graphs = false;  // eager launches (debugging, tools)
     {  // a multiplier coprime with n near n / 148 (one stride per SM) for the spread order
         auto gcd = [](int64_t a, int64_t b) { while (b) { int64_t t = a % b; a = b; b = t; } return a; };
         int64_t m = std::max<int64_t>(1, d->n_atoms / 148) | 1;
@@ -905,7 +962,7 @@ void dmffb_destroy(dmffb_engine* h) {
     void* ptrs[] = {h->d_axis_type, h->d_axis_idx, h->d_cov_ptr, h->d_cov_j, h->d_cov_nb, h->d_Qloc, h->d_pol,
                     h->d_thole, h->d_polsix, h->d_pos, h->d_U, h->d_forces, h->d_posT, h->d_Qg, h->d_QgT,
                     h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
-                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
+                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_mvz, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
                     h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
                     h->d_cub};
     for (void* p : ptrs)
@@ -1135,18 +1192,132 @@ int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, cons
 }
 
 int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box) {
-    if (!h) return DMFFB_BAD_ARG;
-    int64_t need = 0;
-    int st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
-    if (st == DMFFB_NEIGHBOR_OVERFLOW) {
-        if (h->d_pairs) cudaFree(h->d_pairs);
-        h->pair_cap = (int64_t)(need * 1.3) + 64;  // headroom as in nblist.py:37-38
-        if ((st = dalloc(h, &h->d_pairs, h->pair_cap * 3 * sizeof(int32_t)))) return st;
-        st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
+    if (!h || !pos || !box) return DMFFB_BAD_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int n = h->n;
+    Box bx;
+    make_box(box, bx);
+    const double* m = bx.h;
+    const double V = fabs(det3(m));
+    int nc[3];
+    bool cells = true;
+    for (int k = 0; k < 3; ++k) {
+        const double* u = m + 3 * ((k + 1) % 3);
+        const double* w = m + 3 * ((k + 2) % 3);
+        const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+        nc[k] = (int)floor(V / sqrt(cx * cx + cy * cy + cz * cz) / h->rc);
+        if (nc[k] > 64) nc[k] = 64;
+        if (nc[k] < 3) cells = false;
     }
-    if (st) return st;
-    h->npairs = need;
+    if (!cells) {  // small boxes: the generic builder, CSR later from the rows
+        int64_t need = 0;
+        int st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
+        if (st == DMFFB_NEIGHBOR_OVERFLOW) {
+            if (h->d_pairs) cudaFree(h->d_pairs);
+            h->pair_cap = (int64_t)(need * 1.3) + 64;
+            if ((st = dalloc(h, &h->d_pairs, h->pair_cap * 3 * sizeof(int32_t)))) return st;
+            st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
+        }
+        if (st) return st;
+        h->npairs = need;
+        h->have_pairs = true;
+        h->csr_from_build = false;
+        return DMFFB_OK;
+    }
+    int st;
+    if (!h->d_pcount) {
+        if ((st = dalloc(h, &h->d_pcount, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_poff, (n + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_atom_cell, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_atoms, n * sizeof(int32_t)))) return st;
+    }
+    if (!h->d_posf) {
+        if ((st = dalloc(h, &h->d_posf, 4 * n * sizeof(float)))) return st;
+        if ((st = dalloc(h, &h->d_pcount_f, n * sizeof(int32_t)))) return st;
+    }
+    if (!h->d_csr_off) {
+        if ((st = dalloc(h, &h->d_csr_off, (n + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_csr_deg, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_fmv, 3 * n * sizeof(double)))) return st;
+        size_t need = 0;
+        cub::DeviceScan::InclusiveSum(nullptr, need, (int32_t*)nullptr, (int64_t*)nullptr, n);
+        h->cub2_bytes = need;
+        if ((st = dalloc(h, &h->d_cub2, need))) return st;
+    }
+    const int ncell = nc[0] * nc[1] * nc[2];
+    if (ncell + 1 > h->ncell_cap) {
+        if (h->d_cell_count) { cudaFree(h->d_cell_count); cudaFree(h->d_cell_start); cudaFree(h->d_cell_cursor); }
+        h->ncell_cap = ncell + 1;
+        if ((st = dalloc(h, &h->d_cell_count, h->ncell_cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_start, h->ncell_cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_cursor, h->ncell_cap * sizeof(int32_t)))) return st;
+    }
+    size_t need = 0, need2 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, (int32_t*)nullptr, (int32_t*)nullptr, ncell + 1);
+    cub::DeviceScan::InclusiveSum(nullptr, need2, (int32_t*)nullptr, (int64_t*)nullptr, n);
+    need = std::max(need, need2);
+    if (need > h->cub_bytes) {
+        if (h->d_cub) cudaFree(h->d_cub);
+        h->cub_bytes = need;
+        if ((st = dalloc(h, &h->d_cub, need))) return st;
+    }
+    LAUNCH(h, s, KC_NBLIST, k_pos_f32<<<nblk(n, 256), 256, 0, s>>>(n, pos, h->d_posf));
+    CK(cudaMemsetAsync(h->d_cell_count, 0, (ncell + 1) * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(h->d_cell_cursor, 0, (ncell + 1) * sizeof(int32_t), s));
+    LAUNCH(h, s, KC_NBLIST, k_cell_count<<<nblk(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], h->d_atom_cell,
+                                                                     h->d_cell_count));
+    size_t tb = h->cub_bytes;
+    LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_cell_count, h->d_cell_start, ncell + 1, s));
+    LAUNCH(h, s, KC_NBLIST, k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(n, h->d_atom_cell, h->d_cell_start,
+                                                                    h->d_cell_cursor, h->d_cell_atoms));
+    Nb2Args b;
+    b.a.n = n;
+    b.a.pos = pos;
+    b.a.box = bx;
+    b.a.rc = h->rc;
+    for (int k = 0; k < 3; ++k) b.a.nc[k] = nc[k];
+    b.a.cell_start = h->d_cell_start;
+    b.a.cell_atoms = h->d_cell_atoms;
+    b.a.cov_ptr = h->d_cov_ptr;
+    b.a.cov_j = h->d_cov_j;
+    b.a.cov_nb = h->d_cov_nb;
+    b.a.count = h->d_pcount;
+    b.a.offset = h->d_poff;
+    b.posf = h->d_posf;
+    b.count_f = h->d_pcount_f;
+    b.off_f = h->d_csr_off;
+    LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
+    CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
+    CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
+    tb = h->cub_bytes;
+    LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount, h->d_poff + 1, n, s));
+    tb = h->cub_bytes;
+    LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount_f, h->d_csr_off + 1, n, s));
+    int64_t tot[2] = {0, 0};
+    CK(cudaMemcpyAsync(&tot[0], h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&tot[1], h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (tot[0] > h->pair_cap) {
+        if (h->d_pairs) cudaFree(h->d_pairs);
+        h->pair_cap = (int64_t)(tot[0] * 1.3) + 64;  // headroom as in nblist.py:37-38
+        if ((st = dalloc(h, &h->d_pairs, h->pair_cap * 3 * sizeof(int32_t)))) return st;
+    }
+    if (tot[1] > h->csr_cap) {
+        if (h->d_csr_ent) cudaFree(h->d_csr_ent);
+        h->csr_cap = (int64_t)(tot[1] * 1.3) + 1024;
+        if ((st = dalloc(h, &h->d_csr_ent, h->csr_cap * sizeof(int32_t)))) return st;
+    }
+    b.a.pairs = h->d_pairs;
+    b.a.cap = h->pair_cap;
+    b.ent = h->d_csr_ent;
+    b.cap_f = h->csr_cap;
+    LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    prof_collect(h);
+    h->npairs = tot[0];
     h->have_pairs = true;
+    h->csr_from_build = true;
     return DMFFB_OK;
 }
 

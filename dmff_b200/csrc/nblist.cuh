@@ -229,4 +229,117 @@ __global__ void __launch_bounds__(256) k_pairs_warp(NbArgs a) {
     if (PASS == 0 && lane == 0) a.count[i] = cnt;
 }
 
+
+// Same cell scan emitting both layouts the engine uses: half rows (i, j, nbond), j > i, sorted
+// by i (pair kernels), and the full neighbour CSR (j != i, packed j | scale index << 28) for the
+// atomics-free CG matvec.  Positions for the FP32 prefilter come from the FP32 copy (posf);
+// borderline candidates fall back to the exact FP64 test on pos.
+struct Nb2Args {
+    NbArgs a;
+    const float* posf;      // [n*4]
+    int32_t* count_f;       // [n] pass 0: full-list counts
+    const int64_t* off_f;   // [n+1] pass 1
+    int32_t* ent;           // [cap_f]
+    int64_t cap_f;
+};
+
+template <int PASS>
+__global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
+    const NbArgs& a = b.a;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= a.n) return;
+    const double* pi = a.pos + 3 * i;
+    const float pix = b.posf[4 * i], piy = b.posf[4 * i + 1], piz = b.posf[4 * i + 2];
+    float hf[9], hif[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { hf[k] = (float)a.box.h[k]; hif[k] = (float)a.box.hinv[k]; }
+    // FP32 positions carry ~1e-5 A rounding at 100 A: the 2e-3 A band around rc goes to FP64
+    const float rlo = (float)(a.rc - 2e-3), rhi = (float)(a.rc + 2e-3);
+    const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
+    int c3[3];
+    cell_of(a.box, a.nc, pi, c3);
+    int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1) ? b.off_f[i] : 0;
+    int cnt_h = 0, cnt_f = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int dx = -1; dx <= 1; ++dx) {
+        const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
+                const int c = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+                const int cs = a.cell_start[c], ce = a.cell_start[c + 1];
+                for (int base = cs; base < ce; base += 32) {
+                    const int k = base + lane;
+                    bool keep = false;
+                    int j = -1;
+                    if (k < ce) {
+                        j = a.cell_atoms[k];
+                        if (j != i) {
+                            const float d0 = b.posf[4 * j] - pix, d1 = b.posf[4 * j + 1] - piy, d2 = b.posf[4 * j + 2] - piz;
+                            bool amb = false;
+                            float sf[3];
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) {
+                                float t = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
+                                float nn = floorf(t + 0.5f);
+                                sf[q] = t - nn;
+                                amb |= fabsf(sf[q]) > 0.4999f;
+                            }
+                            const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
+                            const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
+                            const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
+                            const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
+                            if (!amb && r2 < rlo2) keep = true;
+                            else if (!amb && r2 > rhi2) keep = false;
+                            // exact test on the (lower, higher) orientation, as the half list defines it
+                            else keep = j > i ? within_rc(a.box, pi, a.pos + 3 * j, a.rc)
+                                              : within_rc(a.box, a.pos + 3 * j, pi, a.rc);
+                        }
+                    }
+                    const bool up = keep && j > i;
+                    const unsigned mf = __ballot_sync(0xffffffffu, keep);
+                    const unsigned mh = __ballot_sync(0xffffffffu, up);
+                    if (PASS == 1) {
+                        if (keep) {
+                            const int nbd = j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i);
+                            int sidx = nbd - 1;
+                            if (sidx < 0) sidx += 6;
+                            const int64_t sf_ = out_f + __popc(mf & lt);
+                            if (sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
+                            if (up) {
+                                const int64_t sh = out_h + __popc(mh & lt);
+                                if (sh < a.cap) {
+                                    a.pairs[3 * sh] = i;
+                                    a.pairs[3 * sh + 1] = j;
+                                    a.pairs[3 * sh + 2] = nbd;
+                                }
+                            }
+                        }
+                        out_f += __popc(mf);
+                        out_h += __popc(mh);
+                    } else {
+                        cnt_f += __popc(mf);
+                        cnt_h += __popc(mh);
+                    }
+                }
+            }
+        }
+    }
+    if (PASS == 0 && lane == 0) {
+        a.count[i] = cnt_h;
+        b.count_f[i] = cnt_f;
+    }
+}
+
+__global__ void k_pos_f32(int n, const double* pos, float* posf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    posf[4 * i] = (float)pos[3 * i];
+    posf[4 * i + 1] = (float)pos[3 * i + 1];
+    posf[4 * i + 2] = (float)pos[3 * i + 2];
+    posf[4 * i + 3] = 0.f;
+}
+
 }  // namespace dmffb

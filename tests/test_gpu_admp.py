@@ -131,3 +131,41 @@ def test_dropin_api_water_dimer_goldens(xml, key, dec):
     np.testing.assert_almost_equal(E.item(), gold, decimal=dec)
     (g,) = torch.autograd.grad(E, pos)
     assert torch.isfinite(g).all()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_pair_row_order_and_padding_do_not_matter(pol_small, prec):
+    """the reference accepts rows in any order with padding / invalid rows (utils.py:67-85)."""
+    s, pr, ref = pol_small
+    rng = np.random.default_rng(0)
+    n = s["n_atoms"]
+    junk = np.array([[n, n, 0], [5, 5, 0], [7, 3, 1], [n, n, 0]] * 50)
+    rows = np.concatenate([pr, junk])[rng.permutation(len(pr) + len(junk))]
+    eng = make_engine(s, precision=prec, cg_tol=1e-6 if prec == "fp32" else 1e-11)
+    res, F, U = _run(eng, s, rows)
+    t = TOL[prec]
+    assert abs(res.energy - ref["E"]) <= t["e"] * abs(ref["E"])
+    assert rel_force_rms(F, ref["F"]) <= t["f"]
+
+
+def test_full_size_fp32_matches_fp64():
+    """size-independent check at the benchmark size (12288 atoms): the FP32 path against the FP64
+    instantiation of the same kernels (which matches the oracle on every small case)."""
+    from dmff_b200.synthetic import workload
+    s = workload("c1")
+    dev = torch.device("cuda")
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
+    out = {}
+    for prec in ("fp64", "fp32"):
+        eng = make_engine(s, precision=prec, cg_tol=1e-8)
+        eng.rebuild_internal_pairs(pos, s["box"])
+        res, F, U = eng.compute(pos, s["box"])
+        out[prec] = (res.energy, F.cpu().numpy().copy(), U.cpu().numpy().copy(), np.array(res.box_grad[:]),
+                     res.n_pairs)
+    e64, F64, U64, B64, n64 = out["fp64"]
+    e32, F32, U32, B32, n32 = out["fp32"]
+    assert n32 == n64 > 1_000_000
+    assert abs(e32 - e64) <= 1e-6 * abs(e64)
+    assert rel_force_rms(F32, F64) <= 1e-5
+    assert np.abs(U32 - U64).max() <= 1e-4 * np.abs(U64).max()
+    assert np.abs(B32 - B64).max() <= 1e-4 * np.abs(B64).max()

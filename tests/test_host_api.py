@@ -1,0 +1,104 @@
+"""Host-side logic: XML / topology / generator set-up, the C-ABI library symbols, builders."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from dmff_b200 import Hamiltonian, PDBFile
+from dmff_b200 import _lib
+from dmff_b200.synthetic import water_box, workload, pairs_nbond
+
+HERE = os.path.dirname(__file__)
+ROOT = os.path.dirname(HERE)
+DATA = os.path.join(HERE, "golden", "data")
+
+
+def test_header_symbols_exported_by_library():
+    """every function include/dmffb200.h declares is exported by libdmffb200.so (no GPU calls)."""
+    header = open(os.path.join(ROOT, "include", "dmffb200.h")).read()
+    declared = set(re.findall(r"\b(dmffb_\w+)\s*\(", header))
+    assert declared, "no declarations found"
+    lib = _lib.load()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(_lib.EXPORTED)
+
+
+def test_ctypes_struct_layout_matches_header():
+    """the ctypes mirror of dmffb_admp_desc / dmffb_admp_result has the C layout (offsets via a
+    tiny C program compiled here)."""
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "dmffb200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(dmffb_admp_desc), offsetof(dmffb_admp_desc, cov_rows),
+         offsetof(dmffb_admp_desc, mscales), offsetof(dmffb_admp_desc, steps_pol), sizeof(dmffb_admp_result),
+         offsetof(dmffb_admp_result, n_pairs));
+  return 0; }'''
+    tmp = os.path.join(os.environ.get("TMPDIR", "/tmp"), "dmffb_layout")
+    with open(tmp + ".c", "w") as f:
+        f.write(src)
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), tmp + ".c", "-o", tmp], check=True)
+    vals = [int(x) for x in subprocess.run([tmp], capture_output=True, text=True, check=True).stdout.split()]
+    D, Rr = _lib.AdmpDesc, _lib.AdmpResult
+    assert vals == [ctypes.sizeof(D), D.cov_rows.offset, D.mscales.offset, D.steps_pol.offset, ctypes.sizeof(Rr),
+                    Rr.n_pairs.offset]
+
+
+def test_generator_parses_reference_xml_like_reference():
+    H = Hamiltonian(os.path.join(DATA, "admp.xml"))
+    pdb = PDBFile(os.path.join(DATA, "water_dimer.pdb"))
+    pot = H.createPotential(pdb.topology, nonbondedMethod="CutoffPeriodic", nonbondedCutoff=0.4, ethresh=5e-4,
+                            step_pol=5)
+    g = H.generators["ADMPPmeForce"]
+    pf = g.pme_force
+    # axis types / indices of tests/test_admp/test_sptial.py:71-142
+    assert pf.axis_type.tolist() == [1, 0, 0, 1, 0, 0]
+    assert pf.axis_indices.tolist() == [[1, 2, -1], [0, 2, -1], [0, 1, -1], [4, 5, -1], [3, 5, -1], [3, 4, -1]]
+    Q = H.paramset["ADMPPmeForce"]["Q_local"].numpy()
+    np.testing.assert_allclose(Q[0], [-1.0614, -0.23671684, 0, 0, -0.0714102, 0, 0, 0.01106659, 0], rtol=1e-6)
+    np.testing.assert_allclose(H.paramset["ADMPPmeForce"]["pol"].numpy(), [0.88, 0.0])
+    assert g.mScales == [0.0, 0.0, 0.0, 1.0, 1.0, 1.0]
+    assert pf.kappa == 0.0 and pf.lpme is False
+    assert pot.meta["cov_map"][0, 1] == 1 and pot.meta["cov_map"][1, 2] == 2 and pot.meta["cov_map"][0, 3] == 0
+    assert "ADMPPmeForce" in pot.dmff_potentials
+
+
+def test_pme_parameters_follow_reference_formula():
+    from dmff_b200.admp.pme import setup_ewald_parameters
+    kappa, K1, K2, K3 = setup_ewald_parameters(6.0, 5e-4, np.eye(3) * 18.6)
+    assert abs(kappa - 0.43804) < 1e-5 and (K1, K2, K3) == (25, 25, 25)
+    kappa, K1, _, _ = setup_ewald_parameters(8.0, 5e-4, np.eye(3) * 49.7)
+    assert abs(kappa - 0.32853) < 1e-5 and K1 == 50
+
+
+def test_covalent_map_matches_dense_reference_semantics():
+    from dmff_b200.api.topology import covalent_rows, CovalentMap
+    # a 7-atom chain with a branch: shortest paths up to 6 bonds
+    bonds = [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (5, 6), (2, 6)]
+    cm = CovalentMap(7, covalent_rows(7, bonds))
+    d = cm.dense()
+    assert d[0, 1] == 1 and d[0, 2] == 2 and d[0, 6] == 3 and d[3, 6] == 2 and d[0, 4] == 4
+    assert (d == d.T).all() and (np.diag(d) == 0).all()
+
+
+def test_water_builder_properties():
+    s = water_box(216, 18.6, seed=0)
+    assert s["pos"].shape == (648, 3)
+    import oracle.admp_ref as R
+    pr = R.brute_force_pairs(s["pos"], s["box"], 1.7)
+    mol = np.arange(648) // 3
+    assert (mol[pr[:, 0]] == mol[pr[:, 1]]).all()  # no intermolecular contact below 1.7 A
+    oh = np.linalg.norm(s["pos"][1::3] - s["pos"][0::3], axis=1)
+    np.testing.assert_allclose(oh, 0.9572, atol=1e-12)
+    assert workload("c1")["K"] == (50, 50, 50)
+
+
+def test_pairs_nbond_lookup():
+    s = water_box(8, 6.2, seed=3)
+    pr = np.array([[0, 1, 0], [1, 2, 0], [0, 3, 0], [3, 5, 0]])
+    np.testing.assert_array_equal(pairs_nbond(pr, s["cov_rows"], s["n_atoms"]), [1, 2, 0, 1])
