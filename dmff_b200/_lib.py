@@ -17,6 +17,8 @@ DMFFB_NOT_CONVERGED = 4
 DMFFB_NEIGHBOR_OVERFLOW = 5
 DMFFB_NONFINITE = 6
 DMFFB_CUFFT_ERROR = 7
+DMFFB_SCRATCH_TOO_SMALL = 8
+NOALLOC_MAX_ATOMS = 65536
 
 DMFFB_FP32 = 0
 DMFFB_FP64 = 1
@@ -28,7 +30,7 @@ EXPORTED = [
     "dmffb_admp_create", "dmffb_destroy", "dmffb_last_error", "dmffb_admp_set_params",
     "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
     "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
-    "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters",
+    "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters", "dmffb_build_neighbors_noalloc",
 ]
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
@@ -105,6 +107,7 @@ def load():
     lib.dmffb_set_profiling.argtypes = [vp, i32]
     lib.dmffb_get_kernel_stats.argtypes = [vp, P(dbl), P(i64), i32]
     lib.dmffb_get_counters.argtypes = [vp, P(i64), i32]
+    lib.dmffb_build_neighbors_noalloc.argtypes = [vp, vp, i32, vp, dbl, vp, vp, vp, vp, i64, P(i64)]
     for name in EXPORTED:
         if name not in ("dmffb_destroy", "dmffb_last_error"):
             getattr(lib, name).restype = ctypes.c_int

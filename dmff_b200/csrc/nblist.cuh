@@ -63,7 +63,7 @@ __device__ __forceinline__ int cell_of(const Box& b, const int nc[3], const doub
     return (c3[0] * nc[1] + c3[1]) * nc[2] + c3[2];
 }
 
-__global__ void k_cell_count(int n, const double* pos, Box b, int nc0, int nc1, int nc2, int32_t* atom_cell,
+static __global__ void k_cell_count(int n, const double* pos, Box b, int nc0, int nc1, int nc2, int32_t* atom_cell,
                              int32_t* cell_count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -74,7 +74,7 @@ __global__ void k_cell_count(int n, const double* pos, Box b, int nc0, int nc1, 
     atomicAdd(cell_count + c, 1);
 }
 
-__global__ void k_cell_fill(int n, const int32_t* atom_cell, const int32_t* cell_start, int32_t* cursor,
+static __global__ void k_cell_fill(int n, const int32_t* atom_cell, const int32_t* cell_start, int32_t* cursor,
                             int32_t* cell_atoms) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
     }
 }
 
-__global__ void k_pos_f32(int n, const double* pos, float* posf) {
+static __global__ void k_pos_f32(int n, const double* pos, float* posf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     posf[4 * i] = (float)pos[3 * i];

@@ -25,7 +25,8 @@ enum {
     DMFFB_NOT_CONVERGED = 4,      /* warning: results written, induced dipoles not converged */
     DMFFB_NEIGHBOR_OVERFLOW = 5,  /* pair capacity too small; *npairs_out holds the count needed */
     DMFFB_NONFINITE = 6,
-    DMFFB_CUFFT_ERROR = 7
+    DMFFB_CUFFT_ERROR = 7,
+    DMFFB_SCRATCH_TOO_SMALL = 8   /* request exceeds a fixed-size scratch limit (see the _noalloc entry) */
 };
 
 /* local-axis types, dmff/admp/spatial.py:59-65 */
@@ -136,6 +137,29 @@ int dmffb_set_profiling(dmffb_engine* h, int32_t enabled);
 int dmffb_get_kernel_stats(const dmffb_engine* h, double* ms_out, int64_t* launches_out, int32_t n);
 /* [0] launches of this library's kernels since create, [1] cuFFT executions. */
 int dmffb_get_counters(const dmffb_engine* h, int64_t* out, int32_t n);
+
+/* Neighbour-list build that allocates no device memory.  No counterpart in the reference (DMFF
+ * has no C ABI); same result as dmffb_build_neighbors for callers that cannot allocate on
+ * demand: a host (an MD platform such as an OpenMM context, a framework with a caching
+ * allocator, a process under a fixed memory budget) that owns the device heap and forbids
+ * cudaMalloc after start-up.  All scratch (cell bins, per-atom counts and offsets, scan storage)
+ * lives in one fixed device array inside the library; the call makes no cudaMalloc / cudaFree
+ * and calls no allocating library routine.  Needs no engine handle.
+ *   pos: device [n_atoms*3] FP64, Angstrom; box: host [9]; rc > 0.
+ *   cov_ptr/cov_j/cov_nb: device CSR of the covalent map restricted to j > i (rows of atom i are
+ *     cov_j[cov_ptr[i] .. cov_ptr[i+1]-1] with nbond cov_nb[...]); all three NULL means nbond 0.
+ *   pairs_out: device [capacity*3] rows (i, j, nbond), i < j, sorted by i; *npairs_out = count.
+ * Limits: n_atoms <= DMFFB_NOALLOC_MAX_ATOMS (larger -> DMFFB_SCRATCH_TOO_SMALL); the cell grid
+ * is coarsened to at most DMFFB_NOALLOC_MAX_CELLS cells.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Every call on a device shares the one array and each call
+ * re-zeroes what it accumulates into; calls that overlap on the GPU (different streams, or
+ * host threads) race on it and must be serialized by the caller. */
+#define DMFFB_NOALLOC_MAX_ATOMS 65536
+#define DMFFB_NOALLOC_MAX_CELLS 32768
+int dmffb_build_neighbors_noalloc(void* stream, const double* pos, int32_t n_atoms, const double* box, double rc,
+                                  const int32_t* cov_ptr, const int32_t* cov_j, const int32_t* cov_nb,
+                                  int32_t* pairs_out, int64_t capacity, int64_t* npairs_out);
 
 #ifdef __cplusplus
 }
