@@ -31,6 +31,7 @@ EXPORTED = [
     "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
     "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
     "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters", "dmffb_build_neighbors_noalloc",
+    "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads",
 ]
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
@@ -76,6 +77,35 @@ class AdmpResult(ctypes.Structure):
     ]
 
 
+class DispDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int32),
+        ("pmax", ctypes.c_int32),
+        ("lpme", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("rc", ctypes.c_double),
+        ("kappa", ctypes.c_double),
+        ("K", ctypes.c_int32 * 3),
+        ("n_cov", ctypes.c_int64),
+        ("cov_rows", ctypes.POINTER(ctypes.c_int32)),
+        ("mscales", ctypes.c_double * 6),
+        ("tt_damping", ctypes.c_int32),
+    ]
+
+
+class DispResult(ctypes.Structure):
+    _fields_ = [
+        ("energy", ctypes.c_double),
+        ("e_real", ctypes.c_double),
+        ("e_recip", ctypes.c_double),
+        ("e_self", ctypes.c_double),
+        ("e_sr", ctypes.c_double),
+        ("box_grad", ctypes.c_double * 9),
+        ("box_grad_sr", ctypes.c_double * 9),
+        ("n_pairs", ctypes.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -108,6 +138,10 @@ def load():
     lib.dmffb_get_kernel_stats.argtypes = [vp, P(dbl), P(i64), i32]
     lib.dmffb_get_counters.argtypes = [vp, P(i64), i32]
     lib.dmffb_build_neighbors_noalloc.argtypes = [vp, vp, i32, vp, dbl, vp, vp, vp, vp, i64, P(i64)]
+    lib.dmffb_disp_create.argtypes = [P(DispDesc), P(vp)]
+    lib.dmffb_disp_set_params.argtypes = [vp, vp, vp, vp, vp]
+    lib.dmffb_disp_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp, P(DispResult)]
+    lib.dmffb_disp_param_grads.argtypes = [vp, vp, vp]
     for name in EXPORTED:
         if name not in ("dmffb_destroy", "dmffb_last_error"):
             getattr(lib, name).restype = ctypes.c_int

@@ -1,0 +1,73 @@
+"""ADMPDispPmeForce backed by the B200 engine (drop-in for dmff/admp/disp_pme.py:13-77).
+
+``get_energy(positions, box, pairs, c_list, mScales)`` returns the dispersion PME energy E_lr
+(real + three reciprocal passes with the k = 0 term + self, disp_pme.py:80-130) as a torch
+scalar with autograd to positions and box.  With ``tt=(a_list, b_list, q_list)`` it returns
+E_sr - E_lr, E_sr the Tang-Toennies damped short-range term of ADMPDispForce
+(pairwise.py:100-118, admp.py:183-208), evaluated in the same pair pass.
+"""
+import numpy as np
+import torch
+
+from .pme import setup_ewald_parameters
+
+
+class ADMPDispPmeForce:
+    def __init__(self, box, rc, ethresh, pmax, lpme=True, cov_rows=None, tt_damping=False, precision="fp32",
+                 device=None):
+        self.rc, self.ethresh, self.pmax, self.lpme = rc, ethresh, pmax, lpme
+        if lpme:
+            self.kappa, self.K1, self.K2, self.K3 = setup_ewald_parameters(rc, ethresh, box)
+        else:
+            self.kappa, self.K1, self.K2, self.K3 = 0.0, 0, 0, 0
+        self.pme_order = 6
+        self.cov_rows = np.zeros((0, 3), np.int32) if cov_rows is None else np.asarray(cov_rows)
+        self.tt = tt_damping
+        self.precision = precision
+        self.device = device
+        self._engine = None
+        self._key = None
+        self.last_result = None
+
+    def _eng(self, n, mScales):
+        from ..engine import DispEngine
+        ms = tuple(float(x) for x in np.asarray(torch.as_tensor(mScales).detach().cpu()))
+        if self._engine is None or self._engine.n != n or self._engine.mscales != ms:
+            self._engine = DispEngine(n, self.pmax, self.lpme, self.rc, self.kappa, (self.K1, self.K2, self.K3),
+                                      self.cov_rows, ms, tt=self.tt, precision=self.precision, device=self.device)
+        return self._engine
+
+    def get_energy(self, positions, box, pairs, c_list, mScales, tt=None):
+        from .pme import _as_cuda_pairs
+        positions = torch.as_tensor(positions, dtype=torch.float64)
+        if not torch.is_tensor(box):
+            box = torch.as_tensor(np.asarray(box), dtype=torch.float64)
+        eng = self._eng(positions.shape[0], mScales)
+        eng.set_params(c_list, *(tt if tt is not None else (None, None, None)))
+        return _DispEnergy.apply(positions, box, eng, _as_cuda_pairs(pairs, eng.device), self, tt is not None)
+
+
+class _DispEnergy(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, positions, box, eng, pairs, force, with_tt):
+        pos = positions.detach().to(device=eng.device, dtype=torch.float64).contiguous()
+        res, F = eng.compute(pos, box, pairs=pairs)
+        force.last_result = res
+        sign = 1.0 if with_tt else 1.0
+        E = (res.e_sr - res.energy) if with_tt else res.energy
+        g_sr = torch.tensor(list(res.box_grad_sr), dtype=torch.float64).reshape(3, 3)
+        g_lr = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
+        # forces from the engine are -dE_lr/dpos (disp) and -dE_sr/dpos (TT) separately
+        Flr, Fsr = F
+        grad = (-(Fsr - Flr)) if with_tt else (-Flr)
+        ctx.save_for_backward(grad.clone())
+        ctx.box_grad = (g_sr - g_lr) if with_tt else g_lr
+        ctx.devs = (positions.device, box.device)
+        del sign
+        return torch.tensor(E, dtype=torch.float64, device=positions.device)
+
+    @staticmethod
+    def backward(ctx, g):
+        (grad,) = ctx.saved_tensors
+        return ((grad * g.to(grad.device)).to(ctx.devs[0]), (ctx.box_grad.to(ctx.devs[1]) * g.to(ctx.devs[1])),
+                None, None, None, None)

@@ -18,6 +18,7 @@
 #include "admp_recip.cuh"
 #include "common.cuh"
 #include "nblist.cuh"
+#include "disp.cuh"
 
 using namespace dmffb;
 
@@ -116,6 +117,13 @@ struct dmffb_engine {
     cudaGraphExec_t cg_exec = nullptr;
     std::vector<double> cg_key;
     bool use_graphs = true;
+    // ---- dispersion PME / TT damping (engines made by dmffb_disp_create)
+    int kind = 0;  // 0 ADMP multipolar PME, 1 dispersion
+    int pmax = 10, tt = 0;
+    void *d_c = nullptr, *d_tta = nullptr, *d_ttb = nullptr, *d_ttq = nullptr;  // kernel precision
+    void *d_glr = nullptr, *d_gsr = nullptr;
+    double* d_dc = nullptr;  // [3n] dE_lr/dc per channel (reciprocal part)
+    double e_self_disp = 0.0;
 };
 
 namespace {
@@ -800,6 +808,183 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     return DMFFB_OK;
 }
 
+
+// reciprocal pass of one point-charge-like channel (dispersion: c_k with the C_k influence
+// function including k = 0), accumulating energy / k-space tensor / mesh box term into scal
+template <typename T>
+int recip_pass_channel(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const T* q, int kind,
+                       double escale, double* grad, double* dq, double* scal_conv, double* scal_gather) {
+    const MeshGeom g = mesh_geom(bx, h->K);
+    const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
+    CK(cudaMemsetAsync(h->d_grid, 0, K3 * sizeof(T), s));
+    SpreadArgs<T> sa;
+    sa.n = h->n;
+    sa.pos = pos;
+    sa.Qg = nullptr;
+    sa.U = nullptr;
+    sa.q1 = q;
+    sa.lmax = 0;
+    sa.g = g;
+    sa.grid = (T*)h->d_grid;
+    sa.perm_mul = h->perm_mul;
+    LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
+    CKFFT(cufftSetStream(h->plan_f, s));
+    CKFFT(cufftSetStream(h->plan_b, s));
+    if (sizeof(T) == 4) FFTCALL(h, s, cufftExecR2C(h->plan_f, (cufftReal*)h->d_grid, (cufftComplex*)h->d_cgrid));
+    else FFTCALL(h, s, cufftExecD2Z(h->plan_f, (cufftDoubleReal*)h->d_grid, (cufftDoubleComplex*)h->d_cgrid));
+    ConvArgs<T> ca;
+    for (int k = 0; k < 3; ++k) ca.K[k] = h->K[k];
+    ca.Kh = h->K[2] / 2 + 1;
+    ca.S = (T*)h->d_cgrid;
+    ca.bmod = h->d_bmod;
+    for (int k = 0; k < 9; ++k) ca.hinv[k] = bx.hinv[k];
+    ca.V = fabs(det3(bx.h));
+    ca.kappa = h->kappa;
+    ca.escale = escale;
+    ca.kind = kind;
+    ca.scal = scal_conv;
+    ca.want_energy = 1;
+    LAUNCH(h, s, KC_CONV, k_conv<T><<<nblk((int64_t)h->K[0] * h->K[1] * ca.Kh, 256), 256, 0, s>>>(ca));
+    if (sizeof(T) == 4) FFTCALL(h, s, cufftExecC2R(h->plan_b, (cufftComplex*)h->d_cgrid, (cufftReal*)h->d_grid));
+    else FFTCALL(h, s, cufftExecZ2D(h->plan_b, (cufftDoubleComplex*)h->d_cgrid, (cufftDoubleReal*)h->d_grid));
+    GatherArgs<T> ga;
+    ga.n = h->n;
+    ga.pos = pos;
+    ga.Qg = nullptr;
+    ga.U = nullptr;
+    ga.q1 = q;
+    ga.lmax = 0;
+    ga.g = g;
+    ga.phi = (const T*)h->d_grid;
+    ga.scale = 2.0 * escale;
+    ga.grad = grad;
+    ga.torque = nullptr;
+    ga.field = nullptr;
+    ga.field_accumulate = 0;
+    ga.gQ = nullptr;
+    ga.dq1 = dq;
+    ga.scal = scal_gather;
+    ga.want_box = 1;
+    ga.mode = GATHER_FULL;
+    LAUNCH(h, s, KC_GATHER_FULL, k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga));
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
+template <typename T>
+__global__ void k_disp_finalize(int n, const T* glr, const T* gsr, const double* gd, double* flr, double* fsr) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= 3 * n) return;
+    if (flr) flr[k] = -((double)glr[k] + gd[k]);
+    if (fsr) fsr[k] = gsr ? -(double)gsr[k] : 0.0;
+}
+
+// box gradient of the reciprocal part: -E h^-T - 2 h^-T Tkk - h^-T X^T NA
+void recip_box_grad(const Box& bx, const int K[3], const double* conv, const double* X, double* out) {
+    const double* hi = bx.hinv;
+    const double E = conv[0];
+    const double* t = conv + 1;
+    const double Tkk[9] = {t[0], t[3], t[4], t[3], t[1], t[5], t[4], t[5], t[2]};
+    const MeshGeom g = mesh_geom(bx, K);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            double v = -E * hi[3 * b + a];
+            double s2 = 0.0, s3 = 0.0;
+            for (int k = 0; k < 3; ++k) s2 += hi[3 * k + a] * Tkk[3 * k + b];
+            for (int k = 0; k < 3; ++k)
+                for (int j = 0; j < 3; ++j) s3 += hi[3 * k + a] * X[3 * j + k] * g.NA[3 * j + b];
+            out[3 * a + b] += v - 2.0 * s2 - s3;
+        }
+}
+
+template <typename T>
+int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const double* box, const int32_t* pairs,
+                      int64_t npairs, double* f_lr, double* f_sr, dmffb_disp_result* res) {
+    if (!h->params_set) return fail(h, DMFFB_BAD_ARG, "dmffb_disp_set_params was not called");
+    Box bx;
+    make_box(box, bx);
+    memset(res, 0, sizeof(*res));
+    const int n = h->n;
+    int st;
+    if (!pairs) {
+        if (!h->have_pairs)
+            if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        pairs = h->d_pairs;
+        npairs = h->npairs;
+    }
+    res->n_pairs = npairs;
+    CK(cudaMemsetAsync(h->d_scal, 0, N_SCAL * sizeof(double), s));
+    CK(cudaMemsetAsync(h->d_glr, 0, (size_t)3 * n * sizeof(T), s));
+    CK(cudaMemsetAsync(h->d_gsr, 0, (size_t)3 * n * sizeof(T), s));
+    CK(cudaMemsetAsync(h->d_grad, 0, (size_t)3 * n * sizeof(double), s));
+    CK(cudaMemsetAsync(h->d_dc, 0, (size_t)3 * n * sizeof(double), s));
+    DispArgs<T> a;
+    a.n = n;
+    a.npairs = npairs;
+    a.pairs = pairs;
+    a.pos = pos;
+    a.c = (const T*)h->d_c;
+    a.a = (const T*)h->d_tta;
+    a.b = (const T*)h->d_ttb;
+    a.q = (const T*)h->d_ttq;
+    for (int k = 0; k < 6; ++k) a.ms[k] = (T)h->ms[k];
+    a.kappa = (T)h->kappa;
+    a.pmax = h->pmax;
+    a.boxd = bx;
+    a.grad_lr = (T*)h->d_glr;
+    a.grad_sr = (T*)h->d_gsr;
+    a.scal = h->d_scal;  // [0] E_lr real [1] E_sr [2..10] box lr [11..19] box sr
+    if (npairs > 0) {
+        const unsigned nbk = nblk(npairs, 128);
+        if (sizeof(T) == 4) {
+            if (h->tt) {
+                LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 1, true><<<nbk, 128, 0, s>>>(a));
+                LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, true><<<nbk, 128, 0, s>>>(a));
+            } else {
+                LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 1, false><<<nbk, 128, 0, s>>>(a));
+                LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, false><<<nbk, 128, 0, s>>>(a));
+            }
+        } else {
+            if (h->tt) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 0, true><<<nbk, 128, 0, s>>>(a));
+            else LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 0, false><<<nbk, 128, 0, s>>>(a));
+        }
+        CK(cudaGetLastError());
+    }
+    const int npass = h->pmax >= 10 ? 3 : (h->pmax >= 8 ? 2 : 1);
+    if (h->lpme && h->have_plans) {
+        const int kinds[3] = {CK_DISP6, CK_DISP8, CK_DISP10};
+        for (int k = 0; k < npass; ++k) {
+            if ((st = recip_pass_channel<T>(h, s, pos, bx, (const T*)h->d_c + (size_t)k * n, kinds[k], 1.0, h->d_grad,
+                                            h->d_dc + (size_t)k * n, h->d_scal + 24, h->d_scal + 32)))
+                return st;
+        }
+    }
+    LAUNCH(h, s, KC_VEC, k_disp_finalize<T><<<nblk(3 * n, 256), 256, 0, s>>>(
+                             n, (const T*)h->d_glr, h->tt ? (const T*)h->d_gsr : nullptr, h->d_grad, f_lr, f_sr));
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    prof_collect(h);
+    const double* sc = h->h_scal;
+    res->e_real = sc[0];
+    res->e_sr = sc[1];
+    res->e_recip = (h->lpme && h->have_plans) ? sc[24] : 0.0;
+    res->e_self = h->lpme ? h->e_self_disp : 0.0;
+    res->energy = res->e_real + res->e_recip + res->e_self;
+    for (int k = 0; k < 9; ++k) {
+        res->box_grad[k] = sc[2 + k];
+        res->box_grad_sr[k] = sc[11 + k];
+    }
+    if (h->lpme && h->have_plans) recip_box_grad(bx, h->K, sc + 24, sc + 33, res->box_grad);
+    if (!std::isfinite(res->energy) || !std::isfinite(res->e_sr)) return fail(h, DMFFB_NONFINITE, "non-finite energy");
+    return DMFFB_OK;
+}
+
+template <typename T>
+__global__ void k_to_t(int m, const double* src, T* dst) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) dst[k] = (T)src[k];
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -964,6 +1149,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
                     h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_mvz, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
                     h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
+                    h->d_c, h->d_tta, h->d_ttb, h->d_ttq, h->d_glr, h->d_gsr, h->d_dc,
                     h->d_cub};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1318,6 +1504,97 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     h->npairs = tot[0];
     h->have_pairs = true;
     h->csr_from_build = true;
+    return DMFFB_OK;
+}
+
+int dmffb_disp_create(const dmffb_disp_desc* d, dmffb_engine** out) {
+    if (!d || !out) return DMFFB_BAD_ARG;
+    *out = nullptr;
+    if (d->n_atoms <= 0 || (d->pmax != 6 && d->pmax != 8 && d->pmax != 10)) return DMFFB_BAD_ARG;
+    dmffb_admp_desc a;
+    memset(&a, 0, sizeof(a));
+    a.n_atoms = d->n_atoms;
+    a.lmax = 0;
+    a.lpol = 0;
+    a.lpme = d->lpme;
+    a.precision = d->precision;
+    a.rc = d->rc;
+    a.kappa = d->kappa;
+    for (int k = 0; k < 3; ++k) a.K[k] = d->K[k];
+    a.n_cov = d->n_cov;
+    a.cov_rows = d->cov_rows;
+    for (int k = 0; k < 6; ++k) a.mscales[k] = a.pscales[k] = a.dscales[k] = d->mscales[k];
+    a.cg_tol = 1e-6;
+    a.max_iter = 1;
+    int st = dmffb_admp_create(&a, out);
+    dmffb_engine* h = *out;
+    if (st) return st;
+    h->kind = 1;
+    h->pmax = d->pmax;
+    h->tt = d->tt_damping ? 1 : 0;
+    const int n = h->n;
+    const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
+    if ((st = dalloc(h, &h->d_c, 3 * n * ts)) || (st = dalloc(h, &h->d_tta, n * ts)) ||
+        (st = dalloc(h, &h->d_ttb, n * ts)) || (st = dalloc(h, &h->d_ttq, n * ts)) || (st = dalloc(h, &h->d_glr, 3 * n * ts)) ||
+        (st = dalloc(h, &h->d_gsr, 3 * n * ts)) || (st = dalloc(h, &h->d_dc, 3 * n * sizeof(double))))
+        return st;
+    return DMFFB_OK;
+}
+
+int dmffb_disp_set_params(dmffb_engine* h, const double* c_list, const double* a, const double* b, const double* q) {
+    if (!h || h->kind != 1 || !c_list) return fail(h, DMFFB_BAD_ARG, "dispersion engine and c_list required");
+    if (h->tt && (!a || !b || !q)) return fail(h, DMFFB_BAD_ARG, "TT damping needs a, b, q");
+    const int n = h->n;
+    // host: channel-major copy and the self energy (disp_pme.py:264-289)
+    std::vector<double> cm(3 * n);
+    double s6 = 0, s8 = 0, s10 = 0;
+    for (int i = 0; i < n; ++i) {
+        for (int k = 0; k < 3; ++k) cm[(size_t)k * n + i] = c_list[3 * i + k];
+        s6 += c_list[3 * i] * c_list[3 * i];
+        s8 += c_list[3 * i + 1] * c_list[3 * i + 1];
+        s10 += c_list[3 * i + 2] * c_list[3 * i + 2];
+    }
+    const double k2 = h->kappa * h->kappa;
+    double e = -k2 * k2 * k2 / 12.0 * s6;
+    if (h->pmax >= 8) e -= k2 * k2 * k2 * k2 / 48.0 * s8;
+    if (h->pmax >= 10) e -= k2 * k2 * k2 * k2 * k2 / 240.0 * s10;
+    h->e_self_disp = e;
+    double* tmp = nullptr;
+    CK(cudaMalloc((void**)&tmp, 3 * n * sizeof(double)));
+    auto up = [&](const double* src, int m, void* dst) -> int {
+        CK(cudaMemcpy(tmp, src, m * sizeof(double), cudaMemcpyHostToDevice));
+        if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256>>>(m, tmp, (float*)dst);
+        else k_to_t<double><<<nblk(m, 256), 256>>>(m, tmp, (double*)dst);
+        CK(cudaDeviceSynchronize());
+        return DMFFB_OK;
+    };
+    int st = up(cm.data(), 3 * n, h->d_c);
+    if (!st && h->tt) st = up(a, n, h->d_tta);
+    if (!st && h->tt) st = up(b, n, h->d_ttb);
+    if (!st && h->tt) st = up(q, n, h->d_ttq);
+    cudaFree(tmp);
+    if (st) return st;
+    h->params_set = true;
+    return DMFFB_OK;
+}
+
+int dmffb_disp_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                       int64_t npairs, double* forces_lr, double* forces_sr, dmffb_disp_result* result) {
+    if (!h || h->kind != 1 || !pos || !box || !result) return fail(h, DMFFB_BAD_ARG, "bad arguments");
+    cudaStream_t caller = (cudaStream_t)stream;
+    CK(cudaEventRecord(h->e_in, caller));
+    CK(cudaStreamWaitEvent(h->s1, h->e_in, 0));
+    int st = h->prec == DMFFB_FP32 ? disp_compute_impl<float>(h, h->s1, pos, box, pairs, npairs, forces_lr, forces_sr, result)
+                                   : disp_compute_impl<double>(h, h->s1, pos, box, pairs, npairs, forces_lr, forces_sr, result);
+    cudaEventRecord(h->e_out, h->s1);
+    cudaStreamWaitEvent(caller, h->e_out, 0);
+    return st;
+}
+
+int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc) {
+    (void)stream;
+    if (!h || h->kind != 1 || !dE_dc) return fail(h, DMFFB_BAD_ARG, "bad arguments");
+    CK(cudaMemcpy(dE_dc, h->d_dc, 3 * h->n * sizeof(double), cudaMemcpyDeviceToDevice));
     return DMFFB_OK;
 }
 

@@ -220,3 +220,77 @@ class AdmpEngine:
         arr = (ctypes.c_double * 6)()
         self.lib.dmffb_get_timings(self.h, arr, 6)
         return list(arr)
+
+
+class DispEngine:
+    """Dispersion PME (C6/C8/C10, dmff/admp/disp_pme.py) with optional Tang-Toennies short range
+    (ADMPDispForce, dmff/admp/pairwise.py:100-118) on one GPU."""
+
+    def __init__(self, n_atoms, pmax, lpme, rc, kappa, K, cov_rows, mscales, tt=False, precision="fp32",
+                 device=None):
+        self.lib = L.load()
+        self.n = int(n_atoms)
+        self.tt = bool(tt)
+        self.mscales = tuple(float(x) for x in mscales)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        d = L.DispDesc()
+        d.n_atoms = self.n
+        d.pmax = int(pmax)
+        d.lpme = int(bool(lpme))
+        d.precision = _PREC[precision]
+        d.rc = float(rc)
+        d.kappa = float(kappa) if lpme else 0.0
+        for k in range(3):
+            d.K[k] = int(K[k]) if lpme else 0
+        cov = _i32(cov_rows if cov_rows is not None else np.zeros((0, 3)), (-1,))
+        self._keep = cov
+        d.n_cov = cov.size // 3
+        d.cov_rows = _ptr(cov)
+        for k in range(6):
+            d.mscales[k] = self.mscales[k]
+        d.tt_damping = int(self.tt)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = self.lib.dmffb_disp_create(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if st != L.DMFFB_OK:
+            msg = self.lib.dmffb_last_error(h).decode() if h.value else "invalid description"
+            if h.value:
+                self.lib.dmffb_destroy(h)
+            self.h = None
+            raise L.EngineError(st, msg)
+        self.f_lr = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+        self.f_sr = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+
+    __del__ = AdmpEngine.__del__
+    _check = AdmpEngine._check
+    _box = staticmethod(AdmpEngine._box)
+    rebuild_internal_pairs = AdmpEngine.rebuild_internal_pairs
+    build_neighbors = AdmpEngine.build_neighbors
+    set_profiling = AdmpEngine.set_profiling
+    kernel_stats = AdmpEngine.kernel_stats
+
+    def set_params(self, c_list, a=None, b=None, q=None):
+        host = lambda x: None if x is None else np.ascontiguousarray(
+            np.asarray(x.detach().cpu() if torch.is_tensor(x) else x, np.float64))
+        c, a, b, q = host(c_list), host(a), host(b), host(q)
+        ptr = lambda x: None if x is None else x.ctypes.data_as(ctypes.c_void_p)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.dmffb_disp_set_params(self.h, ptr(c), ptr(a), ptr(b), ptr(q)))
+
+    def compute(self, pos, box, pairs=None):
+        """Returns (result, (forces_lr, forces_sr)); forces = -dE/dpos of E_lr and E_sr."""
+        assert pos.is_cuda and pos.dtype == torch.float64 and pos.is_contiguous()
+        b = self._box(box)
+        res = L.DispResult()
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_disp_compute(
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p), _dev(pairs),
+            0 if pairs is None else pairs.shape[0], _dev(self.f_lr), _dev(self.f_sr), ctypes.byref(res)))
+        return res, (self.f_lr, self.f_sr)
+
+    def param_grads(self):
+        out = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_disp_param_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out)))
+        return out.reshape(3, self.n).T

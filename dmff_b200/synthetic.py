@@ -191,3 +191,18 @@ def pairs_nbond(pairs, cov_rows, n_atoms):
         hit = key[pos] == q
         out[hit] = nb[pos[hit]]
     return out
+
+
+def disp_params(n_waters, seed=2, b_per_A=3.5):
+    """Dispersion / Tang-Toennies parameters of the differentiation workload: per-type C6, C8, C10
+    log-normal (sigma 0.5) around 1e-3, 1e-4, 1e-5 kJ/mol nm^n; TT b = 3.5 / A (B = 35 / nm);
+    A and Q of the reference's water force field (examples/water_fullpol/forcefield.xml)."""
+    rng = np.random.default_rng(seed)
+    C = np.stack([np.exp(rng.normal(np.log(m), 0.5, size=2)) for m in (1e-3, 1e-4, 1e-5)], axis=1)  # [type, 3]
+    types = np.tile([0, 1, 1], n_waters)
+    Ct = C[types]
+    c_list = np.sqrt(Ct * np.array([1e6, 1e8, 1e10]))
+    A = np.array([1203470.743, 83.2283563])[types] / 2625.5
+    B = np.full(len(types), b_per_A * 10.0 * 0.0529177249)
+    Q = np.array([-0.741706, 0.370853])[types]
+    return dict(C_type=C, c_list=c_list, a=A, b=B, q=Q, mscales=np.array([0.0, 0.0, 0.0, 1.0, 1.0, 1.0]))

@@ -138,6 +138,44 @@ int dmffb_get_kernel_stats(const dmffb_engine* h, double* ms_out, int64_t* launc
 /* [0] launches of this library's kernels since create, [1] cuFFT executions. */
 int dmffb_get_counters(const dmffb_engine* h, int64_t* out, int32_t n);
 
+/* ---------------------------------------------------------------------------------------
+ * Dispersion PME with optional Tang-Toennies short range.
+ * dmffb_disp_create replaces ADMPDispPmeForce.__init__ (dmff/admp/disp_pme.py:21-40) plus the
+ * pairwise TT set-up of ADMPDispGenerator.createPotential (dmff/generators/admp.py:150-174). */
+typedef struct {
+    int32_t n_atoms;
+    int32_t pmax;             /* 6, 8 or 10 */
+    int32_t lpme;             /* 0: kappa = 0, no reciprocal part */
+    int32_t precision;        /* DMFFB_FP32 | DMFFB_FP64 */
+    double rc, kappa;         /* Angstrom, 1/Angstrom */
+    int32_t K[3];
+    int64_t n_cov;
+    const int32_t* cov_rows;  /* host [n_cov*3] (i, j, nbond), i < j */
+    double mscales[6];        /* nbond-1 indexed, [5] = 1.0 */
+    int32_t tt_damping;       /* 1: also evaluate ADMPDispForce's E_sr (pairwise.py:100-118) */
+} dmffb_disp_desc;
+
+typedef struct {
+    double energy;            /* E_lr = real + recip + self (disp_pme.py:80-130), kJ/mol */
+    double e_real, e_recip, e_self;
+    double e_sr;              /* TT short range (0 unless tt_damping) */
+    double box_grad[9];       /* dE_lr/dbox */
+    double box_grad_sr[9];    /* dE_sr/dbox */
+    int64_t n_pairs;
+} dmffb_disp_result;
+
+int dmffb_disp_create(const dmffb_disp_desc* desc, dmffb_engine** out);
+/* c_list host [n*3] = sqrt(C6 1e6), sqrt(C8 1e8), sqrt(C10 1e10) (admp.py:373-378); a, b, q host [n]
+ * (A/2625.5, B*0.0529177249, Q; admp.py:187-193), NULL without TT.  ADMPDispPmeForce.get_energy
+ * argument c_list (disp_pme.py:45-49). */
+int dmffb_disp_set_params(dmffb_engine* h, const double* c_list, const double* a, const double* b, const double* q);
+/* forces_lr = -dE_lr/dpos, forces_sr = -dE_sr/dpos (device [n*3], either may be NULL);
+ * pairs as in dmffb_admp_compute (NULL: the engine's own neighbour list). */
+int dmffb_disp_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                       int64_t npairs, double* forces_lr, double* forces_sr, dmffb_disp_result* result);
+/* reciprocal-space dE_lr/dc (device [3n], channel-major) of the last compute, for parameter gradients */
+int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc);
+
 /* Neighbour-list build that allocates no device memory.  No counterpart in the reference (DMFF
  * has no C ABI); same result as dmffb_build_neighbors for callers that cannot allocate on
  * demand: a host (an MD platform such as an OpenMM context, a framework with a caching

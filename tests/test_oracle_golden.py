@@ -154,3 +154,25 @@ def test_kat_dimer_neighbour_count():
     pdb = PDBFile(_data("water_dimer.pdb"))
     pr = R.brute_force_pairs(pdb.positions * 10, pdb.topology.getPeriodicBoxVectors() * 10, KATS["nblist"]["dimer_rc_A"])
     assert len(pr) == KATS["nblist"]["npairs"]
+
+
+@pytest.mark.slow
+def test_waterbox_996_dispersion_golden():
+    """ADMPDispForce (TT short range minus dispersion PME) on examples/water_fullpol: the reference's
+    two runs of this system report 35247.137 and 35247.438; within 3e-5 of the first."""
+    top, pos, box = _waterbox_topology()
+    H = Hamiltonian(_data("waterbox_forcefield.xml"))
+    pot = H.createPotential(top, nonbondedMethod="PME", nonbondedCutoff=0.6, ethresh=5e-4)
+    g = H.generators["ADMPDispForce"]
+    p = H.paramset["ADMPDispForce"]
+    mt = torch.as_tensor(pot.meta["ADMPDispForce_map_atomtype"])
+    a, b, q = p["A"][mt] / 2625.5, p["B"][mt] * 0.0529177249, p["Q"][mt]
+    c = torch.stack([torch.sqrt(p["C6"][mt] * 1e6), torch.sqrt(p["C8"][mt] * 1e8), torch.sqrt(p["C10"][mt] * 1e10)], 1)
+    cov = top.buildCovMat()
+    posA, boxA = torch.tensor(pos * 10), torch.tensor(box * 10)
+    pr = R.brute_force_pairs(posA.numpy(), boxA.numpy(), 6.0, lambda i, j: int(cov.lookup(i, j)))
+    ms = torch.tensor(g.mScales)
+    Esr = R.pairwise_energy(R.TT_damping_qq_c6_kernel, posA, boxA, pr, ms, a, b, q, c[:, 0])
+    Elr = R.ADMPDispPmeForce(boxA.numpy(), 6.0, 5e-4, 10).get_energy(posA, boxA, pr, c, ms)
+    gold = GOLD["waterbox996_disp_damp"]["value"]
+    assert abs((Esr - Elr).item() - gold) <= 3e-5 * abs(gold)
