@@ -32,7 +32,17 @@ EXPORTED = [
     "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
     "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters", "dmffb_build_neighbors_noalloc",
     "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads",
+    "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
+    "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
 ]
+
+DMFFB_COUL_NONE = 0
+DMFFB_COUL_PME = 1
+DMFFB_COUL_RF = 2
+DMFFB_COUL_NOCUTOFF = 3
+DMFFB_TERM_BOND = 0
+DMFFB_TERM_ANGLE = 1
+DMFFB_TERM_TORSION = 2
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
                   "gather_field", "self_frames", "vector", "neighbors"]
@@ -106,6 +116,39 @@ class DispResult(ctypes.Structure):
     ]
 
 
+class ClassicalDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int32),
+        ("n_types", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("coulomb", ctypes.c_int32),
+        ("pbc", ctypes.c_int32),
+        ("rc", ctypes.c_double),
+        ("kappa", ctypes.c_double),
+        ("K", ctypes.c_int32 * 3),
+        ("eps_solvent", ctypes.c_double),
+        ("n_cov", ctypes.c_int64),
+        ("cov_rows", ctypes.POINTER(ctypes.c_int32)),
+        ("mscales_coul", ctypes.c_double * 6),
+        ("mscales_lj", ctypes.c_double * 6),
+    ]
+
+
+class ClassicalResult(ctypes.Structure):
+    _fields_ = [
+        ("energy", ctypes.c_double),
+        ("e_coul_real", ctypes.c_double),
+        ("e_coul_recip", ctypes.c_double),
+        ("e_coul_self", ctypes.c_double),
+        ("e_lj", ctypes.c_double),
+        ("e_bond", ctypes.c_double),
+        ("e_angle", ctypes.c_double),
+        ("e_torsion", ctypes.c_double),
+        ("box_grad", ctypes.c_double * 9),
+        ("n_pairs", ctypes.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -142,6 +185,12 @@ def load():
     lib.dmffb_disp_set_params.argtypes = [vp, vp, vp, vp, vp]
     lib.dmffb_disp_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp, P(DispResult)]
     lib.dmffb_disp_param_grads.argtypes = [vp, vp, vp]
+    lib.dmffb_classical_create.argtypes = [P(ClassicalDesc), P(vp)]
+    lib.dmffb_classical_set_params.argtypes = [vp, vp, vp, vp, vp]
+    lib.dmffb_classical_set_terms.argtypes = [vp, i32, i64, vp, vp]
+    lib.dmffb_classical_set_param_grads.argtypes = [vp, i32]
+    lib.dmffb_classical_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, P(ClassicalResult)]
+    lib.dmffb_classical_param_grads.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     for name in EXPORTED:
         if name not in ("dmffb_destroy", "dmffb_last_error"):
             getattr(lib, name).restype = ctypes.c_int

@@ -187,7 +187,9 @@ class DMFFTopology:
                 a = by_name.get(p["name"])
                 if a is None:
                     continue
-                a.meta["type"] = p["type"]
+                for k, v in p.items():  # type plus per-atom attributes such as charge
+                    if k != "name":
+                        a.meta[k] = v
                 a.meta["class"] = type2class.get(p["type"])
             if not any(have_bond[a.index] for a in res._atoms):
                 for b in tpl["bonds"]:
@@ -202,9 +204,16 @@ class DMFFTopology:
         return self
 
 
+# water residue / atom name variants that OpenMM's PDB reader maps to the HOH template
+_WATER_RES = {"HOH", "WAT", "SOL", "H2O", "TIP3", "TIP", "T3P", "TP3", "SPC"}
+_WATER_ATOM = {"OW": "O", "OH2": "O", "HW1": "H1", "HW2": "H2"}
+
+
 class PDBFile:
-    """Minimal PDB reader: ATOM/HETATM records (name, residue, element), CRYST1 box.
-    ``positions`` are in nm (numpy [N,3]); ``topology`` is a DMFFTopology."""
+    """Minimal PDB reader: ATOM/HETATM records (name, residue, element), CRYST1 box and CONECT
+    bonds (deduplicated).  Water residues named SOL/WAT/H2O/TIP3... become HOH with atoms O, H1, H2,
+    as OpenMM's reader renames them.  ``positions`` are in nm (numpy [N,3]); ``topology`` is a
+    DMFFTopology."""
 
     def __init__(self, path):
         top = DMFFTopology()
@@ -212,6 +221,8 @@ class PDBFile:
         box = None
         last_key = None
         res = None
+        serial = {}
+        conect = []
         for line in open(path):
             if line.startswith("CRYST1"):
                 a, b, c = float(line[6:15]), float(line[15:24]), float(line[24:33])
@@ -219,13 +230,31 @@ class PDBFile:
             elif line.startswith(("ATOM", "HETATM")):
                 name = line[12:16].strip()
                 resname = line[17:20].strip()
+                if resname in _WATER_RES:
+                    resname = "HOH"
+                    name = _WATER_ATOM.get(name, name)
                 key = (line[21], line[22:27])
                 if key != last_key:
                     res = top.addResidue(resname)
                     last_key = key
                 elem = line[76:78].strip() or name[0]
-                top.addAtom(name, elem, res)
+                atom = top.addAtom(name, elem, res)
+                try:
+                    serial[int(line[6:11])] = atom.index
+                except ValueError:
+                    pass
                 pos.append([float(line[30:38]), float(line[38:46]), float(line[46:54])])
+            elif line.startswith("CONECT"):
+                fields = [line[k:k + 5] for k in range(6, len(line.rstrip()), 5)]
+                ids = [int(f) for f in fields if f.strip().isdigit()]
+                conect += [(ids[0], o) for o in ids[1:]]
+        seen = set()
+        for a, b in conect:
+            if a in serial and b in serial and a != b:
+                i, j = serial[a], serial[b]
+                if (min(i, j), max(i, j)) not in seen:
+                    seen.add((min(i, j), max(i, j)))
+                    top.addBond(i, j)
         top.setPeriodicBoxVectors(box)
         self.topology = top
         self.positions = np.asarray(pos, dtype=np.float64) / 10.0

@@ -14,6 +14,8 @@ namespace dmffb {
 // ------------------------------------------------------------------ math wrappers
 __device__ __forceinline__ float d_erfc(float x) { return erfcf(x); }
 __device__ __forceinline__ double d_erfc(double x) { return erfc(x); }
+__device__ __forceinline__ float d_erf(float x) { return erff(x); }
+__device__ __forceinline__ double d_erf(double x) { return erf(x); }
 __device__ __forceinline__ float d_exp(float x) { return expf(x); }
 __device__ __forceinline__ double d_exp(double x) { return exp(x); }
 __device__ __forceinline__ float d_sqrt(float x) { return sqrtf(x); }

@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "nblist.cuh"
 #include "disp.cuh"
+#include "classical.cuh"
 
 using namespace dmffb;
 
@@ -124,6 +125,20 @@ struct dmffb_engine {
     void *d_glr = nullptr, *d_gsr = nullptr;
     double* d_dc = nullptr;  // [3n] dE_lr/dc per channel (reciprocal part)
     double e_self_disp = 0.0;
+    // ---- classical terms (engines made by dmffb_classical_create, kind 2)
+    int ntypes = 0, coul = 0, pbc = 1;
+    double krf = 0.0, crf = 0.0, e_self_coul = 0.0;
+    double mlj[6] = {0, 0, 0, 0, 0, 0};
+    double* d_q = nullptr;       // [n] FP64 charges
+    void* d_qT = nullptr;        // [n] charges in kernel precision
+    int32_t* d_type = nullptr;   // [n]
+    void *d_sigtt = nullptr, *d_epstt = nullptr;  // [ntypes^2] kernel precision
+    double *d_dq = nullptr, *d_dsig = nullptr, *d_deps = nullptr;
+    int64_t nterm[3] = {0, 0, 0};
+    int32_t* d_tidx[3] = {nullptr, nullptr, nullptr};
+    double* d_tprm[3] = {nullptr, nullptr, nullptr};
+    double* d_tdprm[3] = {nullptr, nullptr, nullptr};
+    bool want_pgrad = false, charges_set = false;
 };
 
 namespace {
@@ -979,6 +994,124 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
     return DMFFB_OK;
 }
 
+// dE/dq of the Ewald self term, -2 D kappa / sqrt(pi) q_i (pme.py:1183-1222 at lmax 0)
+__global__ void k_self_dq(int n, const double* q, double c, double* dq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dq[i] += c * q[i];
+}
+
+template <typename T>
+int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const double* box,
+                           const int32_t* pairs, int64_t npairs, double* forces, dmffb_classical_result* res) {
+    const bool nonbonded = h->coul != COUL_NONE || h->ntypes > 0;
+    if (nonbonded && !h->params_set) return fail(h, DMFFB_BAD_ARG, "dmffb_classical_set_params was not called");
+    Box bx;
+    make_box(box, bx);
+    memset(res, 0, sizeof(*res));
+    const int n = h->n;
+    int st;
+    if (nonbonded && !pairs) {
+        if (!h->have_pairs)
+            if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        pairs = h->d_pairs;
+        npairs = h->npairs;
+    }
+    if (!nonbonded) npairs = 0;
+    res->n_pairs = npairs;
+    const bool pg = h->want_pgrad;
+    CK(cudaMemsetAsync(h->d_scal, 0, N_SCAL * sizeof(double), s));
+    CK(cudaMemsetAsync(h->d_glr, 0, (size_t)3 * n * sizeof(T), s));
+    CK(cudaMemsetAsync(h->d_grad, 0, (size_t)3 * n * sizeof(double), s));
+    if (pg) {
+        CK(cudaMemsetAsync(h->d_dq, 0, (size_t)n * sizeof(double), s));
+        if (h->ntypes > 0) {
+            CK(cudaMemsetAsync(h->d_dsig, 0, (size_t)h->ntypes * h->ntypes * sizeof(double), s));
+            CK(cudaMemsetAsync(h->d_deps, 0, (size_t)h->ntypes * h->ntypes * sizeof(double), s));
+        }
+    }
+    if (npairs > 0) {
+        NbPairArgs<T> a;
+        a.n = n;
+        a.npairs = npairs;
+        a.pairs = pairs;
+        a.pos = pos;
+        a.q = h->d_q;
+        a.qT = (const T*)h->d_qT;
+        a.type = h->ntypes > 0 ? h->d_type : nullptr;
+        a.ntypes = h->ntypes;
+        a.sig_tt = (const T*)h->d_sigtt;
+        a.eps_tt = (const T*)h->d_epstt;
+        for (int k = 0; k < 6; ++k) {
+            a.mc[k] = (T)h->ms[k];
+            a.ml[k] = (T)h->mlj[k];
+        }
+        a.kappa = (T)h->kappa;
+        a.krf = (T)h->krf;
+        a.crf = (T)h->crf;
+        a.coul = h->coul;
+        a.pbc = h->pbc;
+        a.boxd = bx;
+        a.grad = (T*)h->d_glr;
+        a.dq = (pg && h->coul != COUL_NONE) ? h->d_dq : nullptr;
+        a.dsig = (pg && h->ntypes > 0) ? h->d_dsig : nullptr;
+        a.deps = (pg && h->ntypes > 0) ? h->d_deps : nullptr;
+        a.scal = h->d_scal;
+        const unsigned nbk = nblk(npairs, 128);
+        if (sizeof(T) == 4) {
+            LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 1><<<nbk, 128, 0, s>>>(a));
+            LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 2><<<nbk, 128, 0, s>>>(a));
+        } else {
+            LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 0><<<nbk, 128, 0, s>>>(a));
+        }
+        CK(cudaGetLastError());
+    }
+    const bool recip = h->coul == COUL_PME && h->lpme && h->have_plans;
+    if (recip) {
+        if ((st = recip_pass_channel<T>(h, s, pos, bx, (const T*)h->d_qT, CK_COUL, DMFFB_DIELECTRIC, h->d_grad,
+                                        pg ? h->d_dq : nullptr, h->d_scal + 24, h->d_scal + 32)))
+            return st;
+        if (pg)
+            LAUNCH(h, s, KC_SELF, k_self_dq<<<nblk(n, 256), 256, 0, s>>>(
+                                      n, h->d_q, -2.0 * DMFFB_DIELECTRIC * h->kappa / sqrt(M_PI), h->d_dq));
+    }
+    for (int kind = 0; kind < 3; ++kind) {
+        if (h->nterm[kind] <= 0) continue;
+        BondedArgs b;
+        b.nterm = (int)h->nterm[kind];
+        b.idx = h->d_tidx[kind];
+        b.prm = h->d_tprm[kind];
+        b.pos = pos;
+        b.grad = h->d_grad;
+        b.dprm = pg ? h->d_tdprm[kind] : nullptr;
+        b.scal = h->d_scal + 12 + kind;
+        const unsigned nbk = nblk(h->nterm[kind], 128);
+        if (kind == 0) LAUNCH(h, s, KC_PAIR_FULL, k_bonds<<<nbk, 128, 0, s>>>(b));
+        else if (kind == 1) LAUNCH(h, s, KC_PAIR_FULL, k_angles<<<nbk, 128, 0, s>>>(b));
+        else LAUNCH(h, s, KC_PAIR_FULL, k_torsions<<<nbk, 128, 0, s>>>(b));
+        CK(cudaGetLastError());
+    }
+    if (forces)
+        LAUNCH(h, s, KC_VEC, k_disp_finalize<T><<<nblk(3 * n, 256), 256, 0, s>>>(
+                                 n, (const T*)h->d_glr, (const T*)nullptr, h->d_grad, forces, (double*)nullptr));
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    prof_collect(h);
+    const double* sc = h->h_scal;
+    res->e_coul_real = sc[0];
+    res->e_lj = sc[1];
+    res->e_bond = sc[12];
+    res->e_angle = sc[13];
+    res->e_torsion = sc[14];
+    res->e_coul_recip = recip ? sc[24] : 0.0;
+    res->e_coul_self = (h->coul == COUL_PME && h->lpme) ? h->e_self_coul : 0.0;
+    res->energy = res->e_coul_real + res->e_coul_recip + res->e_coul_self + res->e_lj + res->e_bond + res->e_angle +
+                  res->e_torsion;
+    for (int k = 0; k < 9; ++k) res->box_grad[k] = sc[2 + k];
+    if (recip) recip_box_grad(bx, h->K, sc + 24, sc + 33, res->box_grad);
+    if (!std::isfinite(res->energy)) return fail(h, DMFFB_NONFINITE, "non-finite energy");
+    return DMFFB_OK;
+}
+
 template <typename T>
 __global__ void k_to_t(int m, const double* src, T* dst) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1150,6 +1283,9 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_mvz, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
                     h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
                     h->d_c, h->d_tta, h->d_ttb, h->d_ttq, h->d_glr, h->d_gsr, h->d_dc,
+                    h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
+                    h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
+                    h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2],
                     h->d_cub};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1595,6 +1731,150 @@ int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc) {
     (void)stream;
     if (!h || h->kind != 1 || !dE_dc) return fail(h, DMFFB_BAD_ARG, "bad arguments");
     CK(cudaMemcpy(dE_dc, h->d_dc, 3 * h->n * sizeof(double), cudaMemcpyDeviceToDevice));
+    return DMFFB_OK;
+}
+
+int dmffb_classical_create(const dmffb_classical_desc* d, dmffb_engine** out) {
+    if (!d || !out) return DMFFB_BAD_ARG;
+    *out = nullptr;
+    if (d->n_atoms <= 0 || d->n_types < 0 || d->coulomb < DMFFB_COUL_NONE || d->coulomb > DMFFB_COUL_NOCUTOFF)
+        return DMFFB_BAD_ARG;
+    if (d->coulomb == DMFFB_COUL_RF && !(d->rc > 0)) return DMFFB_BAD_ARG;
+    dmffb_admp_desc a;
+    memset(&a, 0, sizeof(a));
+    a.n_atoms = d->n_atoms;
+    a.lmax = 0;
+    a.lpol = 0;
+    a.lpme = d->coulomb == DMFFB_COUL_PME ? 1 : 0;
+    a.precision = d->precision;
+    a.rc = d->rc;
+    a.kappa = d->kappa;
+    for (int k = 0; k < 3; ++k) a.K[k] = d->K[k];
+    a.n_cov = d->n_cov;
+    a.cov_rows = d->cov_rows;
+    for (int k = 0; k < 6; ++k) a.mscales[k] = a.pscales[k] = a.dscales[k] = d->mscales_coul[k];
+    a.cg_tol = 1e-6;
+    a.max_iter = 1;
+    int st = dmffb_admp_create(&a, out);
+    dmffb_engine* h = *out;
+    if (st) return st;
+    h->kind = 2;
+    h->ntypes = d->n_types;
+    h->coul = d->coulomb;
+    h->pbc = d->pbc ? 1 : 0;
+    for (int k = 0; k < 6; ++k) h->mlj[k] = d->mscales_lj[k];
+    if (d->coulomb == DMFFB_COUL_RF) {  // inter.py:196-203
+        const double es = d->eps_solvent > 0 ? d->eps_solvent : 78.5;
+        h->krf = (1.0 / (d->rc * d->rc * d->rc)) * (es - 1.0) / (2.0 * es + 1.0);
+        h->crf = (1.0 / d->rc) * 3.0 * es / (2.0 * es + 1.0);
+    }
+    const int n = h->n;
+    const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
+    const size_t tt = (size_t)std::max(1, h->ntypes) * std::max(1, h->ntypes);
+    if ((st = dalloc(h, &h->d_q, n * sizeof(double))) || (st = dalloc(h, &h->d_qT, n * ts)) ||
+        (st = dalloc(h, &h->d_type, n * sizeof(int32_t))) || (st = dalloc(h, &h->d_sigtt, tt * ts)) ||
+        (st = dalloc(h, &h->d_epstt, tt * ts)) || (st = dalloc(h, &h->d_dq, n * sizeof(double))) ||
+        (st = dalloc(h, &h->d_dsig, tt * sizeof(double))) || (st = dalloc(h, &h->d_deps, tt * sizeof(double))) ||
+        (st = dalloc(h, &h->d_glr, 3 * n * ts)))
+        return st;
+    return DMFFB_OK;
+}
+
+int dmffb_classical_set_params(dmffb_engine* h, const double* charges, const int32_t* atom_type,
+                               const double* sigma_tt, const double* eps_tt) {
+    if (!h || h->kind != 2) return fail(h, DMFFB_BAD_ARG, "classical engine required");
+    if (h->coul != COUL_NONE && !charges) return fail(h, DMFFB_BAD_ARG, "Coulomb needs charges");
+    if (h->ntypes > 0 && (!atom_type || !sigma_tt || !eps_tt)) return fail(h, DMFFB_BAD_ARG, "LJ needs types and tables");
+    const int n = h->n;
+    const int nt = h->ntypes;
+    if (nt > 0)
+        for (int i = 0; i < n; ++i)
+            if (atom_type[i] < 0 || atom_type[i] >= nt) return fail(h, DMFFB_BAD_ARG, "atom type out of range");
+    std::vector<double> qz(n, 0.0);
+    const double* q = charges ? charges : qz.data();
+    double s2 = 0.0;
+    for (int i = 0; i < n; ++i) s2 += q[i] * q[i];
+    h->e_self_coul = -DMFFB_DIELECTRIC * h->kappa / sqrt(M_PI) * s2;  // pme.py:1183-1222, lmax 0
+    CK(cudaMemcpy(h->d_q, q, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(n, 256), 256>>>(n, h->d_q, (float*)h->d_qT);
+    else k_to_t<double><<<nblk(n, 256), 256>>>(n, h->d_q, (double*)h->d_qT);
+    if (nt > 0) {
+        CK(cudaMemcpy(h->d_type, atom_type, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        const int m = nt * nt;
+        double* tmp = nullptr;
+        CK(cudaMalloc((void**)&tmp, m * sizeof(double)));
+        for (int w = 0; w < 2; ++w) {
+            CK(cudaMemcpy(tmp, w == 0 ? sigma_tt : eps_tt, m * sizeof(double), cudaMemcpyHostToDevice));
+            void* dst = w == 0 ? h->d_sigtt : h->d_epstt;
+            if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256>>>(m, tmp, (float*)dst);
+            else k_to_t<double><<<nblk(m, 256), 256>>>(m, tmp, (double*)dst);
+            CK(cudaDeviceSynchronize());
+        }
+        cudaFree(tmp);
+    }
+    CK(cudaDeviceSynchronize());
+    h->params_set = true;
+    return DMFFB_OK;
+}
+
+int dmffb_classical_set_terms(dmffb_engine* h, int32_t kind, int64_t n_terms, const int32_t* idx, const double* prm) {
+    if (!h || h->kind != 2 || kind < 0 || kind > 2 || n_terms < 0 || (n_terms > 0 && (!idx || !prm)))
+        return fail(h, DMFFB_BAD_ARG, "bad term list");
+    if (n_terms > 0x7fffffff) return fail(h, DMFFB_BAD_ARG, "too many terms");
+    const int arity = kind + 2, np = kind == 2 ? 3 : 2;
+    for (int64_t t = 0; t < n_terms * arity; ++t)
+        if (idx[t] < 0 || idx[t] >= h->n) return fail(h, DMFFB_BAD_ARG, "term atom index out of range");
+    if (h->d_tidx[kind]) cudaFree(h->d_tidx[kind]);
+    if (h->d_tprm[kind]) cudaFree(h->d_tprm[kind]);
+    if (h->d_tdprm[kind]) cudaFree(h->d_tdprm[kind]);
+    h->d_tidx[kind] = nullptr;
+    h->d_tprm[kind] = nullptr;
+    h->d_tdprm[kind] = nullptr;
+    h->nterm[kind] = 0;
+    if (n_terms == 0) return DMFFB_OK;
+    int st;
+    if ((st = dalloc(h, &h->d_tidx[kind], n_terms * arity * sizeof(int32_t))) ||
+        (st = dalloc(h, &h->d_tprm[kind], n_terms * np * sizeof(double))) ||
+        (st = dalloc(h, &h->d_tdprm[kind], n_terms * 2 * sizeof(double))))
+        return st;
+    CK(cudaMemcpy(h->d_tidx[kind], idx, n_terms * arity * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_tprm[kind], prm, n_terms * np * sizeof(double), cudaMemcpyHostToDevice));
+    h->nterm[kind] = n_terms;
+    return DMFFB_OK;
+}
+
+int dmffb_classical_set_param_grads(dmffb_engine* h, int32_t enabled) {
+    if (!h || h->kind != 2) return fail(h, DMFFB_BAD_ARG, "classical engine required");
+    h->want_pgrad = enabled != 0;
+    return DMFFB_OK;
+}
+
+int dmffb_classical_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                            int64_t npairs, double* forces_out, dmffb_classical_result* result) {
+    if (!h || h->kind != 2 || !pos || !box || !result) return fail(h, DMFFB_BAD_ARG, "bad arguments");
+    cudaStream_t caller = (cudaStream_t)stream;
+    CK(cudaEventRecord(h->e_in, caller));
+    CK(cudaStreamWaitEvent(h->s1, h->e_in, 0));
+    int st = h->prec == DMFFB_FP32 ? classical_compute_impl<float>(h, h->s1, pos, box, pairs, npairs, forces_out, result)
+                                   : classical_compute_impl<double>(h, h->s1, pos, box, pairs, npairs, forces_out, result);
+    cudaEventRecord(h->e_out, h->s1);
+    cudaStreamWaitEvent(caller, h->e_out, 0);
+    return st;
+}
+
+int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, double* dE_dsig, double* dE_deps,
+                                double* dE_dbond, double* dE_dangle, double* dE_dtorsion) {
+    (void)stream;
+    if (!h || h->kind != 2) return fail(h, DMFFB_BAD_ARG, "classical engine required");
+    if (!h->want_pgrad) return fail(h, DMFFB_BAD_ARG, "parameter gradients are not enabled");
+    const size_t tt = (size_t)h->ntypes * h->ntypes;
+    if (dE_dq) CK(cudaMemcpy(dE_dq, h->d_dq, h->n * sizeof(double), cudaMemcpyDeviceToDevice));
+    if (dE_dsig && tt) CK(cudaMemcpy(dE_dsig, h->d_dsig, tt * sizeof(double), cudaMemcpyDeviceToDevice));
+    if (dE_deps && tt) CK(cudaMemcpy(dE_deps, h->d_deps, tt * sizeof(double), cudaMemcpyDeviceToDevice));
+    double* dst[3] = {dE_dbond, dE_dangle, dE_dtorsion};
+    for (int k = 0; k < 3; ++k)
+        if (dst[k] && h->nterm[k] > 0)
+            CK(cudaMemcpy(dst[k], h->d_tdprm[k], h->nterm[k] * 2 * sizeof(double), cudaMemcpyDeviceToDevice));
     return DMFFB_OK;
 }
 

@@ -294,3 +294,127 @@ class DispEngine:
         s = torch.cuda.current_stream(self.device)
         self._check(self.lib.dmffb_disp_param_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out)))
         return out.reshape(3, self.n).T
+
+
+_COUL = {"none": L.DMFFB_COUL_NONE, "pme": L.DMFFB_COUL_PME, "rf": L.DMFFB_COUL_RF,
+         "nocutoff": L.DMFFB_COUL_NOCUTOFF}
+_TERM = {"bond": (L.DMFFB_TERM_BOND, 2, 2), "angle": (L.DMFFB_TERM_ANGLE, 3, 2),
+         "torsion": (L.DMFFB_TERM_TORSION, 4, 3)}
+
+
+class ClassicalEngine:
+    """Classical terms on one GPU: LJ + point-charge Coulomb (``coulomb`` 'pme' | 'rf' |
+    'nocutoff' | 'none'; dmff/classical/inter.py) and harmonic bond / angle / periodic torsion
+    term lists (dmff/classical/intra.py).  Units: Angstrom, e, kJ/mol, radians.
+
+    ``n_types`` > 0 enables LJ; ``set_params`` takes per-atom charges and LJ type indices plus
+    the type-pair tables sigma_tt / eps_tt (mixing and NBFix applied by the caller)."""
+
+    def __init__(self, n_atoms, n_types=0, coulomb="none", pbc=True, rc=10.0, kappa=0.0, K=(0, 0, 0),
+                 cov_rows=None, mscales_coul=(0, 0, 0, 1, 1, 1), mscales_lj=(0, 0, 0, 1, 1, 1),
+                 eps_solvent=78.5, precision="fp32", device=None):
+        self.lib = L.load()
+        self.n = int(n_atoms)
+        self.n_types = int(n_types)
+        self.coulomb = coulomb
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        d = L.ClassicalDesc()
+        d.n_atoms = self.n
+        d.n_types = self.n_types
+        d.precision = _PREC[precision]
+        d.coulomb = _COUL[coulomb]
+        d.pbc = int(bool(pbc))
+        d.rc = float(rc)
+        d.kappa = float(kappa) if coulomb == "pme" else 0.0
+        for k in range(3):
+            d.K[k] = int(K[k]) if coulomb == "pme" else 0
+        d.eps_solvent = float(eps_solvent)
+        cov = _i32(cov_rows if cov_rows is not None else np.zeros((0, 3)), (-1,))
+        self._keep = cov
+        d.n_cov = cov.size // 3
+        d.cov_rows = _ptr(cov)
+        for k in range(6):
+            d.mscales_coul[k] = float(mscales_coul[k])
+            d.mscales_lj[k] = float(mscales_lj[k])
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = self.lib.dmffb_classical_create(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if st != L.DMFFB_OK:
+            msg = self.lib.dmffb_last_error(h).decode() if h.value else "invalid description"
+            if h.value:
+                self.lib.dmffb_destroy(h)
+            self.h = None
+            raise L.EngineError(st, msg)
+        self.forces = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+        self.n_terms = {"bond": 0, "angle": 0, "torsion": 0}
+        self._pgrad = False
+
+    __del__ = AdmpEngine.__del__
+    _check = AdmpEngine._check
+    _box = staticmethod(AdmpEngine._box)
+    rebuild_internal_pairs = AdmpEngine.rebuild_internal_pairs
+    build_neighbors = AdmpEngine.build_neighbors
+    set_profiling = AdmpEngine.set_profiling
+    kernel_stats = AdmpEngine.kernel_stats
+    counters = AdmpEngine.counters
+
+    @staticmethod
+    def _host(x, dtype=np.float64):
+        if x is None:
+            return None
+        x = x.detach().cpu().numpy() if torch.is_tensor(x) else x
+        return np.ascontiguousarray(np.asarray(x, dtype=dtype))
+
+    def set_params(self, charges=None, atom_type=None, sigma_tt=None, eps_tt=None):
+        q, t = self._host(charges), self._host(atom_type, np.int32)
+        sg, ep = self._host(sigma_tt), self._host(eps_tt)
+        ptr = lambda x: None if x is None else x.ctypes.data_as(ctypes.c_void_p)
+        with torch.cuda.device(self.device):
+            self._check(self.lib.dmffb_classical_set_params(self.h, ptr(q), ptr(t), ptr(sg), ptr(ep)))
+
+    def set_terms(self, kind, idx, prm):
+        code, arity, npar = _TERM[kind]
+        idx = self._host(idx, np.int32).reshape(-1, arity)
+        prm = self._host(prm).reshape(-1, npar)
+        assert idx.shape[0] == prm.shape[0]
+        with torch.cuda.device(self.device):
+            self._check(self.lib.dmffb_classical_set_terms(self.h, code, idx.shape[0],
+                                                           idx.ctypes.data_as(ctypes.c_void_p),
+                                                           prm.ctypes.data_as(ctypes.c_void_p)))
+        self.n_terms[kind] = idx.shape[0]
+
+    def set_param_grads(self, on=True):
+        if bool(on) != self._pgrad:
+            self._check(self.lib.dmffb_classical_set_param_grads(self.h, int(bool(on))))
+            self._pgrad = bool(on)
+
+    def compute(self, pos, box, pairs=None):
+        """Returns (result, forces); forces = -dE/dpos (kJ/mol/A), device [n, 3] FP64."""
+        assert pos.is_cuda and pos.dtype == torch.float64 and pos.is_contiguous()
+        if pairs is not None:
+            assert pairs.is_cuda and pairs.dtype == torch.int32 and pairs.is_contiguous()
+        b = self._box(box)
+        res = L.ClassicalResult()
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_classical_compute(
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p), _dev(pairs),
+            0 if pairs is None else pairs.shape[0], _dev(self.forces), ctypes.byref(res)))
+        return res, self.forces
+
+    def param_grads(self):
+        """{'q': [n], 'sigma_tt': [T, T], 'eps_tt': [T, T], 'bond'|'angle'|'torsion': [m, 2]} of the last compute."""
+        dev = self.device
+        T = max(self.n_types, 0)
+        out = {"q": torch.empty(self.n, dtype=torch.float64, device=dev),
+               "sigma_tt": torch.empty((T, T), dtype=torch.float64, device=dev),
+               "eps_tt": torch.empty((T, T), dtype=torch.float64, device=dev)}
+        for k in ("bond", "angle", "torsion"):
+            out[k] = torch.empty((self.n_terms[k], 2), dtype=torch.float64, device=dev)
+        s = torch.cuda.current_stream(dev)
+        self._check(self.lib.dmffb_classical_param_grads(
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(out["q"]), _dev(out["sigma_tt"]) if T else None,
+            _dev(out["eps_tt"]) if T else None, _dev(out["bond"]) if self.n_terms["bond"] else None,
+            _dev(out["angle"]) if self.n_terms["angle"] else None,
+            _dev(out["torsion"]) if self.n_terms["torsion"] else None))
+        return out

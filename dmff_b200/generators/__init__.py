@@ -1,3 +1,2 @@
-"""Generator registry: importing this package registers the drop-in generator classes."""
-from . import admp  # noqa: F401
-from . import disp  # noqa: F401
+"""Generator registry: importing this package registers every force-field generator by XML tag."""
+from . import admp, classical, disp  # noqa: F401

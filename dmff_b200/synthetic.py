@@ -206,3 +206,91 @@ def disp_params(n_waters, seed=2, b_per_A=3.5):
     B = np.full(len(types), b_per_A * 10.0 * 0.0529177249)
     Q = np.array([-0.741706, 0.370853])[types]
     return dict(C_type=C, c_list=c_list, a=A, b=B, q=Q, mscales=np.array([0.0, 0.0, 0.0, 1.0, 1.0, 1.0]))
+
+
+def _chain_walk(rng, n_beads, start, bond=1.53, ang=(100.0, 120.0), min_dist=3.0, max_tries=200):
+    """Random-walk chain: bond length ``bond``, bond angles U(ang), uniform dihedrals; a new bead is
+    redrawn while it sits within ``min_dist`` of a bead three or more places back."""
+    pos = [np.asarray(start, dtype=np.float64)]
+    d = rng.normal(size=3)
+    pos.append(pos[0] + bond * d / np.linalg.norm(d))
+    for k in range(2, n_beads):
+        best, best_d = None, -1.0
+        for _ in range(max_tries):
+            a, b = pos[k - 1], pos[k - 2]
+            u = (b - a) / np.linalg.norm(b - a)
+            th = math.radians(rng.uniform(*ang))
+            ph = rng.uniform(0, 2 * math.pi)
+            t = rng.normal(size=3)
+            t -= t.dot(u) * u
+            t /= np.linalg.norm(t)
+            w = np.cross(u, t)
+            v = math.cos(th) * u + math.sin(th) * (math.cos(ph) * t + math.sin(ph) * w)
+            p = a + bond * v
+            dmin = min([np.linalg.norm(p - q) for q in pos[:k - 2]], default=1e9)
+            if dmin > best_d:
+                best, best_d = p, dmin
+            if dmin >= min_dist:
+                break
+        pos.append(best)
+    return np.array(pos)
+
+
+def polymer_water_box(n_chains, n_beads, n_waters, L, seed=4, rc=10.0, ethresh=1e-5):
+    """Classical polymer + water system (positions / box in Angstrom, kJ/mol).
+
+    ``n_chains`` linear chains of ``n_beads`` beads (random walk: bonds 1.53 A, angles U(100, 120) deg,
+    redrawn within 3 A of earlier beads), bead charges N(0, 0.3 e) shifted to zero net charge per
+    chain, one LJ type per chain position with sigma U(3.0, 3.8) A and eps U(0.2, 0.8) kJ/mol;
+    harmonic bonds (k 2000 kJ/mol/A^2, r0 U(1.48, 1.58) A), angles (k 400 kJ/mol/rad^2, theta0 110 deg) and
+    3-term periodic torsions (n = 1, 2, 3; k U(0.5, 2) kJ/mol, phase 0 or pi).  Waters: point
+    charges O -0.834 / H +0.417 (O-H 0.9572 A, H-O-H 104.52 deg) on a seeded subset of an m^3
+    lattice with random orientations, O LJ sigma 3.15061 A / eps 0.6364 kJ/mol, H none.  Atom order:
+    chains first, then waters (O, H1, H2).  Covalent map from the bonds (chains: path lengths up to
+    6; waters: O-H 1, H-H 2).  Coulomb PME kappa / K from ethresh by the reference's 'openmm'
+    formula; scales 1-4: LJ 0.5, Coulomb 0.8333 (0 for 1-2, 1-3)."""
+    from .api.topology import covalent_rows
+    rng = np.random.default_rng(seed)
+    nb = n_chains * n_beads
+    chains = [_chain_walk(rng, n_beads, rng.uniform(0, L, size=3)) for _ in range(n_chains)]
+    wpos = water_positions(n_waters, L, rng, min_inter=None) if n_waters else np.zeros((0, 3))
+    pos = np.concatenate(chains + [wpos]) if n_chains else wpos
+    n = nb + 3 * n_waters
+    q = []
+    for _ in range(n_chains):
+        c = rng.normal(0.0, 0.3, size=n_beads)
+        q.append(c - c.mean())
+    q = np.concatenate(q + [np.tile([-0.834, 0.417, 0.417], n_waters)])
+    sig_b = rng.uniform(3.0, 3.8, size=n_beads)
+    eps_b = rng.uniform(0.2, 0.8, size=n_beads)
+    sig = np.concatenate([sig_b, [3.15061, 0.0]])
+    eps = np.concatenate([eps_b, [0.6364, 0.0]])
+    types = np.concatenate([np.tile(np.arange(n_beads), n_chains),
+                            np.tile([n_beads, n_beads + 1, n_beads + 1], n_waters)]).astype(np.int32)
+    bonds, angles, tors = [], [], []
+    for c in range(n_chains):
+        o = c * n_beads
+        bonds += [(o + k, o + k + 1) for k in range(n_beads - 1)]
+        angles += [(o + k, o + k + 1, o + k + 2) for k in range(n_beads - 2)]
+        tors += [(o + k, o + k + 1, o + k + 2, o + k + 3) for k in range(n_beads - 3)]
+    wb = []
+    for w in range(n_waters):
+        o = nb + 3 * w
+        wb += [(o, o + 1), (o, o + 2)]
+    bonds = np.asarray(bonds, dtype=np.int32).reshape(-1, 2)
+    angles = np.asarray(angles, dtype=np.int32).reshape(-1, 3)
+    tors = np.asarray(tors, dtype=np.int32).reshape(-1, 4)
+    cov = covalent_rows(n, np.concatenate([bonds, np.asarray(wb, dtype=np.int32).reshape(-1, 2)]))
+    bond_prm = np.stack([np.full(len(bonds), 2000.0), rng.uniform(1.48, 1.58, size=len(bonds))], axis=1)
+    angle_prm = np.tile([400.0, math.radians(110.0)], (len(angles), 1))
+    t_idx = np.repeat(tors, 3, axis=0)
+    t_prm = np.stack([rng.uniform(0.5, 2.0, size=len(t_idx)), rng.choice([0.0, math.pi], size=len(t_idx)),
+                      np.tile([1.0, 2.0, 3.0], len(tors))], axis=1)
+    kappa = math.sqrt(-math.log(2 * ethresh)) / rc
+    K = int(math.ceil(2 * kappa * L / 3 / ethresh ** 0.2))
+    return dict(n_atoms=n, pos=pos, box=np.eye(3) * L, charges=q, types=types, sigma=sig, epsilon=eps,
+                sigma_tt=(sig[:, None] + sig[None, :]) * 0.5, eps_tt=np.sqrt(eps[:, None] * eps[None, :] + 1e-32),
+                cov_rows=cov.astype(np.int32), bonds=bonds, bond_prm=bond_prm, angles=angles, angle_prm=angle_prm,
+                torsions=t_idx, torsion_prm=t_prm, rc=rc, ethresh=ethresh, kappa=kappa, K=(K, K, K),
+                mscales_coul=np.array([0.0, 0.0, 0.8333333333333334, 1.0, 1.0, 1.0]),
+                mscales_lj=np.array([0.0, 0.0, 0.5, 1.0, 1.0, 1.0]))

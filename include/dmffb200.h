@@ -176,6 +176,64 @@ int dmffb_disp_compute(dmffb_engine* h, void* stream, const double* pos, const d
 /* reciprocal-space dE_lr/dc (device [3n], channel-major) of the last compute, for parameter gradients */
 int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc);
 
+/* ---------------------------------------------------------------------------------------
+ * Classical terms: Lennard-Jones + point-charge Coulomb (PME real+reciprocal+self, reaction
+ * field, or plain 1/r) and harmonic bonds / angles / periodic torsions.
+ * dmffb_classical_create replaces the set-up of CoulombPMEForce / CoulReactionFieldForce /
+ * CoulNoCutoffForce / LennardJonesForce (dmff/classical/inter.py:17-335) and of
+ * HarmonicBondJaxForce / HarmonicAngleJaxForce / PeriodicTorsionJaxForce (intra.py:32-138),
+ * as NonbondedGenerator, CoulombGenerator, LennardJonesGenerator and the bonded generators
+ * build them (dmff/generators/classical.py:154-1394).  Units: Angstrom, e, kJ/mol, radians. */
+enum { DMFFB_COUL_NONE = 0, DMFFB_COUL_PME = 1, DMFFB_COUL_RF = 2, DMFFB_COUL_NOCUTOFF = 3 };
+enum { DMFFB_TERM_BOND = 0, DMFFB_TERM_ANGLE = 1, DMFFB_TERM_TORSION = 2 };
+
+typedef struct {
+    int32_t n_atoms;
+    int32_t n_types;          /* LJ type count (0: no LJ) */
+    int32_t precision;        /* DMFFB_FP32 | DMFFB_FP64 (pair and mesh arithmetic) */
+    int32_t coulomb;          /* DMFFB_COUL_* */
+    int32_t pbc;              /* minimum image on pair vectors (LJ and reaction field; PME always) */
+    double rc;                /* cutoff, Angstrom: internal neighbour build and reaction field */
+    double kappa;             /* Ewald kappa, 1/Angstrom (PME) */
+    int32_t K[3];             /* PME mesh */
+    double eps_solvent;       /* reaction field dielectric (inter.py:205, default 78.5) */
+    int64_t n_cov;
+    const int32_t* cov_rows;  /* host [n_cov*3] (i, j, nbond), i < j */
+    double mscales_coul[6];   /* nbond-1 indexed, [5] = 1.0 (classical.py:878-881) */
+    double mscales_lj[6];
+} dmffb_classical_desc;
+
+typedef struct {
+    double energy;            /* sum of the terms below, kJ/mol */
+    double e_coul_real, e_coul_recip, e_coul_self;
+    double e_lj, e_bond, e_angle, e_torsion;
+    double box_grad[9];       /* dE/dbox at fixed Cartesian positions */
+    int64_t n_pairs;
+} dmffb_classical_result;
+
+int dmffb_classical_create(const dmffb_classical_desc* desc, dmffb_engine** out);
+/* Per-atom charges [n] (may be NULL without Coulomb) and LJ type index [n] with type-pair tables
+ * sigma_tt, eps_tt [n_types^2] (Angstrom, kJ/mol; mixing rule and NBFix already applied), host. */
+int dmffb_classical_set_params(dmffb_engine* h, const double* charges, const int32_t* atom_type,
+                               const double* sigma_tt, const double* eps_tt);
+/* Bonded term list, host arrays: kind DMFFB_TERM_*; idx [n_terms * (2|3|4)] atom indices;
+ * prm: bond (k kJ/mol/A^2, r0 A), angle (k kJ/mol/rad^2, theta0), torsion (k, psi, periodicity)
+ * per term.  Replaces the index/parameter gathers of classical.py:154-787. */
+int dmffb_classical_set_terms(dmffb_engine* h, int32_t kind, int64_t n_terms, const int32_t* idx,
+                              const double* prm);
+/* Parameter adjoints on/off for the following computes (dE/dq, dE/dsigma_tt, dE/deps_tt, dE/dprm). */
+int dmffb_classical_set_param_grads(dmffb_engine* h, int32_t enabled);
+/* Energy, forces (= -dE/dpos, device [n*3], may be NULL) and box gradient; pairs as in
+ * dmffb_admp_compute (NULL: the engine's own neighbour list, rc from the description). */
+int dmffb_classical_compute(dmffb_engine* h, void* stream, const double* pos, const double* box,
+                            const int32_t* pairs, int64_t npairs, double* forces_out,
+                            dmffb_classical_result* result);
+/* Parameter adjoints of the last compute (param grads enabled), device arrays, each may be NULL:
+ * dE_dq [n], dE_dsig [n_types^2], dE_deps [n_types^2], dE_dbond / dE_dangle / dE_dtorsion
+ * [n_terms*2] = (dE/dk, dE/d(r0 | theta0 | psi)). */
+int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, double* dE_dsig, double* dE_deps,
+                                double* dE_dbond, double* dE_dangle, double* dE_dtorsion);
+
 /* Neighbour-list build that allocates no device memory.  No counterpart in the reference (DMFF
  * has no C ABI); same result as dmffb_build_neighbors for callers that cannot allocate on
  * demand: a host (an MD platform such as an OpenMM context, a framework with a caching

@@ -950,14 +950,23 @@ def pairwise_energy(kernel, positions, box, pairs, mScales, *atomic_params):
 # --------------------------------------------------------------------------------------
 # classical terms — dmff/classical/inter.py, intra.py
 # --------------------------------------------------------------------------------------
-def lj_energy(positions, box, pairs, epsilon, sigma, map_prm, mscales, pbc=True):
-    """inter.py:37-93 (Lorentz-Berthelot mixing, no switch); positions/box in the caller's units."""
+ONE_4PI_EPS0 = DIELECTRIC * 0.1  # dmff/classical/inter.py:14 (kJ/mol nm / e^2)
+
+
+def lj_energy(positions, box, pairs, epsilon, sigma, map_prm, mscales, pbc=True, map_nbfix=None, epsfix=None,
+              sigfix=None):
+    """inter.py:37-93 (Lorentz-Berthelot mixing, NBFix overrides, no switch); positions/box in the
+    caller's units."""
     pairs = torch.as_tensor(np.asarray(pairs)).long()
     pr = regularize_pairs(pairs[:, :2])
     mask = pair_buffer_scales(pairs[:, :2])
     map_prm = torch.as_tensor(np.asarray(map_prm)).long()
     eps_mat = torch.sqrt(epsilon[:, None] * epsilon[None, :] + 1e-32)
     sig_mat = (sigma[:, None] + sigma[None, :]) * 0.5
+    if map_nbfix is not None:
+        for a, b, k in np.asarray(map_nbfix, dtype=np.int64).reshape(-1, 3):
+            eps_mat = eps_mat.index_put((torch.tensor([a, b]), torch.tensor([b, a])), epsfix[k].expand(2))
+            sig_mat = sig_mat.index_put((torch.tensor([a, b]), torch.tensor([b, a])), sigfix[k].expand(2))
     msc = _t(mscales)[pairs[:, 2] - 1]
     dr = positions[pr[:, 0]] - positions[pr[:, 1]]
     if pbc:
@@ -968,6 +977,44 @@ def lj_energy(positions, box, pairs, epsilon, sigma, map_prm, mscales, pbc=True)
     d = torch.linalg.norm(dr, dim=1)
     s6 = (sig / d) ** 6
     return torch.sum(4.0 * eps * (s6 * s6 - s6) * mask)
+
+
+def lj_dispersion_correction(box, epsilon, sigma, map_prm, count_mat, r_cut):
+    """inter.py:97-131: -2/3 pi N^2 / V <4 eps sigma^6> / rc^3 over the pair-count matrix."""
+    eps_mat = torch.sqrt(epsilon[:, None] * epsilon[None, :])
+    sig_mat = (sigma[:, None] + sigma[None, :]) * 0.5
+    cm = _t(count_mat)
+    c6 = torch.sum(4 * eps_mat * sig_mat ** 6 * cm) / torch.sum(cm)
+    n = len(map_prm)
+    return -2.0 / 3.0 * math.pi * n * n / torch.linalg.det(box) * c6 / r_cut ** 3
+
+
+def coul_nocutoff_energy(positions, pairs, charges, mscales, eps_1=1.0):
+    """inter.py:134-170: q_i q_j ONE_4PI_EPS0 / eps_1 / r, no periodic image (nm units)."""
+    pairs = torch.as_tensor(np.asarray(pairs)).long()
+    pr = regularize_pairs(pairs[:, :2])
+    mask = pair_buffer_scales(pairs[:, :2])
+    msc = _t(mscales)[pairs[:, 2] - 1]
+    dr = positions[pr[:, 0]] - positions[pr[:, 1]]
+    d = torch.linalg.norm(dr, dim=1)
+    e = charges[pr[:, 0]] * charges[pr[:, 1]] * msc * ONE_4PI_EPS0 / eps_1 / d
+    return torch.sum(e * mask)
+
+
+def coul_rf_energy(positions, box, pairs, charges, mscales, r_cut, eps_1=1.0, eps_solv=78.5, pbc=True):
+    """inter.py:194-260: reaction field q_i q_j ONE_4PI_EPS0 / eps_1 (1/r + k_rf r^2 - c_rf) (nm units)."""
+    krf = (1.0 / r_cut ** 3) * (eps_solv - 1) / (2.0 * eps_solv + 1)
+    crf = (1.0 / r_cut) * 3.0 * eps_solv / (2.0 * eps_solv + 1)
+    pairs = torch.as_tensor(np.asarray(pairs)).long()
+    pr = regularize_pairs(pairs[:, :2])
+    mask = pair_buffer_scales(pairs[:, :2])
+    msc = _t(mscales)[pairs[:, 2] - 1]
+    dr = positions[pr[:, 0]] - positions[pr[:, 1]]
+    if pbc:
+        dr = pbc_shift(dr, box, torch.linalg.inv(box))
+    d = torch.linalg.norm(dr, dim=1)
+    e = charges[pr[:, 0]] * charges[pr[:, 1]] * msc * ONE_4PI_EPS0 / eps_1 * (1.0 / d + krf * d * d - crf)
+    return torch.sum(e * mask)
 
 
 def coulomb_pme_energy(positions_nm, box_nm, pairs, charges, mscales, kappa_nm, K):

@@ -98,6 +98,12 @@ def main():
         f"{wf}/quadrupole_nonpol/forcefield.xml": "waterbox_quadrupole_nonpol.xml",
         f"{wf}/monopole_polarizable/forcefield.xml": "waterbox_monopole_pol.xml",
     }
+    # classical-term inputs (tests/test_classical/*)
+    for f in ["bond1.pdb", "bond1.xml", "angle1.pdb", "angle1.xml", "proper1.pdb", "proper1.xml", "proper2.pdb",
+              "proper2.xml", "impr1.pdb", "impr1.xml", "wild1.xml", "wild2.xml", "lj2.pdb", "lj2.xml", "lj3.pdb",
+              "lj3.xml", "coul2.xml", "coul3.xml", "coul3-res.xml", "methane_water.pdb",
+              "methane_water_coul.xml"]:
+        copies[f"{REF}/tests/data/{f}"] = f
     for src, dst in copies.items():
         shutil.copy(src, os.path.join(DATA, dst))
 
@@ -133,6 +139,18 @@ def main():
         "waterbox996_mpid_es_rc8": {"value": float(mpid[1].split()[1]),
                                     "source": "examples/water_fullpol/mpid_ref/results.txt:2"},
     }
+    # classical goldens: (pdb, xml, value) parametrisations of the reference's classical tests
+    classical = []
+    for path, tol in [("tests/test_classical/test_bonded.py", {"decimal": 3}),
+                      ("tests/test_classical/test_lj.py", {"decimal": 3}),
+                      ("tests/test_classical/test_coul.py", {"decimal": 3})]:
+        for test, cases in parametrize_cases(f"{REF}/{path}").items():
+            for c in cases:
+                entry = {"test": test, "pdb": os.path.basename(c["pdb"]), "xml": os.path.basename(c["prm"]),
+                         "value": float(c["value"]), "source": path}
+                entry.update({"atol": 1e-2} if test == "test_coul_pme" else tol)
+                classical.append(entry)
+    energies["classical"] = classical
     with open(os.path.join(HERE, "energies.json"), "w") as f:
         json.dump(energies, f, indent=1)
 

@@ -45,3 +45,44 @@ def make_engine(sysd, precision="fp32", solver="cg", cg_tol=1e-8, steps_pol=None
                      steps_pol=steps_pol)
     eng.set_params(sysd["Q_local"], sysd.get("pol"), sysd.get("thole"))
     return eng
+
+
+def classical_oracle(H, pos_nm, box_nm, pairs, names=None):
+    """Float64 oracle energy of a Hamiltonian's classical generators (dmff/classical/*.py formulas),
+    using the term lists / maps the generators enumerated in createPotential.  Returns
+    (E, positions tensor, box tensor) with autograd attached."""
+    pos = torch.tensor(np.asarray(pos_nm, dtype=np.float64), requires_grad=True)
+    box = torch.tensor(np.asarray(box_nm, dtype=np.float64), requires_grad=True)
+    E = torch.zeros((), dtype=torch.float64)
+    for name, g in H.generators.items():
+        if names is not None and name not in names:
+            continue
+        P = H.paramset[name]
+        if name == "HarmonicBondForce" and len(g.bond_idx):
+            i, pi = torch.as_tensor(g.bond_idx).long(), g.bond_prm_idx
+            E = E + R.bond_energy(pos, i[:, 0], i[:, 1], P["k"][pi], P["length"][pi])
+        elif name == "HarmonicAngleForce" and len(g.angle_idx):
+            i, pi = torch.as_tensor(g.angle_idx).long(), g.angle_prm_idx
+            E = E + R.angle_energy(pos, i[:, 0], i[:, 1], i[:, 2], P["k"][pi], P["angle"][pi])
+        elif name == "PeriodicTorsionForce" and getattr(g, "torsion_idx", np.zeros((0, 4))).shape[0]:
+            i = torch.as_tensor(g.torsion_idx).long()
+            k = torch.cat([P["proper_k"][g.sel_proper], P["improper_k"][g.sel_improper]])
+            ph = torch.cat([P["proper_phase"][g.sel_proper], P["improper_phase"][g.sel_improper]])
+            E = E + R.torsion_energy(pos, i[:, 0], i[:, 1], i[:, 2], i[:, 3], k, ph, g.torsion_per)
+        elif name in ("NonbondedForce", "CoulombForce"):
+            q = torch.as_tensor(np.asarray(g.charges, dtype=np.float64))
+            if g.coul_mode == "pme":
+                E = E + R.coulomb_pme_energy(pos, box, pairs, q, g.mscales_coul, g.kappa_nm, g.K)
+            elif g.coul_mode == "rf":
+                E = E + R.coul_rf_energy(pos, box, pairs, q, g.mscales_coul, g.r_cut, pbc=g.pbc)
+            elif g.coul_mode == "nocutoff":
+                E = E + R.coul_nocutoff_energy(pos, pairs, q, g.mscales_coul)
+            if name == "NonbondedForce":
+                E = E + R.lj_energy(pos, box, pairs, P["epsilon"], P["sigma"], g.map_prm, g.mscales_lj, pbc=g.pbc)
+                if g.disp_corr is not None:
+                    E = E + R.lj_dispersion_correction(box, P["epsilon"], P["sigma"], g.map_prm,
+                                                       g.disp_corr.count, g.r_cut)
+        elif name == "LennardJonesForce":
+            E = E + R.lj_energy(pos, box, pairs, P["epsilon"], P["sigma"], g.map_prm, g.mscales_lj, pbc=g.pbc,
+                                map_nbfix=g.nbfix, epsfix=P["epsilon_nbfix"], sigfix=P["sigma_nbfix"])
+    return E, pos, box
