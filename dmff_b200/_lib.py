@@ -27,13 +27,15 @@ DMFFB_SOLVER_REFERENCE = 1
 
 # every function the header declares (checked by the CPU test suite)
 EXPORTED = [
-    "dmffb_admp_create", "dmffb_destroy", "dmffb_last_error", "dmffb_admp_set_params",
+    "dmffb_admp_create", "dmffb_admp_reconfigure", "dmffb_destroy", "dmffb_last_error", "dmffb_admp_set_params",
     "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
     "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
     "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters", "dmffb_build_neighbors_noalloc",
     "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads",
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
+    "dmffb_set_graphs", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
+    "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy",
 ]
 
 DMFFB_COUL_NONE = 0
@@ -149,6 +151,58 @@ class ClassicalResult(ctypes.Structure):
     ]
 
 
+class ServerDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_slots", ctypes.c_int32),
+        ("capacity_atoms", ctypes.c_int32),
+        ("hbm_budget_bytes", ctypes.c_int64),
+        ("lmax", ctypes.c_int32),
+        ("lpol", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("mscales", ctypes.c_double * 6),
+        ("pscales", ctypes.c_double * 6),
+        ("dscales", ctypes.c_double * 6),
+        ("solver", ctypes.c_int32),
+        ("cg_tol", ctypes.c_double),
+        ("max_iter", ctypes.c_int32),
+        ("use_graphs", ctypes.c_int32),
+    ]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int32),
+        ("pos", ctypes.c_void_p),
+        ("box", ctypes.c_double * 9),
+        ("axis_types", ctypes.c_void_p),
+        ("axis_indices", ctypes.c_void_p),
+        ("n_cov", ctypes.c_int64),
+        ("cov_rows", ctypes.c_void_p),
+        ("Q_local", ctypes.c_void_p),
+        ("pol", ctypes.c_void_p),
+        ("thole", ctypes.c_void_p),
+        ("rc", ctypes.c_double),
+        ("kappa", ctypes.c_double),
+        ("K", ctypes.c_int32 * 3),
+        ("t_arrival", ctypes.c_double),
+        ("forces_out", ctypes.c_void_p),
+        ("energy", ctypes.c_double),
+        ("box_grad", ctypes.c_double * 9),
+        ("n_iter", ctypes.c_int32),
+        ("status", ctypes.c_int32),
+        ("slot", ctypes.c_int32),
+        ("done", ctypes.c_int32),
+        ("t_start", ctypes.c_double),
+        ("t_done", ctypes.c_double),
+        ("footprint_bytes", ctypes.c_int64),
+    ]
+
+
+# C struct name of each ctypes mirror (layout checked against the header by the CPU tests)
+STRUCTS = {"dmffb_admp_desc": AdmpDesc, "dmffb_admp_result": AdmpResult, "dmffb_disp_desc": DispDesc,
+           "dmffb_disp_result": DispResult, "dmffb_classical_desc": ClassicalDesc,
+           "dmffb_classical_result": ClassicalResult, "dmffb_server_desc": ServerDesc, "dmffb_request": Request}
+
 _lib = None
 
 
@@ -164,6 +218,7 @@ def load():
     P = ctypes.POINTER
     lib.dmffb_admp_create.argtypes = [P(AdmpDesc), P(vp)]
     lib.dmffb_admp_create.restype = ctypes.c_int
+    lib.dmffb_admp_reconfigure.argtypes = [vp, P(AdmpDesc)]
     lib.dmffb_destroy.argtypes = [vp]
     lib.dmffb_destroy.restype = None
     lib.dmffb_last_error.argtypes = [vp]
@@ -191,9 +246,21 @@ def load():
     lib.dmffb_classical_set_param_grads.argtypes = [vp, i32]
     lib.dmffb_classical_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, P(ClassicalResult)]
     lib.dmffb_classical_param_grads.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.dmffb_set_graphs.argtypes = [vp, i32]
+    lib.dmffb_server_create.argtypes = [P(ServerDesc), P(vp)]
+    lib.dmffb_server_submit.argtypes = [vp, P(Request)]
+    lib.dmffb_server_wait.argtypes = [vp, dbl]
+    lib.dmffb_server_prewarm.argtypes = [vp, P(Request), i32]
+    lib.dmffb_server_destroy.argtypes = [vp]
+    lib.dmffb_server_clock.argtypes = [vp]
+    lib.dmffb_request_footprint.argtypes = [i32, dbl, P(i32), dbl, i32]
     for name in EXPORTED:
-        if name not in ("dmffb_destroy", "dmffb_last_error"):
+        if name not in ("dmffb_destroy", "dmffb_last_error", "dmffb_server_destroy", "dmffb_server_clock",
+                        "dmffb_request_footprint"):
             getattr(lib, name).restype = ctypes.c_int
+    lib.dmffb_server_destroy.restype = None
+    lib.dmffb_server_clock.restype = dbl
+    lib.dmffb_request_footprint.restype = i64
     _lib = lib
     return lib
 

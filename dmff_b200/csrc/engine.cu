@@ -10,6 +10,8 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <array>
+#include <map>
 #include <vector>
 
 #include "../../include/dmffb200.h"
@@ -139,6 +141,11 @@ struct dmffb_engine {
     double* d_tprm[3] = {nullptr, nullptr, nullptr};
     double* d_tdprm[3] = {nullptr, nullptr, nullptr};
     bool want_pgrad = false, charges_set = false;
+    // ---- capacities (dmffb_admp_reconfigure reuses the allocations for systems that fit)
+    int n_cap = 0;
+    int64_t cov_cap = 0, grid_cap = 0, cgrid_cap = 0;
+    int bmod_cap = 0;
+    std::map<std::array<int, 3>, std::pair<cufftHandle, cufftHandle>> plan_cache;  // mesh -> (R2C, C2R)
 };
 
 namespace {
@@ -166,7 +173,16 @@ int dalloc(dmffb_engine* h, P** p, size_t bytes) {
     if (bytes == 0) bytes = 16;
     cudaError_t e = cudaMalloc((void**)p, bytes);
     if (e != cudaSuccess) return fail(h, DMFFB_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    cudaMemset(*p, 0, bytes);
+    // zeroed on the engine stream and waited for: the engine's streams are non-blocking, so a
+    // zeroing on the legacy default stream would not be ordered before their kernels
+    if (h->s1) {
+        cudaMemsetAsync(*p, 0, bytes, h->s1);
+        e = cudaStreamSynchronize(h->s1);
+    } else {
+        cudaMemset(*p, 0, bytes);
+        e = cudaDeviceSynchronize();
+    }
+    if (e != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("zeroing: ") + cudaGetErrorString(e));
     return DMFFB_OK;
 }
 
@@ -498,11 +514,12 @@ int build_csr(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npa
     if (h->csr_from_build && pairs == h->d_pairs) return DMFFB_OK;  // made by the neighbour build
     h->csr_from_build = false;
     if (!h->d_csr_off) {
-        if ((st = dalloc(h, &h->d_csr_off, (n + 1) * sizeof(int64_t)))) return st;
-        if ((st = dalloc(h, &h->d_csr_deg, n * sizeof(int32_t)))) return st;
-        if ((st = dalloc(h, &h->d_fmv, 3 * n * sizeof(double)))) return st;
+        const int nc = h->n_cap;
+        if ((st = dalloc(h, &h->d_csr_off, (nc + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_csr_deg, nc * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_fmv, 3 * nc * sizeof(double)))) return st;
         size_t need = 0;
-        cub::DeviceScan::InclusiveSum(nullptr, need, (int32_t*)nullptr, (int64_t*)nullptr, n);
+        cub::DeviceScan::InclusiveSum(nullptr, need, (int32_t*)nullptr, (int64_t*)nullptr, nc);
         h->cub2_bytes = need;
         if ((st = dalloc(h, &h->d_cub2, need))) return st;
     }
@@ -1118,6 +1135,138 @@ __global__ void k_to_t(int m, const double* src, T* dst) {
     if (k < m) dst[k] = (T)src[k];
 }
 
+// description -> scalar state (n, cut-off, Ewald, scales, solver, spread order)
+void set_scalars(dmffb_engine* h, const dmffb_admp_desc* d) {
+    h->n = d->n_atoms;
+    h->rc = d->rc;
+    h->kappa = d->lpme ? d->kappa : 0.0;
+    for (int k = 0; k < 3; ++k) h->K[k] = d->lpme ? d->K[k] : 0;
+    for (int k = 0; k < 6; ++k) {
+        h->ms[k] = d->mscales[k];
+        h->ps[k] = d->pscales[k];
+        h->dsc[k] = d->dscales[k];
+    }
+    h->solver = d->solver;
+    {  // a multiplier coprime with n near n / 148 (one stride per SM) for the spread order
+        auto gcd = [](int64_t a, int64_t b) { while (b) { int64_t t = a % b; a = b; b = t; } return a; };
+        int64_t m = std::max<int64_t>(1, d->n_atoms / 148) | 1;
+        while (gcd(m, d->n_atoms) != 1) m += 2;
+        h->perm_mul = (int)(m % std::max(1, d->n_atoms));
+        if (h->perm_mul == 0) h->perm_mul = 1;
+    }
+    h->cg_tol = d->cg_tol > 0 ? d->cg_tol : 1e-6;
+    h->max_iter = d->max_iter > 0 ? d->max_iter : 500;
+    h->steps_pol = d->steps_pol;
+}
+
+// validate and upload local-axis data and the covalent map (CSR of j > i rows) of the description
+int upload_topology(dmffb_engine* h, const dmffb_admp_desc* d) {
+    const int n = d->n_atoms;
+    std::vector<int32_t> at(n, DMFFB_NOAXISTYPE), ai(3 * n, -1);
+    if (d->axis_types) for (int i = 0; i < n; ++i) at[i] = d->axis_types[i];
+    if (d->axis_indices) for (int i = 0; i < 3 * n; ++i) ai[i] = d->axis_indices[i];
+    for (int i = 0; i < n; ++i) {
+        if (at[i] < 0 || at[i] > 5) return fail(h, DMFFB_BAD_ARG, "bad axis type");
+        for (int k = 0; k < 3; ++k)
+            if (ai[3 * i + k] >= n) return fail(h, DMFFB_BAD_ARG, "axis index out of range");
+        // every axis atom the frame type reads must exist
+        const int need = (at[i] == DMFFB_ZBISECT || at[i] == DMFFB_THREEFOLD) ? 3
+                         : (at[i] == DMFFB_ZONLY ? 1 : (at[i] == DMFFB_NOAXISTYPE ? 0 : 2));
+        if (d->lmax > 0)
+            for (int k = 0; k < need; ++k)
+                if (ai[3 * i + k] < 0) return fail(h, DMFFB_BAD_ARG, "missing axis atom");
+    }
+    std::vector<int32_t> cnt(n + 1, 0);
+    for (int64_t r = 0; r < d->n_cov; ++r) {
+        int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
+        if (i < 0 || j < 0 || i >= n || j >= n || i == j) return fail(h, DMFFB_BAD_ARG, "bad covalent row");
+        cnt[std::min(i, j) + 1]++;
+    }
+    for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+    const int64_t nc = std::max<int64_t>(d->n_cov, 1);
+    std::vector<int32_t> cj(nc), cn(nc), cur(cnt.begin(), cnt.end() - 1);
+    for (int64_t r = 0; r < d->n_cov; ++r) {
+        int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
+        int lo = std::min(i, j), hi = std::max(i, j);
+        int k = cur[lo]++;
+        cj[k] = hi;
+        cn[k] = d->cov_rows[3 * r + 2];
+    }
+    int st;
+    if (nc > h->cov_cap) {
+        if (h->d_cov_j) cudaFree(h->d_cov_j);
+        if (h->d_cov_nb) cudaFree(h->d_cov_nb);
+        h->d_cov_j = h->d_cov_nb = nullptr;
+        h->cov_cap = nc;
+        if ((st = dalloc(h, &h->d_cov_j, nc * sizeof(int32_t))) || (st = dalloc(h, &h->d_cov_nb, nc * sizeof(int32_t))))
+            return st;
+    }
+    CK(cudaMemcpyAsync(h->d_axis_type, at.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaMemcpyAsync(h->d_axis_idx, ai.data(), 3 * n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaMemcpyAsync(h->d_cov_ptr, cnt.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaMemcpyAsync(h->d_cov_j, cj.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaMemcpyAsync(h->d_cov_nb, cn.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaStreamSynchronize(h->s1));  // the host vectors go out of scope
+    return DMFFB_OK;
+}
+
+// PME mesh of h->K: grids grown to fit, B-spline moduli, cuFFT plans (cached per mesh shape)
+int setup_mesh(dmffb_engine* h) {
+    const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
+    const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
+    const int64_t Kc = (int64_t)h->K[0] * h->K[1] * (h->K[2] / 2 + 1);
+    int st;
+    if (K3 > h->grid_cap) {
+        if (h->d_grid) cudaFree(h->d_grid);
+        h->d_grid = nullptr;
+        h->grid_cap = K3;
+        if ((st = dalloc(h, &h->d_grid, K3 * ts))) return st;
+    }
+    if (Kc > h->cgrid_cap) {
+        if (h->d_cgrid) cudaFree(h->d_cgrid);
+        h->d_cgrid = nullptr;
+        h->cgrid_cap = Kc;
+        if ((st = dalloc(h, &h->d_cgrid, 2 * Kc * ts))) return st;
+    }
+    const int ksum = h->K[0] + h->K[1] + h->K[2];
+    if (ksum > h->bmod_cap) {
+        if (h->d_bmod) cudaFree(h->d_bmod);
+        h->d_bmod = nullptr;
+        h->bmod_cap = ksum;
+        if ((st = dalloc(h, &h->d_bmod, ksum * sizeof(double)))) return st;
+    }
+    // per-dimension B-spline moduli, recip.py:440-448: sum_{m=-2..2} M6(m+3) cos(2 pi m k / K)
+    const double M6[5] = {1.0 / 120, 26.0 / 120, 66.0 / 120, 26.0 / 120, 1.0 / 120};
+    std::vector<double> bm;
+    for (int dd = 0; dd < 3; ++dd)
+        for (int k = 0; k < h->K[dd]; ++k) {
+            const int m = k < (h->K[dd] + 1) / 2 ? k : k - h->K[dd];
+            double sm = 0;
+            for (int q = -2; q <= 2; ++q) sm += M6[q + 2] * cos(2.0 * M_PI * q * m / h->K[dd]);
+            bm.push_back(sm);
+        }
+    CK(cudaMemcpyAsync(h->d_bmod, bm.data(), bm.size() * sizeof(double), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaStreamSynchronize(h->s1));
+    const std::array<int, 3> key = {h->K[0], h->K[1], h->K[2]};
+    auto it = h->plan_cache.find(key);
+    if (it == h->plan_cache.end()) {
+        cufftHandle pf = 0, pb = 0;
+        cufftType tf = h->prec == DMFFB_FP32 ? CUFFT_R2C : CUFFT_D2Z;
+        cufftType tb = h->prec == DMFFB_FP32 ? CUFFT_C2R : CUFFT_Z2D;
+        if (cufftPlan3d(&pf, h->K[0], h->K[1], h->K[2], tf) != CUFFT_SUCCESS)
+            return fail(h, DMFFB_CUFFT_ERROR, "cufftPlan3d failed");
+        if (cufftPlan3d(&pb, h->K[0], h->K[1], h->K[2], tb) != CUFFT_SUCCESS) {
+            cufftDestroy(pf);
+            return fail(h, DMFFB_CUFFT_ERROR, "cufftPlan3d failed");
+        }
+        it = h->plan_cache.emplace(key, std::make_pair(pf, pb)).first;
+    }
+    h->plan_f = it->second.first;
+    h->plan_b = it->second.second;
+    h->have_plans = true;
+    return DMFFB_OK;
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -1132,81 +1281,33 @@ int dmffb_admp_create(const dmffb_admp_desc* d, dmffb_engine** out) {
         return DMFFB_BAD_ARG;
     if (d->lpme && (d->K[0] <= 0 || d->K[1] <= 0 || d->K[2] <= 0 || !(d->kappa > 0))) return DMFFB_BAD_ARG;
     dmffb_engine* h = new dmffb_engine();
-    h->n = d->n_atoms;
+    *out = h;
+    // streams and events first: every upload and zeroing below is ordered on the engine stream
+    for (int k = 0; k < 8; ++k) cudaEventCreate(&h->ev[k]);
+    cudaStreamCreateWithFlags(&h->s1, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&h->e_in, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->e_out, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->e_fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&h->e_join, cudaEventDisableTiming);
     h->lmax = d->lmax;
     h->lpol = d->lpol ? 1 : 0;
     h->lpme = d->lpme ? 1 : 0;
     h->prec = d->precision;
-    h->rc = d->rc;
-    h->kappa = d->lpme ? d->kappa : 0.0;
-    for (int k = 0; k < 3; ++k) h->K[k] = d->lpme ? d->K[k] : 0;
-    for (int k = 0; k < 6; ++k) {
-        h->ms[k] = d->mscales[k];
-        h->ps[k] = d->pscales[k];
-        h->dsc[k] = d->dscales[k];
-    }
-    h->solver = d->solver;
+    h->n_cap = d->n_atoms;
     if (getenv("DMFFB_DISABLE_GRAPHS")) h->use_graphs = false;  // eager launches (debugging, tools)
-    {  // a multiplier coprime with n near n / 148 (one stride per SM) for the spread order
-        auto gcd = [](int64_t a, int64_t b) { while (b) { int64_t t = a % b; a = b; b = t; } return a; };
-        int64_t m = std::max<int64_t>(1, d->n_atoms / 148) | 1;
-        while (gcd(m, d->n_atoms) != 1) m += 2;
-        h->perm_mul = (int)(m % std::max(1, d->n_atoms));
-        if (h->perm_mul == 0) h->perm_mul = 1;
-    }
-    h->cg_tol = d->cg_tol > 0 ? d->cg_tol : 1e-6;
-    h->max_iter = d->max_iter > 0 ? d->max_iter : 500;
-    h->steps_pol = d->steps_pol;
-    const int n = h->n;
+    set_scalars(h, d);
+    const int n = h->n_cap;
     const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
     int st = 0;
 #define AL(p, b)                                  \
     if ((st = dalloc(h, &(p), (b))) != DMFFB_OK) { \
-        *out = h;                                 \
         return st;                                \
     }
     AL(h->d_axis_type, n * sizeof(int32_t));
     AL(h->d_axis_idx, 3 * n * sizeof(int32_t));
-    {
-        std::vector<int32_t> at(n, DMFFB_NOAXISTYPE), ai(3 * n, -1);
-        if (d->axis_types) for (int i = 0; i < n; ++i) at[i] = d->axis_types[i];
-        if (d->axis_indices) for (int i = 0; i < 3 * n; ++i) ai[i] = d->axis_indices[i];
-        for (int i = 0; i < n; ++i) {
-            if (at[i] < 0 || at[i] > 5) { *out = h; return fail(h, DMFFB_BAD_ARG, "bad axis type"); }
-            for (int k = 0; k < 3; ++k)
-                if (ai[3 * i + k] >= n) { *out = h; return fail(h, DMFFB_BAD_ARG, "axis index out of range"); }
-            // every axis atom the frame type reads must exist
-            const int need = (at[i] == DMFFB_ZBISECT || at[i] == DMFFB_THREEFOLD) ? 3
-                             : (at[i] == DMFFB_ZONLY ? 1 : (at[i] == DMFFB_NOAXISTYPE ? 0 : 2));
-            if (d->lmax > 0)
-                for (int k = 0; k < need; ++k)
-                    if (ai[3 * i + k] < 0) { *out = h; return fail(h, DMFFB_BAD_ARG, "missing axis atom"); }
-        }
-        cudaMemcpy(h->d_axis_type, at.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice);
-        cudaMemcpy(h->d_axis_idx, ai.data(), 3 * n * sizeof(int32_t), cudaMemcpyHostToDevice);
-        // sparse covalent map -> per-atom rows of j > i
-        std::vector<int32_t> cnt(n + 1, 0);
-        for (int64_t r = 0; r < d->n_cov; ++r) {
-            int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
-            if (i < 0 || j < 0 || i >= n || j >= n || i == j) { *out = h; return fail(h, DMFFB_BAD_ARG, "bad covalent row"); }
-            cnt[std::min(i, j) + 1]++;
-        }
-        for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
-        std::vector<int32_t> cj(std::max<int64_t>(d->n_cov, 1)), cn(std::max<int64_t>(d->n_cov, 1)), cur(cnt.begin(), cnt.end() - 1);
-        for (int64_t r = 0; r < d->n_cov; ++r) {
-            int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
-            int lo = std::min(i, j), hi = std::max(i, j);
-            int k = cur[lo]++;
-            cj[k] = hi;
-            cn[k] = d->cov_rows[3 * r + 2];
-        }
-        AL(h->d_cov_ptr, (n + 1) * sizeof(int32_t));
-        AL(h->d_cov_j, cj.size() * sizeof(int32_t));
-        AL(h->d_cov_nb, cn.size() * sizeof(int32_t));
-        cudaMemcpy(h->d_cov_ptr, cnt.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice);
-        cudaMemcpy(h->d_cov_j, cj.data(), cj.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
-        cudaMemcpy(h->d_cov_nb, cn.data(), cn.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
-    }
+    AL(h->d_cov_ptr, (n + 1) * sizeof(int32_t));
+    if ((st = upload_topology(h, d))) return st;
     AL(h->d_Qloc, 9 * n * sizeof(double));
     AL(h->d_pol, n * sizeof(double));
     AL(h->d_thole, n * ts);
@@ -1231,47 +1332,40 @@ int dmffb_admp_create(const dmffb_admp_desc* d, dmffb_engine** out) {
         AL(h->d_Ap, 3 * n * sizeof(double));
         AL(h->d_fr, 3 * n * sizeof(double));
     }
-    if (cudaMallocHost((void**)&h->h_scal, N_SCAL * sizeof(double)) != cudaSuccess) {
-        *out = h;
-        return fail(h, DMFFB_OOM, "cudaMallocHost failed");
-    }
-    if (h->lpme) {
-        const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
-        const int64_t Kc = (int64_t)h->K[0] * h->K[1] * (h->K[2] / 2 + 1);
-        AL(h->d_grid, K3 * ts);
-        AL(h->d_cgrid, 2 * Kc * ts);
-        AL(h->d_bmod, (h->K[0] + h->K[1] + h->K[2]) * sizeof(double));
-        // per-dimension B-spline moduli, recip.py:440-448: sum_{m=-2..2} M6(m+3) cos(2 pi m k / K)
-        const double M6[5] = {1.0 / 120, 26.0 / 120, 66.0 / 120, 26.0 / 120, 1.0 / 120};
-        std::vector<double> bm;
-        for (int dd = 0; dd < 3; ++dd)
-            for (int k = 0; k < h->K[dd]; ++k) {
-                const int m = k < (h->K[dd] + 1) / 2 ? k : k - h->K[dd];
-                double s = 0;
-                for (int q = -2; q <= 2; ++q) s += M6[q + 2] * cos(2.0 * M_PI * q * m / h->K[dd]);
-                bm.push_back(s);
-            }
-        cudaMemcpy(h->d_bmod, bm.data(), bm.size() * sizeof(double), cudaMemcpyHostToDevice);
-        cufftType tf = h->prec == DMFFB_FP32 ? CUFFT_R2C : CUFFT_D2Z;
-        cufftType tb = h->prec == DMFFB_FP32 ? CUFFT_C2R : CUFFT_Z2D;
-        if (cufftPlan3d(&h->plan_f, h->K[0], h->K[1], h->K[2], tf) != CUFFT_SUCCESS ||
-            cufftPlan3d(&h->plan_b, h->K[0], h->K[1], h->K[2], tb) != CUFFT_SUCCESS) {
-            *out = h;
-            return fail(h, DMFFB_CUFFT_ERROR, "cufftPlan3d failed");
-        }
-        h->have_plans = true;
-    }
-    for (int k = 0; k < 8; ++k) cudaEventCreate(&h->ev[k]);
-    cudaStreamCreateWithFlags(&h->s1, cudaStreamNonBlocking);
-    cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking);
-    cudaEventCreateWithFlags(&h->e_in, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&h->e_out, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&h->e_fork, cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&h->e_join, cudaEventDisableTiming);
 #undef AL
-    cudaError_t e = cudaDeviceSynchronize();
-    *out = h;
+    if (cudaMallocHost((void**)&h->h_scal, N_SCAL * sizeof(double)) != cudaSuccess)
+        return fail(h, DMFFB_OOM, "cudaMallocHost failed");
+    if (h->lpme && (st = setup_mesh(h))) return st;
+    cudaError_t e = cudaStreamSynchronize(h->s1);
     if (e != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, cudaGetErrorString(e));
+    return DMFFB_OK;
+}
+
+int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* d) {
+    if (!h || !d) return DMFFB_BAD_ARG;
+    if (h->kind != 0) return fail(h, DMFFB_BAD_ARG, "reconfigure applies to ADMP engines");
+    if (d->n_atoms <= 0 || d->n_atoms > h->n_cap)
+        return fail(h, DMFFB_SCRATCH_TOO_SMALL, "n_atoms exceeds the capacity the engine was created with");
+    if (d->lmax != h->lmax || (d->lpol ? 1 : 0) != h->lpol || (d->lpme ? 1 : 0) != h->lpme || d->precision != h->prec)
+        return fail(h, DMFFB_BAD_ARG, "lmax, lpol, lpme and precision are fixed at create");
+    if (d->lpme && (d->K[0] <= 0 || d->K[1] <= 0 || d->K[2] <= 0 || !(d->kappa > 0)))
+        return fail(h, DMFFB_BAD_ARG, "bad PME mesh or kappa");
+    CK(cudaStreamSynchronize(h->s1));
+    set_scalars(h, d);
+    int st;
+    if ((st = upload_topology(h, d))) return st;
+    if (h->lpme && (st = setup_mesh(h))) return st;
+    // everything derived from the previous system is stale
+    h->have_pairs = false;
+    h->npairs = 0;
+    h->csr_from_build = false;
+    h->csr_pairs = nullptr;
+    if (h->cg_exec) {
+        cudaGraphExecDestroy(h->cg_exec);
+        h->cg_exec = nullptr;
+    }
+    h->cg_key.clear();
+    h->params_set = false;
     return DMFFB_OK;
 }
 
@@ -1290,9 +1384,9 @@ void dmffb_destroy(dmffb_engine* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
-    if (h->have_plans) {
-        cufftDestroy(h->plan_f);
-        cufftDestroy(h->plan_b);
+    for (auto& kv : h->plan_cache) {
+        cufftDestroy(kv.second.first);
+        cufftDestroy(kv.second.second);
     }
     for (int k = 0; k < 8; ++k) cudaEventDestroy(h->ev[k]);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
@@ -1310,20 +1404,22 @@ int dmffb_admp_set_params(dmffb_engine* h, const double* Q_local, const double* 
     if (!h || !Q_local) return fail(h, DMFFB_BAD_ARG, "null handle or Q_local");
     if (h->lpol && (!pol || !thole)) return fail(h, DMFFB_BAD_ARG, "polarizable system needs pol and thole");
     const int n = h->n;
-    CK(cudaMemcpy(h->d_Qloc, Q_local, 9 * n * sizeof(double), cudaMemcpyHostToDevice));
-    std::vector<double> pz(n, 0.0);
-    CK(cudaMemcpy(h->d_pol, pol ? pol : pz.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    // ordered on the engine stream (no device-wide synchronisation: other engines keep running)
+    cudaStream_t s = h->s1;
+    CK(cudaMemcpyAsync(h->d_Qloc, Q_local, 9 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (pol) CK(cudaMemcpyAsync(h->d_pol, pol, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    else CK(cudaMemsetAsync(h->d_pol, 0, n * sizeof(double), s));
     double* dth = nullptr;
-    if (thole) {
-        CK(cudaMalloc((void**)&dth, n * sizeof(double)));
-        CK(cudaMemcpy(dth, thole, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (thole) {  // staged in the gradient scratch, which compute() overwrites anyway
+        dth = h->d_grad;
+        CK(cudaMemcpyAsync(dth, thole, n * sizeof(double), cudaMemcpyHostToDevice, s));
     }
     if (h->prec == DMFFB_FP32)
-        k_set_thole<float><<<nblk(n, 128), 128>>>(n, h->d_pol, dth, (float*)h->d_thole, (float*)h->d_polsix);
+        k_set_thole<float><<<nblk(n, 128), 128, 0, s>>>(n, h->d_pol, dth, (float*)h->d_thole, (float*)h->d_polsix);
     else
-        k_set_thole<double><<<nblk(n, 128), 128>>>(n, h->d_pol, dth, (double*)h->d_thole, (double*)h->d_polsix);
-    CK(cudaDeviceSynchronize());
-    if (dth) cudaFree(dth);
+        k_set_thole<double><<<nblk(n, 128), 128, 0, s>>>(n, h->d_pol, dth, (double*)h->d_thole, (double*)h->d_polsix);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
     h->params_set = true;
     return DMFFB_OK;
 }
@@ -1348,12 +1444,23 @@ int dmffb_admp_compute(dmffb_engine* h, void* stream, const double* pos, const d
 int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* box, const int32_t* pairs,
                             int64_t npairs, double* U_inout, double* forces_out, dmffb_admp_result* result) {
     if (!h || !pos) return fail(h, DMFFB_BAD_ARG, "null handle or positions");
+    if (pairs && npairs < 0) return fail(h, DMFFB_BAD_ARG, "negative npairs");
     const int n = h->n;
-    cudaStream_t s = 0;
+    cudaStream_t s = h->s1;  // engine stream: host-buffer calls of different engines overlap on the GPU
     CK(cudaMemcpyAsync(h->d_pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     int32_t* dp = nullptr;
-    if (pairs) {
-        CK(cudaMalloc((void**)&dp, std::max<int64_t>(npairs, 1) * 3 * sizeof(int32_t)));
+    if (pairs) {  // staged in the engine's pair buffer (grown when short)
+        if (npairs > h->pair_cap) {
+            CK(cudaStreamSynchronize(s));
+            if (h->d_pairs) cudaFree(h->d_pairs);
+            h->d_pairs = nullptr;
+            h->pair_cap = npairs + 64;
+            int sa = dalloc(h, &h->d_pairs, h->pair_cap * 3 * sizeof(int32_t));
+            if (sa) return sa;
+        }
+        h->have_pairs = false;
+        h->csr_from_build = false;
+        dp = h->d_pairs;
         CK(cudaMemcpyAsync(dp, pairs, npairs * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     }
     if (h->lpol) {
@@ -1365,10 +1472,11 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
         if (sb) return sb;
     }
     int st = dmffb_admp_compute(h, s, h->d_pos, box, dp, npairs, h->lpol ? h->d_U : nullptr, h->d_forces, result);
-    if (dp) cudaFree(dp);
+    if (dp) h->have_pairs = false;  // the staged rows are not the engine's own neighbour list
     if (st != DMFFB_OK && st != DMFFB_NOT_CONVERGED) return st;
-    if (forces_out) CK(cudaMemcpy(forces_out, h->d_forces, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
-    if (h->lpol && U_inout) CK(cudaMemcpy(U_inout, h->d_U, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (forces_out) CK(cudaMemcpyAsync(forces_out, h->d_forces, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->lpol && U_inout) CK(cudaMemcpyAsync(U_inout, h->d_U, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
     return st;
 }
 
@@ -1413,10 +1521,9 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
 }
 
 int dmffb_admp_multipole_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal) {
-    (void)stream;
     (void)dE_dQlocal;
     if (!h || !dE_dQglobal) return fail(h, DMFFB_BAD_ARG, "null argument");
-    CK(cudaMemcpy(dE_dQglobal, h->d_gQ, 9 * h->n * sizeof(double), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpyAsync(dE_dQglobal, h->d_gQ, 9 * h->n * sizeof(double), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return DMFFB_OK;
 }
 
@@ -1443,10 +1550,11 @@ int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, cons
     }
     int st;
     if (!h->d_pcount) {
-        if ((st = dalloc(h, &h->d_pcount, n * sizeof(int32_t)))) return st;
-        if ((st = dalloc(h, &h->d_poff, (n + 1) * sizeof(int64_t)))) return st;
-        if ((st = dalloc(h, &h->d_atom_cell, n * sizeof(int32_t)))) return st;
-        if ((st = dalloc(h, &h->d_cell_atoms, n * sizeof(int32_t)))) return st;
+        const int nc = h->n_cap;
+        if ((st = dalloc(h, &h->d_pcount, nc * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_poff, (nc + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_atom_cell, nc * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_atoms, nc * sizeof(int32_t)))) return st;
     }
     const int ncell = cells ? nc[0] * nc[1] * nc[2] : 1;
     if (ncell + 1 > h->ncell_cap) {
@@ -1548,21 +1656,23 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     }
     int st;
     if (!h->d_pcount) {
-        if ((st = dalloc(h, &h->d_pcount, n * sizeof(int32_t)))) return st;
-        if ((st = dalloc(h, &h->d_poff, (n + 1) * sizeof(int64_t)))) return st;
-        if ((st = dalloc(h, &h->d_atom_cell, n * sizeof(int32_t)))) return st;
-        if ((st = dalloc(h, &h->d_cell_atoms, n * sizeof(int32_t)))) return st;
+        const int nc = h->n_cap;
+        if ((st = dalloc(h, &h->d_pcount, nc * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_poff, (nc + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_atom_cell, nc * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_atoms, nc * sizeof(int32_t)))) return st;
     }
     if (!h->d_posf) {
-        if ((st = dalloc(h, &h->d_posf, 4 * n * sizeof(float)))) return st;
-        if ((st = dalloc(h, &h->d_pcount_f, n * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_posf, 4 * h->n_cap * sizeof(float)))) return st;
+        if ((st = dalloc(h, &h->d_pcount_f, h->n_cap * sizeof(int32_t)))) return st;
     }
     if (!h->d_csr_off) {
-        if ((st = dalloc(h, &h->d_csr_off, (n + 1) * sizeof(int64_t)))) return st;
-        if ((st = dalloc(h, &h->d_csr_deg, n * sizeof(int32_t)))) return st;
-        if ((st = dalloc(h, &h->d_fmv, 3 * n * sizeof(double)))) return st;
+        const int nc = h->n_cap;
+        if ((st = dalloc(h, &h->d_csr_off, (nc + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_csr_deg, nc * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_fmv, 3 * nc * sizeof(double)))) return st;
         size_t need = 0;
-        cub::DeviceScan::InclusiveSum(nullptr, need, (int32_t*)nullptr, (int64_t*)nullptr, n);
+        cub::DeviceScan::InclusiveSum(nullptr, need, (int32_t*)nullptr, (int64_t*)nullptr, nc);
         h->cub2_bytes = need;
         if ((st = dalloc(h, &h->d_cub2, need))) return st;
     }
@@ -1695,20 +1805,19 @@ int dmffb_disp_set_params(dmffb_engine* h, const double* c_list, const double* a
     if (h->pmax >= 8) e -= k2 * k2 * k2 * k2 / 48.0 * s8;
     if (h->pmax >= 10) e -= k2 * k2 * k2 * k2 * k2 / 240.0 * s10;
     h->e_self_disp = e;
-    double* tmp = nullptr;
-    CK(cudaMalloc((void**)&tmp, 3 * n * sizeof(double)));
+    // staged through the FP64 gradient scratch ([3n], rewritten by every compute), on the engine stream
+    double* tmp = h->d_grad;
     auto up = [&](const double* src, int m, void* dst) -> int {
-        CK(cudaMemcpy(tmp, src, m * sizeof(double), cudaMemcpyHostToDevice));
-        if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256>>>(m, tmp, (float*)dst);
-        else k_to_t<double><<<nblk(m, 256), 256>>>(m, tmp, (double*)dst);
-        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpyAsync(tmp, src, m * sizeof(double), cudaMemcpyHostToDevice, h->s1));
+        if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256, 0, h->s1>>>(m, tmp, (float*)dst);
+        else k_to_t<double><<<nblk(m, 256), 256, 0, h->s1>>>(m, tmp, (double*)dst);
+        CK(cudaStreamSynchronize(h->s1));
         return DMFFB_OK;
     };
     int st = up(cm.data(), 3 * n, h->d_c);
     if (!st && h->tt) st = up(a, n, h->d_tta);
     if (!st && h->tt) st = up(b, n, h->d_ttb);
     if (!st && h->tt) st = up(q, n, h->d_ttq);
-    cudaFree(tmp);
     if (st) return st;
     h->params_set = true;
     return DMFFB_OK;
@@ -1728,9 +1837,8 @@ int dmffb_disp_compute(dmffb_engine* h, void* stream, const double* pos, const d
 }
 
 int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc) {
-    (void)stream;
     if (!h || h->kind != 1 || !dE_dc) return fail(h, DMFFB_BAD_ARG, "bad arguments");
-    CK(cudaMemcpy(dE_dc, h->d_dc, 3 * h->n * sizeof(double), cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpyAsync(dE_dc, h->d_dc, 3 * h->n * sizeof(double), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return DMFFB_OK;
 }
 
@@ -1795,24 +1903,24 @@ int dmffb_classical_set_params(dmffb_engine* h, const double* charges, const int
     double s2 = 0.0;
     for (int i = 0; i < n; ++i) s2 += q[i] * q[i];
     h->e_self_coul = -DMFFB_DIELECTRIC * h->kappa / sqrt(M_PI) * s2;  // pme.py:1183-1222, lmax 0
-    CK(cudaMemcpy(h->d_q, q, n * sizeof(double), cudaMemcpyHostToDevice));
-    if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(n, 256), 256>>>(n, h->d_q, (float*)h->d_qT);
-    else k_to_t<double><<<nblk(n, 256), 256>>>(n, h->d_q, (double*)h->d_qT);
+    cudaStream_t s = h->s1;
+    CK(cudaMemcpyAsync(h->d_q, q, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(n, 256), 256, 0, s>>>(n, h->d_q, (float*)h->d_qT);
+    else k_to_t<double><<<nblk(n, 256), 256, 0, s>>>(n, h->d_q, (double*)h->d_qT);
+    CK(cudaStreamSynchronize(s));
     if (nt > 0) {
-        CK(cudaMemcpy(h->d_type, atom_type, n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(h->d_type, atom_type, n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
         const int m = nt * nt;
-        double* tmp = nullptr;
-        CK(cudaMalloc((void**)&tmp, m * sizeof(double)));
+        double* tmp = h->d_dsig;  // [nt^2] FP64 adjoint scratch, zeroed by every compute that uses it
         for (int w = 0; w < 2; ++w) {
-            CK(cudaMemcpy(tmp, w == 0 ? sigma_tt : eps_tt, m * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(tmp, w == 0 ? sigma_tt : eps_tt, m * sizeof(double), cudaMemcpyHostToDevice, s));
             void* dst = w == 0 ? h->d_sigtt : h->d_epstt;
-            if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256>>>(m, tmp, (float*)dst);
-            else k_to_t<double><<<nblk(m, 256), 256>>>(m, tmp, (double*)dst);
-            CK(cudaDeviceSynchronize());
+            if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256, 0, s>>>(m, tmp, (float*)dst);
+            else k_to_t<double><<<nblk(m, 256), 256, 0, s>>>(m, tmp, (double*)dst);
+            CK(cudaStreamSynchronize(s));
         }
-        cudaFree(tmp);
     }
-    CK(cudaDeviceSynchronize());
+    CK(cudaGetLastError());
     h->params_set = true;
     return DMFFB_OK;
 }
@@ -1837,8 +1945,9 @@ int dmffb_classical_set_terms(dmffb_engine* h, int32_t kind, int64_t n_terms, co
         (st = dalloc(h, &h->d_tprm[kind], n_terms * np * sizeof(double))) ||
         (st = dalloc(h, &h->d_tdprm[kind], n_terms * 2 * sizeof(double))))
         return st;
-    CK(cudaMemcpy(h->d_tidx[kind], idx, n_terms * arity * sizeof(int32_t), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_tprm[kind], prm, n_terms * np * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpyAsync(h->d_tidx[kind], idx, n_terms * arity * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaMemcpyAsync(h->d_tprm[kind], prm, n_terms * np * sizeof(double), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaStreamSynchronize(h->s1));
     h->nterm[kind] = n_terms;
     return DMFFB_OK;
 }
@@ -1864,17 +1973,17 @@ int dmffb_classical_compute(dmffb_engine* h, void* stream, const double* pos, co
 
 int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, double* dE_dsig, double* dE_deps,
                                 double* dE_dbond, double* dE_dangle, double* dE_dtorsion) {
-    (void)stream;
+    cudaStream_t cs = (cudaStream_t)stream;
     if (!h || h->kind != 2) return fail(h, DMFFB_BAD_ARG, "classical engine required");
     if (!h->want_pgrad) return fail(h, DMFFB_BAD_ARG, "parameter gradients are not enabled");
     const size_t tt = (size_t)h->ntypes * h->ntypes;
-    if (dE_dq) CK(cudaMemcpy(dE_dq, h->d_dq, h->n * sizeof(double), cudaMemcpyDeviceToDevice));
-    if (dE_dsig && tt) CK(cudaMemcpy(dE_dsig, h->d_dsig, tt * sizeof(double), cudaMemcpyDeviceToDevice));
-    if (dE_deps && tt) CK(cudaMemcpy(dE_deps, h->d_deps, tt * sizeof(double), cudaMemcpyDeviceToDevice));
+    if (dE_dq) CK(cudaMemcpyAsync(dE_dq, h->d_dq, h->n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    if (dE_dsig && tt) CK(cudaMemcpyAsync(dE_dsig, h->d_dsig, tt * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    if (dE_deps && tt) CK(cudaMemcpyAsync(dE_deps, h->d_deps, tt * sizeof(double), cudaMemcpyDeviceToDevice, cs));
     double* dst[3] = {dE_dbond, dE_dangle, dE_dtorsion};
     for (int k = 0; k < 3; ++k)
         if (dst[k] && h->nterm[k] > 0)
-            CK(cudaMemcpy(dst[k], h->d_tdprm[k], h->nterm[k] * 2 * sizeof(double), cudaMemcpyDeviceToDevice));
+            CK(cudaMemcpyAsync(dst[k], h->d_tdprm[k], h->nterm[k] * 2 * sizeof(double), cudaMemcpyDeviceToDevice, cs));
     return DMFFB_OK;
 }
 
@@ -1910,6 +2019,17 @@ int dmffb_get_counters(const dmffb_engine* h, int64_t* out, int32_t n) {
 int dmffb_set_timing(dmffb_engine* h, int32_t enabled) {
     if (!h) return DMFFB_BAD_ARG;
     h->timing = enabled != 0;
+    return DMFFB_OK;
+}
+
+int dmffb_set_graphs(dmffb_engine* h, int32_t enabled) {
+    if (!h) return DMFFB_BAD_ARG;
+    h->use_graphs = enabled != 0;
+    if (!h->use_graphs && h->cg_exec) {
+        cudaGraphExecDestroy(h->cg_exec);
+        h->cg_exec = nullptr;
+        h->cg_key.clear();
+    }
     return DMFFB_OK;
 }
 

@@ -45,21 +45,40 @@ class AdmpEngine:
                  mscales, pscales=None, dscales=None, precision="fp32", solver="cg", cg_tol=1e-6, max_iter=500,
                  steps_pol=None, device=None):
         self.lib = L.load()
-        self.n = int(n_atoms)
-        self.lpol = bool(lpol)
+        self.n = self.n_cap = int(n_atoms)
+        self.lmax, self.lpol, self.lpme, self.precision = int(lmax), bool(lpol), bool(lpme), precision
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        d = self._desc(n_atoms, rc, kappa, K, axis_types, axis_indices, cov_rows, mscales, pscales, dscales,
+                       solver, cg_tol, max_iter, steps_pol)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = self.lib.dmffb_admp_create(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if st != L.DMFFB_OK:
+            msg = self.lib.dmffb_last_error(h).decode() if h.value else "invalid description"
+            if h.value:
+                self.lib.dmffb_destroy(h)
+            self.h = None
+            raise L.EngineError(st, msg)
+        self._U_buf = torch.zeros((self.n_cap, 3), dtype=torch.float64, device=self.device)
+        self._F_buf = torch.zeros((self.n_cap, 3), dtype=torch.float64, device=self.device)
+        self.U, self.forces = self._U_buf, self._F_buf
+
+    def _desc(self, n_atoms, rc, kappa, K, axis_types, axis_indices, cov_rows, mscales, pscales, dscales, solver,
+              cg_tol, max_iter, steps_pol):
+        n = int(n_atoms)
         d = L.AdmpDesc()
-        d.n_atoms = self.n
-        d.lmax = int(lmax)
-        d.lpol = int(bool(lpol))
-        d.lpme = int(bool(lpme))
-        d.precision = _PREC[precision]
+        d.n_atoms = n
+        d.lmax = self.lmax
+        d.lpol = int(self.lpol)
+        d.lpme = int(self.lpme)
+        d.precision = _PREC[self.precision]
         d.rc = float(rc)
-        d.kappa = float(kappa) if lpme else 0.0
+        d.kappa = float(kappa) if self.lpme else 0.0
         for k in range(3):
-            d.K[k] = int(K[k]) if lpme else 0
-        at = _i32(axis_types if axis_types is not None else np.full(self.n, 5), (self.n,))
-        ai = _i32(axis_indices if axis_indices is not None else np.full((self.n, 3), -1), (self.n * 3,))
+            d.K[k] = int(K[k]) if self.lpme else 0
+        at = _i32(axis_types if axis_types is not None else np.full(n, 5), (n,))
+        ai = _i32(axis_indices if axis_indices is not None else np.full((n, 3), -1), (n * 3,))
         cov = _i32(cov_rows if cov_rows is not None else np.zeros((0, 3)), (-1,))
         self._keep = (at, ai, cov)
         d.axis_types = _ptr(at)
@@ -75,18 +94,18 @@ class AdmpEngine:
         d.cg_tol = float(cg_tol)
         d.max_iter = int(max_iter)
         d.steps_pol = int(steps_pol) if steps_pol else 0
-        h = ctypes.c_void_p()
+        return d
+
+    def reconfigure(self, n_atoms, rc, kappa, K, axis_types, axis_indices, cov_rows, mscales, pscales=None,
+                    dscales=None, solver="cg", cg_tol=1e-6, max_iter=500, steps_pol=None):
+        """Point this engine at another system of the same kind with n_atoms <= the capacity it was
+        created with (buffers and cuFFT plans are reused); set_params must follow."""
+        d = self._desc(n_atoms, rc, kappa, K, axis_types, axis_indices, cov_rows, mscales, pscales, dscales,
+                       solver, cg_tol, max_iter, steps_pol)
         with torch.cuda.device(self.device):
-            st = self.lib.dmffb_admp_create(ctypes.byref(d), ctypes.byref(h))
-        self.h = h
-        if st != L.DMFFB_OK:
-            msg = self.lib.dmffb_last_error(h).decode() if h.value else "invalid description"
-            if h.value:
-                self.lib.dmffb_destroy(h)
-            self.h = None
-            raise L.EngineError(st, msg)
-        self.U = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
-        self.forces = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+            self._check(self.lib.dmffb_admp_reconfigure(self.h, ctypes.byref(d)))
+        self.n = int(n_atoms)
+        self.U, self.forces = self._U_buf[: self.n], self._F_buf[: self.n]
 
     def __del__(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -294,3 +294,64 @@ def polymer_water_box(n_chains, n_beads, n_waters, L, seed=4, rc=10.0, ethresh=1
                 torsions=t_idx, torsion_prm=t_prm, rc=rc, ethresh=ethresh, kappa=kappa, K=(K, K, K),
                 mscales_coul=np.array([0.0, 0.0, 0.8333333333333334, 1.0, 1.0, 1.0]),
                 mscales_lj=np.array([0.0, 0.0, 0.5, 1.0, 1.0, 1.0]))
+
+
+def water_positions_fast(n_waters, L, rng, min_inter=1.7, max_rounds=100):
+    """Vectorised variant of ``water_positions`` for streams of many boxes: lattice centres with
+    U(+-0.3 A) jitter and uniform random orientations; in rounds, one molecule of every pair with
+    an intermolecular atom contact below ``min_inter`` (periodic k-d tree query; the later one in
+    even rounds, the earlier one in odd rounds) gets a new jitter and orientation, until no contact
+    is left."""
+    from scipy.spatial import cKDTree
+    m = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
+    sites = np.array([(i, j, k) for i in range(m) for j in range(m) for k in range(m)], dtype=np.float64)
+    if n_waters < m ** 3:
+        sites = sites[np.sort(rng.choice(m ** 3, n_waters, replace=False))]
+    centers = (sites + 0.5) * (L / m) + rng.uniform(-0.3, 0.3, size=(n_waters, 3))
+    body = _body()
+    R = _random_rotations(rng, n_waters)
+    pos = centers[:, None, :] + np.einsum("nij,aj->nai", R, body)
+    base = (sites + 0.5) * (L / m)
+    for rnd in range(max_rounds):
+        flat = pos.reshape(-1, 3) % L
+        pr = cKDTree(flat, boxsize=L).query_pairs(min_inter, output_type="ndarray")
+        mol = pr // 3
+        mol = mol[mol[:, 0] != mol[:, 1]]
+        if len(mol) == 0:
+            break
+        bad = np.unique(mol.max(axis=1) if rnd % 2 == 0 else mol.min(axis=1))
+        centers[bad] = base[bad] + rng.uniform(-0.3, 0.3, size=(len(bad), 3))
+        pos[bad] = centers[bad][:, None, :] + np.einsum("nij,aj->nai", _random_rotations(rng, len(bad)), body)
+    return pos.reshape(-1, 3)
+
+
+def serving_system(n_waters, index, density=0.0334, rc=8.0, ethresh=5e-4, lmax=2, seed=3):
+    """One request of the serving stream: a polarizable water box of ``n_waters`` molecules at
+    ``density`` molecules/A^3 (L = (n / density)^(1/3)), built as ``water_box`` (per-type multipoles
+    of seed ``seed``, O 1.0 / H 0.5 A^3, Thole 0.33) with positions from ``water_positions_fast``
+    seeded by (seed, index).  Boxes narrower than 2 rc use rc' = 0.5 L (1 - 1e-6), with kappa and K
+    re-derived from rc' ('openmm' formula)."""
+    L = (n_waters / density) ** (1.0 / 3.0)
+    rcx = min(rc, 0.5 * L * (1 - 1e-6))
+    rng_t = np.random.default_rng(seed)
+    Qt = type_multipoles(rng_t)
+    if lmax < 2:
+        Qt[:, 4:] = 0.0
+    if lmax < 1:
+        Qt[:, 1:4] = 0.0
+    rng = np.random.default_rng([seed, int(index)])
+    pos = water_positions_fast(n_waters, L, rng)
+    types, axis_types, axis_indices, cov = water_topology(n_waters)
+    kappa = math.sqrt(-math.log(2 * ethresh)) / rcx
+    K = int(math.ceil(2 * kappa * L / 3 / ethresh ** 0.2))
+    return dict(n_atoms=3 * n_waters, pos=pos, box=np.eye(3) * L, types=types, axis_types=axis_types,
+                axis_indices=axis_indices, cov_rows=cov, Q_type=Qt, Q_local=Qt[types], lmax=lmax, lpol=True, rc=rcx,
+                ethresh=ethresh, kappa=kappa, K=(K, K, K), mscales=np.array([0.0, 0.0, 1.0, 1.0, 1.0, 1.0]),
+                pscales=np.array([0.0, 0.0, 1.0, 1.0, 1.0, 1.0]), dscales=np.ones(6),
+                pol=np.where(types == 0, 1.0, 0.5).astype(np.float64), thole=np.full(3 * n_waters, 0.33))
+
+
+def serving_arrivals(n_requests, rate, seed=33):
+    """Poisson arrival times (s) of the serving stream at ``rate`` requests/s."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n_requests))

@@ -83,6 +83,16 @@ int dmffb_admp_create(const dmffb_admp_desc* desc, dmffb_engine** out);
 void dmffb_destroy(dmffb_engine* h);
 const char* dmffb_last_error(const dmffb_engine* h);
 
+/* Re-point an existing engine at another system of the same kind (same lmax, lpol, lpme and
+ * precision) with n_atoms <= the n_atoms it was created with: new positions' topology, cut-off,
+ * Ewald kappa / mesh K, scales and solver settings.  Device buffers are reused (grown only for a
+ * larger mesh or covalent map); cuFFT plans are cached per mesh shape.  The neighbour list,
+ * dipole-solve graph and parameters of the previous system are dropped: call set_params next.
+ * No counterpart in the reference (its ADMPPmeForce is rebuilt per system); this is what lets a
+ * serving loop keep a fixed pool of engines.  Returns DMFFB_SCRATCH_TOO_SMALL when n_atoms
+ * exceeds the capacity. */
+int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* desc);
+
 /* Per-atom parameters, host arrays: Q_local [n*9] harmonic local-frame multipoles in the
  * reference's units (params["ADMPPmeForce"]["Q_local"][map_atomtype], admp.py:1373),
  * zero-padded to 9 components; pol [n] (A^3) and thole [n] (may be NULL when lpol == 0). */
@@ -233,6 +243,73 @@ int dmffb_classical_compute(dmffb_engine* h, void* stream, const double* pos, co
  * [n_terms*2] = (dE/dk, dE/d(r0 | theta0 | psi)). */
 int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, double* dE_dsig, double* dE_deps,
                                 double* dE_dbond, double* dE_dangle, double* dE_dtorsion);
+
+/* CUDA-graph capture of the dipole-solve loop on/off for this engine (on by default). */
+int dmffb_set_graphs(dmffb_engine* h, int32_t enabled);
+
+/* ---------------------------------------------------------------------------------------
+ * Serving: continuous batching of independent ADMP evaluations (energy + forces + virial) on
+ * one GPU.  No counterpart in the reference (its callers evaluate one system at a time through
+ * ADMPPmeForce.get_energy, dmff/admp/pme.py:186-232).  A server owns a pool of engines ("slots",
+ * each with its own streams, created at capacity_atoms and re-pointed at each request with
+ * dmffb_admp_reconfigure) and one host worker thread per slot.  Requests wait in arrival order;
+ * the head request is admitted when its arrival time has passed, a slot is idle and the summed
+ * device footprint of the requests in flight plus its own stays within hbm_budget_bytes.
+ * Admitted requests run concurrently on their slots' streams, so small requests overlap on the
+ * GPU while large ones limit how many run at once. */
+typedef struct dmffb_server dmffb_server;
+
+typedef struct {
+    int32_t n_slots;          /* engines / worker threads */
+    int32_t capacity_atoms;   /* largest request */
+    int64_t hbm_budget_bytes; /* admission limit on summed request footprints (0: no limit) */
+    int32_t lmax, lpol, precision;
+    double mscales[6], pscales[6], dscales[6];
+    int32_t solver;
+    double cg_tol;
+    int32_t max_iter;
+    int32_t use_graphs;
+} dmffb_server_desc;
+
+typedef struct {
+    /* inputs (host memory, alive until the request completes) */
+    int32_t n_atoms;
+    const double* pos;           /* [n*3] A */
+    double box[9];               /* A, rows = lattice vectors */
+    const int32_t* axis_types;   /* [n] */
+    const int32_t* axis_indices; /* [n*3] */
+    int64_t n_cov;
+    const int32_t* cov_rows;     /* [n_cov*3] */
+    const double* Q_local;       /* [n*9] */
+    const double* pol;           /* [n] or NULL */
+    const double* thole;         /* [n] or NULL */
+    double rc, kappa;
+    int32_t K[3];
+    double t_arrival;            /* seconds on the server clock; not admitted before */
+    /* outputs */
+    double* forces_out;          /* [n*3] host, -dE/dpos */
+    double energy;
+    double box_grad[9];
+    int32_t n_iter;
+    int32_t status;              /* DMFFB_* of the evaluation */
+    int32_t slot;
+    int32_t done;                /* set to 1 last */
+    double t_start, t_done;      /* server clock */
+    int64_t footprint_bytes;
+} dmffb_request;
+
+int dmffb_server_create(const dmffb_server_desc* desc, dmffb_server** out);
+/* Queue a request (non-blocking).  Requests must be submitted in non-decreasing t_arrival. */
+int dmffb_server_submit(dmffb_server* srv, dmffb_request* req);
+/* Block until every submitted request is done or timeout_s passes (DMFFB_CUDA_ERROR on timeout). */
+int dmffb_server_wait(dmffb_server* srv, double timeout_s);
+/* Seconds since the server was created (the clock of t_arrival / t_start / t_done). */
+double dmffb_server_clock(const dmffb_server* srv);
+/* Device bytes a request of this size is accounted for at admission. */
+int64_t dmffb_request_footprint(int32_t n_atoms, double rc, const int32_t K[3], double box_volume, int32_t lpol);
+/* Run each request once on every slot, untimed (grows buffers and caches cuFFT plans). */
+int dmffb_server_prewarm(dmffb_server* srv, dmffb_request* reqs, int32_t n_reqs);
+void dmffb_server_destroy(dmffb_server* srv);
 
 /* Neighbour-list build that allocates no device memory.  No counterpart in the reference (DMFF
  * has no C ABI); same result as dmffb_build_neighbors for callers that cannot allocate on

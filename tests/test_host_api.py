@@ -28,25 +28,25 @@ def test_header_symbols_exported_by_library():
 
 
 def test_ctypes_struct_layout_matches_header():
-    """the ctypes mirror of dmffb_admp_desc / dmffb_admp_result has the C layout (offsets via a
-    tiny C program compiled here)."""
-    src = r'''
-#include <stdio.h>
-#include <stddef.h>
-#include "dmffb200.h"
-int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(dmffb_admp_desc), offsetof(dmffb_admp_desc, cov_rows),
-         offsetof(dmffb_admp_desc, mscales), offsetof(dmffb_admp_desc, steps_pol), sizeof(dmffb_admp_result),
-         offsetof(dmffb_admp_result, n_pairs));
-  return 0; }'''
+    """every ctypes mirror of a header struct has the C layout: size and the offset of each field,
+    printed by a tiny C program compiled here against include/dmffb200.h."""
+    lines = []
+    for cname, cls in _lib.STRUCTS.items():
+        lines.append(f'  printf("%zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("%zu\\n", offsetof({cname}, {fname}));')
+    src = "#include <stdio.h>\n#include <stddef.h>\n#include \"dmffb200.h\"\nint main(void) {\n" + \
+          "\n".join(lines) + "\n  return 0; }\n"
     tmp = os.path.join(os.environ.get("TMPDIR", "/tmp"), "dmffb_layout")
     with open(tmp + ".c", "w") as f:
         f.write(src)
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), tmp + ".c", "-o", tmp], check=True)
     vals = [int(x) for x in subprocess.run([tmp], capture_output=True, text=True, check=True).stdout.split()]
-    D, Rr = _lib.AdmpDesc, _lib.AdmpResult
-    assert vals == [ctypes.sizeof(D), D.cov_rows.offset, D.mscales.offset, D.steps_pol.offset, ctypes.sizeof(Rr),
-                    Rr.n_pairs.offset]
+    want = []
+    for cls in _lib.STRUCTS.values():
+        want.append(ctypes.sizeof(cls))
+        want += [getattr(cls, fname).offset for fname, _ in cls._fields_]
+    assert vals == want
 
 
 def test_generator_parses_reference_xml_like_reference():
