@@ -38,6 +38,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="c1")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--serving-requests", type=int, default=300,
+                   help="requests of the serving stream measured beside the step (0: skip)")
+    p.add_argument("--serving-rates", default="100,500,2000", help="Poisson arrival rates (req/s)")
+    p.add_argument("--serving-slots", type=int, default=12)
+    p.add_argument("--serving-budget-gb", type=float, default=2.0)
     return p.parse_args()
 
 
@@ -199,6 +204,58 @@ def run_reference(args, s, rank):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------------------------- serving
+def make_serving_systems(n_req, seed=3):
+    """The serving stream's boxes (sizes log-uniform in [100, 10000] waters, seed 3), built in a
+    spawn process pool (started before this process touches CUDA)."""
+    import multiprocessing as mp
+    from dmff_b200.synthetic import serving_sizes, serving_system
+    sizes = serving_sizes(2000, seed=seed)[:n_req]
+    with mp.get_context("spawn").Pool(max(1, min(os.cpu_count() or 1, 32))) as pool:
+        return pool.starmap_async(serving_system, [(int(n), k) for k, n in enumerate(sizes)]).get(timeout=900)
+
+
+def bench_serving(args, systems, dev):
+    """Continuous-batching FP32 server vs the plain FP64 path (one request at a time, no graphs)
+    on the same requests; latency = completion - arrival."""
+    from dmff_b200.serving import AdmpServer, ServingRequest
+    from dmff_b200.synthetic import serving_arrivals
+    cap = max(s["n_atoms"] for s in systems)
+    by_k = {}
+    for s in systems:
+        by_k.setdefault(tuple(s["K"]), s)
+    warm = sorted(by_k.values(), key=lambda s: -s["n_atoms"])  # largest first: buffers grow once
+    out = {"requests": len(systems), "atoms": int(sum(s["n_atoms"] for s in systems)),
+           "sizes": "log-uniform 100-10000 waters (seed 3), 0.0334 molecules/A^3, rc 8 A (rc' = L/2 when L < 16 A)",
+           "slots": args.serving_slots, "hbm_budget_GB": args.serving_budget_gb,
+           "cg_tol_rel": 1e-6, "step": "polarizable ADMP energy + forces + virial, host buffers in and out"}
+    srv = AdmpServer(n_slots=args.serving_slots, capacity_atoms=cap, precision="fp32",
+                     hbm_budget_bytes=int(args.serving_budget_gb * (1 << 30)), device=dev)
+    srv.prewarm([ServingRequest(s) for s in warm])
+    reqs, st = srv.run_stream(systems, np.zeros(len(systems)))
+    out["offline_fp32"] = st
+    fp32 = reqs
+    for rate in [float(x) for x in args.serving_rates.split(",") if x]:
+        _, st = srv.run_stream(systems, serving_arrivals(len(systems), rate, seed=33))
+        out[f"poisson_{int(rate)}_per_s"] = st
+    srv.close()
+    # plain path: FP64, one slot, graphs off, every 5th request back to back
+    sub = systems[::5]
+    plain = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp64", use_graphs=False, cg_tol=1e-6, device=dev)
+    plain.prewarm([ServingRequest(s) for s in warm[:1]])
+    preqs, pst = plain.run_stream(sub, np.zeros(len(sub)))
+    plain.close()
+    out["plain_fp64"] = dict(pst, sample="every 5th request of the stream, one at a time")
+    out["speedup_vs_plain"] = out["offline_fp32"]["atom_evals_per_s"] / pst["atom_evals_per_s"]
+    errs_e, errs_f = [], []
+    for k, p in enumerate(preqs):
+        q = fp32[5 * k]
+        errs_e.append(abs(q.energy - p.energy) / abs(p.energy))
+        errs_f.append(float(np.sqrt(np.mean((q.forces - p.forces) ** 2)) / np.sqrt(np.mean(p.forces ** 2))))
+    out["fp32_vs_fp64"] = {"max_rel_energy": float(max(errs_e)), "max_rel_force_rms": float(max(errs_f))}
+    return out
+
+
 # ---------------------------------------------------------------------------------- GPU side
 def main():
     args = parse()
@@ -210,6 +267,9 @@ def main():
     if args.impl == "reference":
         run_reference(args, s, rank)
         return
+    serving_systems = None
+    if args.serving_requests > 0 and world == 1:
+        serving_systems = make_serving_systems(args.serving_requests)
     import torch
     import torch.distributed as dist
     from dmff_b200.engine import AdmpEngine
@@ -316,6 +376,8 @@ def main():
                 "sample": (f"one dE/dU pass ({t_g:.2f} s) and one energy+forces pass ({t_ef:.2f} s) of the same "
                            f"box with the float64 oracle; evaluation = E+F + {n_iter} dE/dU passes (the GPU's CG "
                            f"iteration count)")}
+        if serving_systems is not None:
+            out["serving"] = bench_serving(args, serving_systems, dev)
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()
