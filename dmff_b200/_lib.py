@@ -31,10 +31,10 @@ EXPORTED = [
     "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
     "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
     "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters", "dmffb_build_neighbors_noalloc",
-    "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads",
+    "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads", "dmffb_disp_set_param_grads",
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
-    "dmffb_set_graphs", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
+    "dmffb_set_graphs", "dmffb_admp_set_param_grads", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
     "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy",
 ]
 
@@ -228,6 +228,8 @@ def load():
     lib.dmffb_admp_compute_host.argtypes = [vp, vp, vp, vp, i64, vp, vp, P(AdmpResult)]
     lib.dmffb_admp_field.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp]
     lib.dmffb_admp_multipole_grads.argtypes = [vp, vp, vp, vp]
+    lib.dmffb_admp_set_param_grads.argtypes = [vp, i32]
+    lib.dmffb_admp_param_grads.argtypes = [vp, vp, vp, vp, vp, vp]
     lib.dmffb_build_neighbors.argtypes = [vp, vp, vp, vp, dbl, vp, i64, P(i64)]
     lib.dmffb_admp_build_neighbors.argtypes = [vp, vp, vp, vp]
     lib.dmffb_get_timings.argtypes = [vp, P(dbl), i32]
@@ -239,7 +241,8 @@ def load():
     lib.dmffb_disp_create.argtypes = [P(DispDesc), P(vp)]
     lib.dmffb_disp_set_params.argtypes = [vp, vp, vp, vp, vp]
     lib.dmffb_disp_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp, P(DispResult)]
-    lib.dmffb_disp_param_grads.argtypes = [vp, vp, vp]
+    lib.dmffb_disp_param_grads.argtypes = [vp, vp, vp, vp]
+    lib.dmffb_disp_set_param_grads.argtypes = [vp, i32]
     lib.dmffb_classical_create.argtypes = [P(ClassicalDesc), P(vp)]
     lib.dmffb_classical_set_params.argtypes = [vp, vp, vp, vp, vp]
     lib.dmffb_classical_set_terms.argtypes = [vp, i32, i64, vp, vp]

@@ -44,16 +44,24 @@ class ADMPDispPmeForce:
             box = torch.as_tensor(np.asarray(box), dtype=torch.float64)
         eng = self._eng(positions.shape[0], mScales)
         eng.set_params(c_list, *(tt if tt is not None else (None, None, None)))
-        return _DispEnergy.apply(positions, box, eng, _as_cuda_pairs(pairs, eng.device), self, tt is not None)
+        c_list = torch.as_tensor(c_list, dtype=torch.float64)
+        a, b, q = (None, None, None) if tt is None else (torch.as_tensor(x, dtype=torch.float64) for x in tt)
+        return _DispEnergy.apply(positions, box, c_list, a, b, q, eng, _as_cuda_pairs(pairs, eng.device), self,
+                                 tt is not None)
 
 
 class _DispEnergy(torch.autograd.Function):
+    """E_lr, or E_sr - E_lr with TT damping, of (positions, box, c_list, a, b, q); backward gives
+    position / box gradients and, when the parameter tensors require grad, the engine's
+    parameter adjoints."""
+
     @staticmethod
-    def forward(ctx, positions, box, eng, pairs, force, with_tt):
+    def forward(ctx, positions, box, c_list, a, b, q, eng, pairs, force, with_tt):
         pos = positions.detach().to(device=eng.device, dtype=torch.float64).contiguous()
+        want_p = any(ctx.needs_input_grad[2:6])
+        eng.set_param_grads(want_p)
         res, F = eng.compute(pos, box, pairs=pairs)
         force.last_result = res
-        sign = 1.0 if with_tt else 1.0
         E = (res.e_sr - res.energy) if with_tt else res.energy
         g_sr = torch.tensor(list(res.box_grad_sr), dtype=torch.float64).reshape(3, 3)
         g_lr = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
@@ -63,11 +71,26 @@ class _DispEnergy(torch.autograd.Function):
         ctx.save_for_backward(grad.clone())
         ctx.box_grad = (g_sr - g_lr) if with_tt else g_lr
         ctx.devs = (positions.device, box.device)
-        del sign
+        ctx.pdevs = [None if t is None else t.device for t in (c_list, a, b, q)]
+        ctx.with_tt = with_tt
+        ctx.pg = None
+        if want_p:
+            pg = eng.param_grads()
+            if with_tt:
+                dc = -pg["c"].clone()
+                dc[:, 0] += pg["c6"]
+                ctx.pg = (dc, pg["a"], pg["b"], pg["q"])
+            else:
+                ctx.pg = (pg["c"], None, None, None)
         return torch.tensor(E, dtype=torch.float64, device=positions.device)
 
     @staticmethod
     def backward(ctx, g):
         (grad,) = ctx.saved_tensors
+        outs = [None] * 4
+        if ctx.pg is not None:
+            for k, t in enumerate(ctx.pg):
+                if t is not None and ctx.pdevs[k] is not None:
+                    outs[k] = (t * g.to(t.device)).to(ctx.pdevs[k])
         return ((grad * g.to(grad.device)).to(ctx.devs[0]), (ctx.box_grad.to(ctx.devs[1]) * g.to(ctx.devs[1])),
-                None, None, None, None)
+                *outs, None, None, None, None)

@@ -56,17 +56,23 @@ def _as_cuda_pairs(pairs, device):
 
 
 class _AdmpEnergy(torch.autograd.Function):
-    """E(positions, box); backward returns -forces and dE/dbox from the engine's forward pass."""
+    """E(positions, box, Q_local, pol, tholes); backward returns -forces, dE/dbox and, when the
+    parameter tensors require grad, the engine's parameter adjoints (dE/dQ_local, dE/dpol,
+    dE/dthole at the converged dipoles, where E is stationary in U)."""
 
     @staticmethod
-    def forward(ctx, positions, box, force, pairs, U0, aux):
-        dev = force.engine.device
+    def forward(ctx, positions, box, Q_local, pol, tholes, force, pairs, U0, aux):
+        eng = force.engine
+        dev = eng.device
         pos = positions.detach().to(device=dev, dtype=torch.float64).contiguous()
+        want = [t is not None and torch.is_tensor(t) and t.requires_grad for t in (Q_local, pol, tholes)]
+        want_p = any(ctx.needs_input_grad[2:5]) and any(want)
+        eng.set_param_grads(want_p)
         U = None
         if force.lpol:
             U = (U0.detach().to(device=dev, dtype=torch.float64).contiguous().clone() if U0 is not None
                  else torch.zeros((force.n_atoms, 3), dtype=torch.float64, device=dev))
-        res, forces, U = force.engine.compute(pos, box, pairs=pairs, U=U)
+        res, forces, U = eng.compute(pos, box, pairs=pairs, U=U)
         force.last_result = res
         if aux is not None:
             aux["U_ind_A"] = U
@@ -75,6 +81,8 @@ class _AdmpEnergy(torch.autograd.Function):
         ctx.save_for_backward(forces.clone())
         ctx.box_grad = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
         ctx.pos_device, ctx.box_device = positions.device, box.device if torch.is_tensor(box) else None
+        ctx.pg = eng.param_grads() if want_p else None
+        ctx.pshapes = [None if t is None else (tuple(t.shape), t.device) for t in (Q_local, pol, tholes)]
         return torch.tensor(res.energy, dtype=torch.float64, device=positions.device)
 
     @staticmethod
@@ -84,7 +92,16 @@ class _AdmpEnergy(torch.autograd.Function):
         gbox = None
         if ctx.box_device is not None:
             gbox = (ctx.box_grad.to(ctx.box_device) * g.to(ctx.box_device))
-        return gpos, gbox, None, None, None, None
+        gq = gp = gt = None
+        if ctx.pg is not None:
+            if ctx.pshapes[0] is not None:
+                shp, dv = ctx.pshapes[0]
+                gq = (ctx.pg["Q_local"][:, : shp[1]] * g.to(ctx.pg["Q_local"].device)).to(dv)
+            if ctx.pshapes[1] is not None:
+                gp = (ctx.pg["pol"] * g.to(ctx.pg["pol"].device)).to(ctx.pshapes[1][1])
+            if ctx.pshapes[2] is not None:
+                gt = (ctx.pg["thole"] * g.to(ctx.pg["thole"].device)).to(ctx.pshapes[2][1])
+        return gpos, gbox, gq, gp, gt, None, None, None, None
 
 
 class ADMPPmeForce:
@@ -129,12 +146,17 @@ class ADMPPmeForce:
         return self._engine
 
     def _sync_params(self, Q_local, pol, tholes, mScales, pScales, dScales):
-        key = tuple(None if t is None else (t.data_ptr() if torch.is_tensor(t) else id(t), getattr(t, "_version", 0))
-                    for t in (Q_local, pol, tholes)) + tuple(
-            tuple(np.asarray(torch.as_tensor(s).detach().cpu()).tolist()) if s is not None else None
-            for s in (mScales, pScales, dScales))
-        if key == self._param_key:
+        # keyed by value: a fresh tensor can reuse a freed one's address, so identity is not enough
+        vals = tuple(None if t is None else torch.as_tensor(t, dtype=torch.float64).detach().cpu().clone()
+                     for t in (Q_local, pol, tholes))
+        scales = tuple(tuple(np.asarray(torch.as_tensor(s).detach().cpu()).tolist()) if s is not None else None
+                       for s in (mScales, pScales, dScales))
+        old = self._param_key
+        if old is not None and old[1] == scales and all(
+                (a is None and b is None) or (a is not None and b is not None and a.shape == b.shape and torch.equal(a, b))
+                for a, b in zip(old[0], vals)):
             return
+        key = (vals, scales)
         eng = self.engine
         d = eng.lib  # scales are part of the description: rebuild when they change
         ms = np.asarray(torch.as_tensor(mScales).detach().cpu(), np.float64)
@@ -169,5 +191,11 @@ class ADMPPmeForce:
         if self.lpol:
             U0 = U_init if U_init is not None else self.U_ind
             U0 = torch.as_tensor(U0, dtype=torch.float64)
-        E = _AdmpEnergy.apply(positions, box, self, pairs_d, U0, aux)
+        Q_local = torch.as_tensor(Q_local, dtype=torch.float64)
+        if self.lpol:
+            pol = torch.as_tensor(pol, dtype=torch.float64)
+            tholes = torch.as_tensor(tholes, dtype=torch.float64)
+        else:
+            pol = tholes = None
+        E = _AdmpEnergy.apply(positions, box, Q_local, pol, tholes, self, pairs_d, U0, aux)
         return E

@@ -239,6 +239,84 @@ __global__ void __launch_bounds__(128) k_self_frames(SelfArgs<T> a) {
     block_reduce_add<11>(red, a.scal);
 }
 
+// Per-atom end of the parameter adjoints (after the pair pass and the reciprocal gather have
+// accumulated dE/dQ_global into dQ): the Ewald self term's -2 D f_l (Q + U) (pme.py:1183-1222),
+// dE/dpol from the penalty D |U|^2 / (2 pol) (pme.py:1225-1240, zero where pol is clamped at 1e-8)
+// plus the pair damping sum dpa (-dpa / (6 pol)), and dE/dQ_local as the transpose of the
+// local -> global rotation k_prepare applies (rot_local2global, multipole.py:218-236).
+struct LocalGradArgs {
+    FrameArgs f;
+    const double* Qg;     // [n*9]
+    const double* U;      // [n*3] or null
+    const double* pol;    // [n] or null
+    const double* dpa;    // [n] or null
+    double kappa;
+    int lmax, lmax_eff, lpme;
+    double* dQ;           // [n*9] in: dE/dQ_global (pair + reciprocal), out: + self
+    double* dQloc;        // [n*9] out: dE/dQ_local
+    double* dpol;         // [n] out (may be null)
+};
+
+__global__ void __launch_bounds__(128) k_local_grad(LocalGradArgs a) {
+    const int at = blockIdx.x * blockDim.x + threadIdx.x;
+    if (at >= a.f.n) return;
+    const double D = DMFFB_DIELECTRIC;
+    double g[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) g[k] = a.dQ[9 * at + k];
+    double Ux = 0, Uy = 0, Uz = 0;
+    if (a.U) { Ux = a.U[3 * at]; Uy = a.U[3 * at + 1]; Uz = a.U[3 * at + 2]; }
+    if (a.lpme) {
+        const double k = a.kappa;
+        const double f0 = k / 1.7724538509055159;
+        const double f1 = f0 * 2.0 * k * k / 3.0;
+        const double f2 = f0 * 4.0 * k * k * k * k / 15.0;
+        double Qt[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) Qt[q] = a.Qg[9 * at + q];
+        Qt[1] += Uz; Qt[2] += Ux; Qt[3] += Uy;
+        g[0] += -2.0 * D * f0 * Qt[0];
+        if (a.lmax_eff >= 1)
+            for (int q = 1; q < 4; ++q) g[q] += -2.0 * D * f1 * Qt[q];
+        if (a.lmax_eff >= 2)
+            for (int q = 4; q < 9; ++q) g[q] += -2.0 * D * f2 * Qt[q];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a.dQ[9 * at + k] = g[k];
+    if (a.dpol) {
+        const double p = a.pol ? a.pol[at] : 0.0;
+        double d = 0.0;
+        if (a.U && p >= 1e-8) d += -0.5 * D * (Ux * Ux + Uy * Uy + Uz * Uz) / (p * p);
+        if (a.dpa && p > 0.0) d += -a.dpa[at] / (6.0 * p);
+        a.dpol[at] = d;
+    }
+    double gl[9];
+    if (a.lmax == 0) {
+        for (int k = 0; k < 9; ++k) gl[k] = k == 0 ? g[0] : 0.0;
+    } else {
+        V3D X, Y, Z;
+        double nimg[3][3];
+        double F[3][3];
+        if (build_frame(a.f, at, -1, 0, X, Y, Z, nimg)) {
+            F[0][0] = X.x.v; F[0][1] = X.y.v; F[0][2] = X.z.v;
+            F[1][0] = Y.x.v; F[1][1] = Y.y.v; F[1][2] = Y.z.v;
+            F[2][0] = Z.x.v; F[2][1] = Z.y.v; F[2][2] = Z.z.v;
+        } else {
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) F[r][c] = r == c ? 1.0 : 0.0;
+        }
+        const double ex[3] = {F[0][0], F[1][0], F[2][0]};
+        const double ey[3] = {F[0][1], F[1][1], F[2][1]};
+        const double ez[3] = {F[0][2], F[1][2], F[2][2]};
+        double C[5][5];
+        quad_rot<double>(ex, ey, ez, C);
+        rot9T<double>(g, ex, ey, ez, C, gl);
+        if (a.lmax < 2) for (int k = 4; k < 9; ++k) gl[k] = 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a.dQloc[9 * at + k] = gl[k];
+}
+
 // forces = -(pair gradient + everything accumulated in FP64)
 template <typename T>
 __global__ void k_finalize_forces(int n, const T* gpair, const double* gd, double* forces) {

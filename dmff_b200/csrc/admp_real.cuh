@@ -341,6 +341,152 @@ __device__ __forceinline__ void pair_eval(const TC dr[3], const TC* QIg, const T
     e = (double)Ev;
 }
 
+// transpose of rot9: the global-frame gradient G of a function of the frame components q
+template <typename T>
+__device__ __forceinline__ void rot9T(const T* g, const T ex[3], const T ey[3], const T ez[3], const T C[5][5], T G[9]) {
+    G[0] = g[0];
+    // q1 = ez.d, q2 = ex.d, q3 = ey.d with d = (Q2, Q3, Q1) Cartesian
+    const T cx = ez[0] * g[1] + ex[0] * g[2] + ey[0] * g[3];
+    const T cy = ez[1] * g[1] + ex[1] * g[2] + ey[1] * g[3];
+    const T cz = ez[2] * g[1] + ex[2] * g[2] + ey[2] * g[3];
+    G[1] = cz;
+    G[2] = cx;
+    G[3] = cy;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        T s = T(0);
+#pragma unroll
+        for (int j = 0; j < 5; ++j) s += C[j][k] * g[4 + j];
+        G[4 + k] = s;
+    }
+}
+
+// Parameter adjoints of one pair at fixed (converged) induced dipoles: dE/dQ_global of both
+// sites (9 each), and for the Thole damping dE/d(au) times au (-> dE/dpol through
+// dmp = (pol_i pol_j)^(1/6)) and times u (-> dE/dthole when the width is thole_i + thole_j).
+// The damped coefficients are differentiated in au with value+slope pairs: d/dau of
+// e^-au P(au) = e^-au (P' - P).
+template <typename TC, bool POL>
+__device__ __forceinline__ void pair_eval_pgrad(const TC dr[3], const TC* QIg, const TC* QJg, const TC UI[3],
+                                                const TC UJ[3], TC m, TC pp, TC dsv, TC Ath, TC dmp, TC kap,
+                                                TC GI[9], TC GJ[9], TC& dau_au, TC& dau_u) {
+    const TC D = TC(DMFFB_DIELECTRIC);
+    const TC r2 = dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2];
+    const TC rinv = d_rsqrt(r2);
+    const TC r = r2 * rinv;
+    TC ez[3] = {dr[0] * rinv, dr[1] * rinv, dr[2] * rinv};
+    const TC av = kap * r;
+    const TC a2v = av * av;
+    const TC Xv = TC(DMFFB_TWO_OVER_SQRTPI) * d_exp(-a2v);
+    const TC ERFC = d_erfc(av);
+    const TC t2 = av * Xv;
+    const TC a3X = a2v * t2;
+    const TC t3 = TC(2.0 / 3.0) * a3X;
+    const TC a5X = a2v * a3X;
+    const TC t4 = TC(4.0 / 15.0) * a5X;
+    const TC R1 = rinv, R2 = rinv * rinv, R3 = R2 * rinv, R4 = R2 * R2, R5 = R4 * rinv;
+    TC ex[3], ey[3];
+    qi_frame(ez, ex, ey);
+    TC C[5][5];
+    quad_rot(ex, ey, ez, C);
+    TC qI[9], qJ[9];
+    rot9(QIg, ex, ey, ez, C, qI);
+    rot9(QJg, ex, ey, ez, C, qJ);
+    const TC b2m = (m - TC(1)) + (ERFC + t2);
+    const TC b3m = b2m + t3;
+    const TC b4m = b3m + t4;
+    const TC cc = D * (R1 * ((m - TC(1)) + ERFC));
+    const TC cd = D * (R2 * b2m);
+    const TC dd0 = TC(-2.0 / 3.0 * DMFFB_DIELECTRIC) * (R3 * (TC(3) * b3m + a3X));
+    const TC dd1 = D * (R3 * (b3m - TC(2.0 / 3.0) * a3X));
+    const TC cq = D * (R3 * b3m);
+    const TC dq0 = D * (R4 * (TC(3) * b3m + TC(4.0 / 3.0) * a5X));
+    const TC dq1 = TC(-DMFFB_SQRT3 * DMFFB_DIELECTRIC) * (R4 * b3m);
+    const TC qq0 = D * (R5 * (TC(6) * b4m + TC(4.0 / 45.0) * ((TC(-3) + TC(10) * a2v) * a5X)));
+    const TC qq1 = TC(-4.0 / 15.0 * DMFFB_DIELECTRIC) * (R5 * (TC(15) * b4m + a5X));
+    const TC qq2 = D * (R5 * (b4m - TC(4.0 / 15.0) * a5X));
+    TC gI[9], gJ[9];
+    gI[0] = cc * qJ[0] + cd * qJ[1] + cq * qJ[4];
+    gI[1] = -cd * qJ[0] + dd0 * qJ[1] - dq0 * qJ[4];
+    gI[2] = dd1 * qJ[2] - dq1 * qJ[5];
+    gI[3] = dd1 * qJ[3] - dq1 * qJ[6];
+    gI[4] = cq * qJ[0] + dq0 * qJ[1] + qq0 * qJ[4];
+    gI[5] = dq1 * qJ[2] + qq1 * qJ[5];
+    gI[6] = dq1 * qJ[3] + qq1 * qJ[6];
+    gI[7] = qq2 * qJ[7];
+    gI[8] = qq2 * qJ[8];
+    gJ[0] = cc * qI[0] - cd * qI[1] + cq * qI[4];
+    gJ[1] = cd * qI[0] + dd0 * qI[1] + dq0 * qI[4];
+    gJ[2] = dd1 * qI[2] + dq1 * qI[5];
+    gJ[3] = dd1 * qI[3] + dq1 * qI[6];
+    gJ[4] = cq * qI[0] - dq0 * qI[1] + qq0 * qI[4];
+    gJ[5] = qq1 * qI[5] - dq1 * qI[2];
+    gJ[6] = qq1 * qI[6] - dq1 * qI[3];
+    gJ[7] = qq2 * qI[7];
+    gJ[8] = qq2 * qI[8];
+    dau_au = dau_u = TC(0);
+    if (POL) {
+        TC uI[3], uJ[3];
+        uI[0] = ez[0] * UI[0] + ez[1] * UI[1] + ez[2] * UI[2];
+        uI[1] = ex[0] * UI[0] + ex[1] * UI[1] + ex[2] * UI[2];
+        uI[2] = ey[0] * UI[0] + ey[1] * UI[1] + ey[2] * UI[2];
+        uJ[0] = ez[0] * UJ[0] + ez[1] * UJ[1] + ez[2] * UJ[2];
+        uJ[1] = ex[0] * UJ[0] + ex[1] * UJ[1] + ex[2] * UJ[2];
+        uJ[2] = ey[0] * UJ[0] + ey[1] * UJ[1] + ey[2] * UJ[2];
+        TC u = r / dmp;
+        const bool u_live = u < TC(1e8);
+        if (!u_live) u = TC(1e8);
+        const Dl<TC> au(Ath * u, TC(1));
+        Dl<TC> ee(TC(0), TC(0));
+        if (au.v < TC(50)) {
+            const TC ev = d_exp(-au.v);
+            ee = Dl<TC>(ev, -ev);
+        }
+        const Dl<TC> au2 = au * au;
+        const Dl<TC> au3 = au2 * au;
+        const Dl<TC> Pc = TC(1) + (au + TC(0.5) * au2);
+        const Dl<TC> Pd0 = Pc + TC(0.25) * au3;
+        const Dl<TC> Pq1 = Pc + TC(1.0 / 6.0) * au3;
+        const Dl<TC> Pq0 = Pq1 + TC(1.0 / 18.0) * (au3 * au);
+        const TC base2 = ERFC + t2, base3 = base2 + t3;
+        const Dl<TC> eP_c = ee * Pc, eP_d0 = ee * Pd0, eP_q0 = ee * Pq0, eP_q1 = ee * Pq1;
+        const Dl<TC> bc2 = Dl<TC>((pp - TC(1)) + base2, TC(0)) - pp * eP_c;
+        const Dl<TC> bc3 = Dl<TC>((pp - TC(1)) + base3, TC(0)) - pp * eP_c;
+        const Dl<TC> bd0 = Dl<TC>((pp - TC(1)) + base3, TC(0)) - pp * eP_d0;
+        const Dl<TC> bq0 = Dl<TC>((pp - TC(1)) + base3, TC(0)) - pp * eP_q0;
+        const Dl<TC> bq1 = Dl<TC>((pp - TC(1)) + base3, TC(0)) - pp * eP_q1;
+        const Dl<TC> ed0 = Dl<TC>((dsv - TC(1)) + base3, TC(0)) - dsv * eP_d0;
+        const Dl<TC> ed1 = Dl<TC>((dsv - TC(1)) + base3, TC(0)) - dsv * eP_c;
+        const Dl<TC> cud = TC(2 * DMFFB_DIELECTRIC) * R2 * bc2;
+        const Dl<TC> dud0 = TC(-4.0 / 3.0 * DMFFB_DIELECTRIC) * R3 * (TC(3) * bd0 + a3X);
+        const Dl<TC> dud1 = TC(2 * DMFFB_DIELECTRIC) * R3 * (bc3 - TC(2.0 / 3.0) * a3X);
+        const Dl<TC> udq0 = TC(2 * DMFFB_DIELECTRIC) * R4 * (TC(3) * bq0 + TC(4.0 / 3.0) * a5X);
+        const Dl<TC> udq1 = TC(-2 * DMFFB_SQRT3 * DMFFB_DIELECTRIC) * R4 * bq1;
+        const Dl<TC> udud0 = TC(-2.0 / 3.0 * DMFFB_DIELECTRIC) * R3 * (TC(3) * ed0 + a3X);
+        const Dl<TC> udud1 = D * R3 * (ed1 - TC(2.0 / 3.0) * a3X);
+        const Dl<TC> hJ[7] = {TC(-0.5) * (cud * uI[0]), TC(0.5) * (dud0 * uI[0]), TC(0.5) * (dud1 * uI[1]),
+                              TC(0.5) * (dud1 * uI[2]), TC(-0.5) * (udq0 * uI[0]), TC(-0.5) * (udq1 * uI[1]),
+                              TC(-0.5) * (udq1 * uI[2])};
+        const Dl<TC> hI[7] = {TC(0.5) * (cud * uJ[0]), TC(0.5) * (dud0 * uJ[0]), TC(0.5) * (dud1 * uJ[1]),
+                              TC(0.5) * (dud1 * uJ[2]), TC(0.5) * (udq0 * uJ[0]), TC(0.5) * (udq1 * uJ[1]),
+                              TC(0.5) * (udq1 * uJ[2])};
+        TC dEd = TC(0);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            gJ[k] += hJ[k].v;
+            gI[k] += hI[k].v;
+            dEd += qJ[k] * hJ[k].d + qI[k] * hI[k].d;
+        }
+        dEd += udud0.d * uI[0] * uJ[0] + udud1.d * (uI[1] * uJ[1] + uI[2] * uJ[2]);
+        if (u_live) {
+            dau_au = dEd * au.v;
+            dau_u = dEd * u;
+        }
+    }
+    rot9T(gI, ex, ey, ez, C, GI);
+    rot9T(gJ, ex, ey, ez, C, GJ);
+}
+
 // load one row's inputs in arithmetic TC and evaluate it
 template <typename TC, typename T, bool POL, int MODE>
 __device__ __forceinline__ void pair_row(const PairArgs<T>& a, int i, int j, int nb, TC oi[6], TC oj[6], double& e,
@@ -464,6 +610,96 @@ __global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
     }
 }
 
+
+// Parameter-adjoint pass (param grads requested): per pair, dE/dQ_global of both sites and the
+// Thole damping sums; at the converged dipoles E is stationary in U, so these partials are the
+// total derivatives.  Outputs (FP64 atomics): dQ [n*9] += dE/dQ_global; dpa [n] += sum of
+// dE/d(au) au over the atom's pairs (dE/dpol_i = -dpa_i / (6 pol_i), zero where dmp or u is
+// clamped); dth [n] += sum of dE/d(au) u over pairs whose Thole width is thole_i + thole_j.
+template <typename T>
+struct PgradArgs {
+    PairArgs<T> p;
+    double* dQ;
+    double* dpa;
+    double* dth;
+};
+
+template <typename TC, typename T, bool POL>
+__device__ __forceinline__ void pgrad_row(const PairArgs<T>& a, int i, int j, int nb, double oi[11], double oj[11]) {
+    TC dr[3];
+    if (sizeof(TC) > sizeof(T)) {
+        for (int c = 0; c < 3; ++c) dr[c] = (TC)(a.posd[3 * i + c] - a.posd[3 * j + c]);
+    } else {
+        for (int c = 0; c < 3; ++c) dr[c] = (TC)(a.pos[4 * i + c] - a.pos[4 * j + c]);
+    }
+    BoxT<TC> bx;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { bx.h[k] = (TC)a.boxd.h[k]; bx.hinv[k] = (TC)a.boxd.hinv[k]; }
+    TC nimg[3];
+    pbc_shift(bx, dr[0], dr[1], dr[2], nimg);
+    int sidx = nb - 1;
+    if (sidx < 0) sidx += 6;
+    sidx = sidx < 0 ? 0 : (sidx > 5 ? 5 : sidx);
+    TC QI[9], QJ[9];
+    if (sizeof(TC) > sizeof(T)) {
+        for (int k = 0; k < 9; ++k) { QI[k] = (TC)a.Qgd[9 * i + k]; QJ[k] = (TC)a.Qgd[9 * j + k]; }
+    } else {
+        for (int k = 0; k < 9; ++k) { QI[k] = (TC)a.Qg[9 * i + k]; QJ[k] = (TC)a.Qg[9 * j + k]; }
+    }
+    TC UI[3] = {TC(0), TC(0), TC(0)}, UJ[3] = {TC(0), TC(0), TC(0)};
+    if (POL && a.U)
+        for (int c = 0; c < 3; ++c) { UI[c] = (TC)a.U[3 * i + c]; UJ[c] = (TC)a.U[3 * j + c]; }
+    TC Ath = TC(0), dmp = TC(1);
+    bool dmp_live = true;
+    const TC pp = (TC)a.ps[sidx], dsv = (TC)a.dsc[sidx];
+    if (POL) {
+        Ath = pp > TC(0) ? TC(5.0) : (TC)a.thole[i] + (TC)a.thole[j];
+        dmp = (TC)a.polsix[i] * (TC)a.polsix[j];
+        if (dmp < TC(1e-8)) { dmp = TC(1e-8); dmp_live = false; }
+    }
+    TC GI[9], GJ[9], dau_au, dau_u;
+    pair_eval_pgrad<TC, POL>(dr, QI, QJ, UI, UJ, (TC)a.ms[sidx], pp, dsv, Ath, dmp, (TC)a.kappa, GI, GJ, dau_au, dau_u);
+    for (int k = 0; k < 9; ++k) { oi[k] = (double)GI[k]; oj[k] = (double)GJ[k]; }
+    oi[9] = oj[9] = dmp_live ? (double)dau_au : 0.0;
+    oi[10] = oj[10] = (POL && !(pp > TC(0))) ? (double)dau_u : 0.0;
+}
+
+template <typename T, bool POL, int ROWS = ROWS_ALL>
+__global__ void __launch_bounds__(128) k_admp_pgrad(PgradArgs<T> g) {
+    const PairArgs<T>& a = g.p;
+    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int i = -1, j = -1, nb = 0;
+    if (row < a.npairs) {
+        i = a.pairs[3 * row];
+        j = a.pairs[3 * row + 1];
+        nb = a.pairs[3 * row + 2];
+    }
+    const bool valid = (row < a.npairs) && i >= 0 && i < j && j < a.n &&
+                       (ROWS == ROWS_ALL || (ROWS == ROWS_UNSCALED) == (nb == 0));
+    const int key = valid ? i : -1;
+    double oi[11], oj[11];
+#pragma unroll
+    for (int k = 0; k < 11; ++k) { oi[k] = 0.0; oj[k] = 0.0; }
+    if (valid) {
+        if (sizeof(T) < sizeof(double) && nb != 0) pgrad_row<double, T, POL>(a, i, j, nb, oi, oj);
+        else pgrad_row<T, T, POL>(a, i, j, nb, oi, oj);
+    }
+    const bool head = seg_head(key);
+    const int run = seg_run_id(key);
+#pragma unroll
+    for (int k = 0; k < 11; ++k) {
+        if (!POL && k >= 9) break;
+        const double s = seg_sum(oi[k], run);
+        if (head && key >= 0) {
+            double* dst = k < 9 ? g.dQ + 9 * key + k : (k == 9 ? g.dpa + key : g.dth + key);
+            atomicAdd(dst, s);
+        }
+        if (valid) {
+            double* dst = k < 9 ? g.dQ + 9 * j + k : (k == 9 ? g.dpa + j : g.dth + j);
+            atomicAdd(dst, oj[k]);
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------------------------
 // Induced-dipole matrix-vector product for the CG solve, atomics-free: a full (both-direction)

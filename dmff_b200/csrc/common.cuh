@@ -38,6 +38,9 @@ template <typename T> __device__ __forceinline__ Dl<T> operator*(Dl<T> a, Dl<T> 
 template <typename T> __device__ __forceinline__ Dl<T> operator*(T s, Dl<T> a) { return Dl<T>(s * a.v, s * a.d); }
 template <typename T> __device__ __forceinline__ Dl<T> operator+(T s, Dl<T> a) { return Dl<T>(s + a.v, a.d); }
 template <typename T> __device__ __forceinline__ Dl<T> operator-(Dl<T> a) { return Dl<T>(-a.v, -a.d); }
+template <typename T> __device__ __forceinline__ Dl<T> operator*(Dl<T> a, T s) { return Dl<T>(a.v * s, a.d * s); }
+template <typename T> __device__ __forceinline__ Dl<T> operator+(Dl<T> a, T s) { return Dl<T>(a.v + s, a.d); }
+template <typename T> __device__ __forceinline__ Dl<T> operator-(Dl<T> a, T s) { return Dl<T>(a.v - s, a.d); }
 
 // ------------------------------------------------------------------ warp helpers
 __device__ __forceinline__ double warp_sum(double v) {

@@ -31,7 +31,58 @@ struct DispArgs {
     T* grad_lr;          // [n*3] dE_lr/dpos
     T* grad_sr;          // [n*3] dE_sr/dpos (TT)
     double* scal;        // [0] E_lr real, [1] E_sr, [2..10] box grad lr, [11..19] box grad sr
+    double* dlr;         // [3][n] += dE_lr/dc (channel-major), parameter adjoints, or null
+    double* dsr;         // [4][n] += dE_sr/d(a, b, q, c6), or null
 };
+
+// Parameter partials of one pair: dE_lr/dc_i^p and dE_lr/dc_j^p (p = 6, 8, 10; the real-space
+// factor (m + g_p - 1) / r^p times the partner's c), and for the TT term dE_sr/d(a, b, q, c6) of
+// both sites through a = sqrt(a_i a_j), b = sqrt(b_i b_j), q = q_i q_j, c = c6_i c6_j.  With
+// x = b r_b, the truncated exponential sum obeys d/dx [e^-x P6(x)] = -e^-x x^6 / 720.
+template <typename TC>
+__device__ __forceinline__ void disp_pgrad(TC r, TC m, const TC ci[3], const TC cj[3], TC kap, int pmax, bool tt, TC ai,
+                                           TC aj, TC bi, TC bj, TC qi, TC qj, TC li[3], TC lj[3], TC si[4], TC sj[4]) {
+    const TC x2 = kap * kap * r * r;
+    const TC e = d_exp(-x2);
+    const TC rinv2 = TC(1) / (r * r);
+    const TC rinv6 = rinv2 * rinv2 * rinv2;
+    const TC x4 = x2 * x2;
+    const TC P6 = TC(1) + x2 + TC(0.5) * x4;
+    const TC P8 = P6 + TC(1.0 / 6.0) * x4 * x2;
+    const TC P10 = P8 + TC(1.0 / 24.0) * x4 * x4;
+    const TC f6 = ((m - TC(1)) + e * P6) * rinv6;
+    const TC f8 = ((m - TC(1)) + e * P8) * rinv6 * rinv2;
+    const TC f10 = ((m - TC(1)) + e * P10) * rinv6 * rinv2 * rinv2;
+    li[0] = f6 * cj[0];
+    lj[0] = f6 * ci[0];
+    li[1] = pmax >= 8 ? f8 * cj[1] : TC(0);
+    lj[1] = pmax >= 8 ? f8 * ci[1] : TC(0);
+    li[2] = pmax >= 10 ? f10 * cj[2] : TC(0);
+    lj[2] = pmax >= 10 ? f10 * ci[2] : TC(0);
+    for (int k = 0; k < 4; ++k) si[k] = sj[k] = TC(0);
+    if (tt) {
+        const TC BOHR = TC(1.889726878);
+        const TC a = d_sqrt(ai * aj), b = d_sqrt(bi * bj), c = ci[0] * cj[0], q = qi * qj;
+        const TC rb = r * BOHR;
+        const TC br = b * rb;
+        const TC eb = d_exp(-br);
+        const TC br2 = br * br, br3 = br2 * br, br6 = br3 * br3;
+        const TC poly = TC(1) + br + TC(0.5) * br2 + TC(1.0 / 6.0) * br3 + TC(1.0 / 24.0) * (br2 * br2) +
+                        TC(1.0 / 120.0) * (br3 * br2) + TC(1.0 / 720.0) * br6;
+        const TC dfa = m * TC(2625.5) * eb;                          // dE/da
+        const TC dfq = -m * TC(2625.5) * eb * (TC(1) + br) / rb;     // dE/dq
+        const TC dfc = m * eb * poly * rinv6;                        // dE/dc
+        const TC dfb = m * rb * (-TC(2625.5) * a * eb + TC(2625.5) * q * eb * br / rb - c * eb * br6 / TC(720) * rinv6);
+        si[0] = a > TC(0) ? dfa * aj / (TC(2) * a) : TC(0);
+        sj[0] = a > TC(0) ? dfa * ai / (TC(2) * a) : TC(0);
+        si[1] = b > TC(0) ? dfb * bj / (TC(2) * b) : TC(0);
+        sj[1] = b > TC(0) ? dfb * bi / (TC(2) * b) : TC(0);
+        si[2] = dfq * qj;
+        sj[2] = dfq * qi;
+        si[3] = dfc * cj[0];
+        sj[3] = dfc * ci[0];
+    }
+}
 
 template <typename TC>
 __device__ __forceinline__ void disp_eval(TC r, TC m, const TC ci[3], const TC cj[3], TC kap, int pmax, bool tt,
@@ -150,7 +201,54 @@ __global__ void __launch_bounds__(128) k_disp_pair(DispArgs<T> a) {
             if (TT) atomicAdd(a.grad_sr + 3 * j + c, -gs[c]);
         }
     }
+    if (a.dlr) {  // parameter adjoints (FP64, i-side segmented sums, j-side atomics)
+        double pi_[7], pj_[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) pi_[k] = pj_[k] = 0.0;
+        if (valid) {
+            double dv[3] = {a.pos[3 * i] - a.pos[3 * j], a.pos[3 * i + 1] - a.pos[3 * j + 1], a.pos[3 * i + 2] - a.pos[3 * j + 2]};
+            BoxT<double> bx;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) { bx.h[k] = a.boxd.h[k]; bx.hinv[k] = a.boxd.hinv[k]; }
+            double nim[3];
+            pbc_shift(bx, dv[0], dv[1], dv[2], nim);
+            const double r = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+            int sidx = nb - 1;
+            if (sidx < 0) sidx += 6;
+            sidx = sidx < 0 ? 0 : (sidx > 5 ? 5 : sidx);
+            const double ci[3] = {(double)a.c[i], (double)a.c[a.n + i], (double)a.c[2 * a.n + i]};
+            const double cj[3] = {(double)a.c[j], (double)a.c[a.n + j], (double)a.c[2 * a.n + j]};
+            double li[3], lj[3], si[4], sj[4];
+            disp_pgrad<double>(r, (double)a.ms[sidx], ci, cj, (double)a.kappa, a.pmax, TT, TT ? (double)a.a[i] : 0.0,
+                               TT ? (double)a.a[j] : 0.0, TT ? (double)a.b[i] : 0.0, TT ? (double)a.b[j] : 0.0,
+                               TT ? (double)a.q[i] : 0.0, TT ? (double)a.q[j] : 0.0, li, lj, si, sj);
+            for (int k = 0; k < 3; ++k) { pi_[k] = li[k]; pj_[k] = lj[k]; }
+            for (int k = 0; k < 4; ++k) { pi_[3 + k] = si[k]; pj_[3 + k] = sj[k]; }
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            if (!TT && k >= 3) break;
+            const double sum = seg_sum(pi_[k], run);
+            double* base = k < 3 ? a.dlr + (size_t)k * a.n : a.dsr + (size_t)(k - 3) * a.n;
+            if (head && key >= 0) atomicAdd(base + key, sum);
+            if (valid) atomicAdd(base + j, pj_[k]);
+        }
+    }
     block_reduce_add<20>(red, a.scal);
 }
 
+}  // namespace dmffb
+
+namespace dmffb {
+// Ewald self term of the dispersion parameter adjoints (disp_pme.py:264-289):
+// dE/dc6_i -= kappa^6 / 6 c6_i, dE/dc8_i -= kappa^8 / 24 c8_i, dE/dc10_i -= kappa^10 / 120 c10_i
+template <typename T>
+__global__ void k_disp_self_dc(int n, int pmax, double kappa, const T* c, double* dc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double k2 = kappa * kappa, k6 = k2 * k2 * k2;
+    dc[i] -= k6 / 6.0 * (double)c[i];
+    if (pmax >= 8) dc[n + i] -= k6 * k2 / 24.0 * (double)c[n + i];
+    if (pmax >= 10) dc[2 * n + i] -= k6 * k2 * k2 / 120.0 * (double)c[2 * n + i];
+}
 }  // namespace dmffb

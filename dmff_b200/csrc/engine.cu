@@ -141,6 +141,10 @@ struct dmffb_engine {
     double* d_tprm[3] = {nullptr, nullptr, nullptr};
     double* d_tdprm[3] = {nullptr, nullptr, nullptr};
     bool want_pgrad = false, charges_set = false;
+    // ---- ADMP parameter adjoints (dmffb_admp_set_param_grads)
+    bool admp_pgrad = false, have_pgrad = false;
+    double *d_dQloc = nullptr, *d_dpa = nullptr, *d_dth = nullptr, *d_dpol = nullptr;
+    double* d_dsr = nullptr;  // [4n] dE_sr/d(a, b, q, c6) (dispersion engines)
     // ---- capacities (dmffb_admp_reconfigure reuses the allocations for systems that fit)
     int n_cap = 0;
     int64_t cov_cap = 0, grid_cap = 0, cgrid_cap = 0;
@@ -788,6 +792,47 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     LAUNCH(h, s, KC_SELF, k_self_frames<T><<<nblk(n, 32), 32, 0, s>>>(sa));
     if (forces) LAUNCH(h, s, KC_VEC, k_finalize_forces<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_gpair, h->d_grad, forces));
     CK(cudaGetLastError());
+    h->have_pgrad = false;
+    if (h->admp_pgrad) {  // parameter adjoints at the converged dipoles (E is stationary in U)
+        CK(cudaMemsetAsync(h->d_dpa, 0, (size_t)n * sizeof(double), s));
+        CK(cudaMemsetAsync(h->d_dth, 0, (size_t)n * sizeof(double), s));
+        if (npairs > 0) {
+            PgradArgs<T> g;
+            g.p = pair_args<T>(h, bx, pairs, npairs, h->lpol ? U : nullptr);
+            g.dQ = h->d_gQ;
+            g.dpa = h->d_dpa;
+            g.dth = h->d_dth;
+            const unsigned nbk = nblk(npairs, 128);
+            if (sizeof(T) == 4) {
+                if (h->lpol) {
+                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
+                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_SCALED><<<nbk, 128, 0, s>>>(g));
+                } else {
+                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
+                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_SCALED><<<nbk, 128, 0, s>>>(g));
+                }
+            } else {
+                if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true><<<nbk, 128, 0, s>>>(g));
+                else LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false><<<nbk, 128, 0, s>>>(g));
+            }
+        }
+        LocalGradArgs la;
+        la.f = pa.f;
+        la.Qg = h->d_Qg;
+        la.U = h->lpol ? U : nullptr;
+        la.pol = h->lpol ? h->d_pol : nullptr;
+        la.dpa = h->lpol ? h->d_dpa : nullptr;
+        la.kappa = h->kappa;
+        la.lmax = h->lmax;
+        la.lmax_eff = lmax_eff(h);
+        la.lpme = h->lpme;
+        la.dQ = h->d_gQ;
+        la.dQloc = h->d_dQloc;
+        la.dpol = h->lpol ? h->d_dpol : nullptr;
+        LAUNCH(h, s, KC_SELF, k_local_grad<<<nblk(n, 128), 128, 0, s>>>(la));
+        CK(cudaGetLastError());
+        h->have_pgrad = true;
+    }
     if (h->timing) CK(cudaEventRecord(h->ev[5], s));
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
@@ -966,6 +1011,10 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
     a.grad_lr = (T*)h->d_glr;
     a.grad_sr = (T*)h->d_gsr;
     a.scal = h->d_scal;  // [0] E_lr real [1] E_sr [2..10] box lr [11..19] box sr
+    const bool pg = h->want_pgrad;
+    a.dlr = pg ? h->d_dc : nullptr;
+    a.dsr = (pg && h->tt) ? h->d_dsr : nullptr;
+    if (pg && h->tt) CK(cudaMemsetAsync(h->d_dsr, 0, (size_t)4 * n * sizeof(double), s));
     if (npairs > 0) {
         const unsigned nbk = nblk(npairs, 128);
         if (sizeof(T) == 4) {
@@ -991,6 +1040,10 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
                 return st;
         }
     }
+    if (pg && h->lpme)
+        LAUNCH(h, s, KC_SELF, k_disp_self_dc<T><<<nblk(n, 256), 256, 0, s>>>(n, h->pmax, h->kappa, (const T*)h->d_c,
+                                                                         h->d_dc));
+    h->have_pgrad = pg;
     LAUNCH(h, s, KC_VEC, k_disp_finalize<T><<<nblk(3 * n, 256), 256, 0, s>>>(
                              n, (const T*)h->d_glr, h->tt ? (const T*)h->d_gsr : nullptr, h->d_grad, f_lr, f_sr));
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1379,7 +1432,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_c, h->d_tta, h->d_ttb, h->d_ttq, h->d_glr, h->d_gsr, h->d_dc,
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
-                    h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2],
+                    h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr,
                     h->d_cub};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1520,10 +1573,41 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
     return run(double(0));
 }
 
+int dmffb_admp_set_param_grads(dmffb_engine* h, int32_t enabled) {
+    if (!h || h->kind != 0) return fail(h, DMFFB_BAD_ARG, "ADMP engine required");
+    if (enabled && !h->d_dQloc) {
+        const int nc = h->n_cap;
+        int st;
+        if ((st = dalloc(h, &h->d_dQloc, 9 * (size_t)nc * sizeof(double))) ||
+            (st = dalloc(h, &h->d_dpa, (size_t)nc * sizeof(double))) ||
+            (st = dalloc(h, &h->d_dth, (size_t)nc * sizeof(double))) ||
+            (st = dalloc(h, &h->d_dpol, (size_t)nc * sizeof(double))))
+            return st;
+    }
+    h->admp_pgrad = enabled != 0;
+    return DMFFB_OK;
+}
+
 int dmffb_admp_multipole_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal) {
-    (void)dE_dQlocal;
-    if (!h || !dE_dQglobal) return fail(h, DMFFB_BAD_ARG, "null argument");
-    CK(cudaMemcpyAsync(dE_dQglobal, h->d_gQ, 9 * h->n * sizeof(double), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    return dmffb_admp_param_grads(h, stream, dE_dQglobal, dE_dQlocal, nullptr, nullptr);
+}
+
+int dmffb_admp_param_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal, double* dE_dpol,
+                           double* dE_dthole) {
+    if (!h || h->kind != 0) return fail(h, DMFFB_BAD_ARG, "ADMP engine required");
+    if (!h->have_pgrad) return fail(h, DMFFB_BAD_ARG, "enable dmffb_admp_set_param_grads before compute");
+    cudaStream_t cs = (cudaStream_t)stream;
+    const size_t n = h->n;
+    if (dE_dQglobal) CK(cudaMemcpyAsync(dE_dQglobal, h->d_gQ, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    if (dE_dQlocal) CK(cudaMemcpyAsync(dE_dQlocal, h->d_dQloc, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    if (dE_dpol) {
+        if (h->lpol) CK(cudaMemcpyAsync(dE_dpol, h->d_dpol, n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+        else CK(cudaMemsetAsync(dE_dpol, 0, n * sizeof(double), cs));
+    }
+    if (dE_dthole) {
+        if (h->lpol) CK(cudaMemcpyAsync(dE_dthole, h->d_dth, n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+        else CK(cudaMemsetAsync(dE_dthole, 0, n * sizeof(double), cs));
+    }
     return DMFFB_OK;
 }
 
@@ -1836,9 +1920,25 @@ int dmffb_disp_compute(dmffb_engine* h, void* stream, const double* pos, const d
     return st;
 }
 
-int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc) {
-    if (!h || h->kind != 1 || !dE_dc) return fail(h, DMFFB_BAD_ARG, "bad arguments");
-    CK(cudaMemcpyAsync(dE_dc, h->d_dc, 3 * h->n * sizeof(double), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+int dmffb_disp_set_param_grads(dmffb_engine* h, int32_t enabled) {
+    if (!h || h->kind != 1) return fail(h, DMFFB_BAD_ARG, "dispersion engine required");
+    if (enabled && h->tt && !h->d_dsr) {
+        int st = dalloc(h, &h->d_dsr, 4 * (size_t)h->n_cap * sizeof(double));
+        if (st) return st;
+    }
+    h->want_pgrad = enabled != 0;
+    return DMFFB_OK;
+}
+
+int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc, double* dEsr_dabqc) {
+    if (!h || h->kind != 1) return fail(h, DMFFB_BAD_ARG, "dispersion engine required");
+    if (!h->have_pgrad) return fail(h, DMFFB_BAD_ARG, "enable dmffb_disp_set_param_grads before compute");
+    cudaStream_t cs = (cudaStream_t)stream;
+    if (dE_dc) CK(cudaMemcpyAsync(dE_dc, h->d_dc, 3 * (size_t)h->n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+    if (dEsr_dabqc) {
+        if (h->tt) CK(cudaMemcpyAsync(dEsr_dabqc, h->d_dsr, 4 * (size_t)h->n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
+        else CK(cudaMemsetAsync(dEsr_dabqc, 0, 4 * (size_t)h->n * sizeof(double), cs));
+    }
     return DMFFB_OK;
 }
 

@@ -185,11 +185,24 @@ class AdmpEngine:
             0 if pairs is None else pairs.shape[0], _dev(U), _dev(out)))
         return out
 
-    def multipole_grads(self):
-        out = torch.empty((self.n, 9), dtype=torch.float64, device=self.device)
-        s = torch.cuda.current_stream(self.device)
-        self._check(self.lib.dmffb_admp_multipole_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out), None))
+    def set_param_grads(self, on=True):
+        """Parameter adjoints (dE/dQ, dE/dpol, dE/dthole) on/off for the following computes."""
+        self._check(self.lib.dmffb_admp_set_param_grads(self.h, int(bool(on))))
+
+    def param_grads(self):
+        """{'Q_global', 'Q_local': [n, 9], 'pol', 'thole': [n]} of the last compute."""
+        dev = self.device
+        out = {"Q_global": torch.empty((self.n, 9), dtype=torch.float64, device=dev),
+               "Q_local": torch.empty((self.n, 9), dtype=torch.float64, device=dev),
+               "pol": torch.empty(self.n, dtype=torch.float64, device=dev),
+               "thole": torch.empty(self.n, dtype=torch.float64, device=dev)}
+        s = torch.cuda.current_stream(dev)
+        self._check(self.lib.dmffb_admp_param_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out["Q_global"]),
+                                                    _dev(out["Q_local"]), _dev(out["pol"]), _dev(out["thole"])))
         return out
+
+    def multipole_grads(self):
+        return self.param_grads()["Q_global"]
 
     def build_neighbors(self, pos, box, rc, capacity=None):
         """All i<j within rc (FP64 minimum-image test) as a cuda int32 [np,3] tensor sorted by i."""
@@ -308,11 +321,17 @@ class DispEngine:
             0 if pairs is None else pairs.shape[0], _dev(self.f_lr), _dev(self.f_sr), ctypes.byref(res)))
         return res, (self.f_lr, self.f_sr)
 
+    def set_param_grads(self, on=True):
+        self._check(self.lib.dmffb_disp_set_param_grads(self.h, int(bool(on))))
+
     def param_grads(self):
-        out = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        """{'c': dE_lr/dc [n, 3], 'a', 'b', 'q', 'c6': dE_sr/d. [n]} of the last compute."""
+        dc = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        dsr = torch.empty(4 * self.n, dtype=torch.float64, device=self.device)
         s = torch.cuda.current_stream(self.device)
-        self._check(self.lib.dmffb_disp_param_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out)))
-        return out.reshape(3, self.n).T
+        self._check(self.lib.dmffb_disp_param_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(dc), _dev(dsr)))
+        dsr = dsr.reshape(4, self.n)
+        return {"c": dc.reshape(3, self.n).T, "a": dsr[0], "b": dsr[1], "q": dsr[2], "c6": dsr[3]}
 
 
 _COUL = {"none": L.DMFFB_COUL_NONE, "pme": L.DMFFB_COUL_PME, "rf": L.DMFFB_COUL_RF,

@@ -120,8 +120,18 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
 int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const double* box,
                      const int32_t* pairs, int64_t npairs, const double* U, double* field_out);
 
-/* Per-atom dE/dQ_global (harmonic, [n*9]) and dE/dQ_local ([n*9]) at the last compute(),
- * for parameter gradients; device arrays. */
+/* Parameter adjoints on/off for the following computes.  When on, compute() also evaluates,
+ * at the converged induced dipoles (where E is stationary in U, so no adjoint solve is needed),
+ * the derivatives of the energy with respect to every atom's multipoles, polarizability and
+ * Thole width: the quantities jax.grad gives for params["ADMPPmeForce"] in the reference
+ * (dmff/admp/pme.py:186-232 under jax.value_and_grad), before the per-type scatter. */
+int dmffb_admp_set_param_grads(dmffb_engine* h, int32_t enabled);
+/* Per-atom parameter adjoints of the last compute (device arrays, each may be NULL):
+ * dE/dQ_global [n*9] and dE/dQ_local [n*9] (harmonic), dE/dpol [n] (A^-3 kJ/mol),
+ * dE/dthole [n]. */
+int dmffb_admp_param_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal,
+                           double* dE_dpol, double* dE_dthole);
+/* dE/dQ_global and dE/dQ_local only (same requirements as dmffb_admp_param_grads). */
 int dmffb_admp_multipole_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal);
 
 /* Cell-list neighbour build: NeighborList.allocate (dmff/common/nblist.py:27-55) semantics —
@@ -183,8 +193,13 @@ int dmffb_disp_set_params(dmffb_engine* h, const double* c_list, const double* a
  * pairs as in dmffb_admp_compute (NULL: the engine's own neighbour list). */
 int dmffb_disp_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
                        int64_t npairs, double* forces_lr, double* forces_sr, dmffb_disp_result* result);
-/* reciprocal-space dE_lr/dc (device [3n], channel-major) of the last compute, for parameter gradients */
-int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc);
+/* Parameter adjoints on/off for the following computes (the C6/C8/C10 and TT A/B/Q entries of
+ * jax.grad over params in the reference, dmff/admp/disp_pme.py:45-77, pairwise.py:47-118). */
+int dmffb_disp_set_param_grads(dmffb_engine* h, int32_t enabled);
+/* Adjoints of the last compute (device arrays, each may be NULL): dE_lr/dc [3n] channel-major
+ * (c = sqrt(C_n 10^n) per atom: real space + reciprocal + self), dE_sr/d(a, b, q, c6) [4n]
+ * channel-major (TT short range; zero without TT). */
+int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc, double* dEsr_dabqc);
 
 /* ---------------------------------------------------------------------------------------
  * Classical terms: Lennard-Jones + point-charge Coulomb (PME real+reciprocal+self, reaction
