@@ -41,7 +41,18 @@ struct PairArgs {
     T* field;    // [n*3]  dE/dU (FIELD, MATVEC)
     double* scal;  // [0] energy, [1..9] box gradient
     int want_box;
+    const int32_t* rowmap = nullptr;  // ROWS_SCALED launches: indices of the rows with nbond != 0
+    int64_t nrowmap = 0;
 };
+
+// row handled by this thread: the thread index, or for a scaled-rows launch with a row map the
+// thread's entry of the map (threads past its end get an out-of-range row)
+template <int ROWS, typename A>
+__device__ __forceinline__ int64_t launch_row(const A& a) {
+    int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ROWS == 2 && a.rowmap) row = row < a.nrowmap ? (int64_t)a.rowmap[row] : a.npairs;
+    return row;
+}
 
 // l=2 harmonic rotation into frame (ex, ey, ez): local[j] = sum_k C[j][k] global[k]  (multipole.py:155-203)
 template <typename T>
@@ -543,7 +554,7 @@ enum { ROWS_ALL = 0, ROWS_UNSCALED = 1, ROWS_SCALED = 2 };
 // that no warp mixes the two arithmetic paths.
 template <typename T, bool POL, int MODE, int ROWS = ROWS_ALL>
 __global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
-    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t row = launch_row<ROWS>(a);
     int i = -1, j = -1, nb = 0;
     if (row < a.npairs) {
         i = a.pairs[3 * row];
@@ -667,7 +678,7 @@ __device__ __forceinline__ void pgrad_row(const PairArgs<T>& a, int i, int j, in
 template <typename T, bool POL, int ROWS = ROWS_ALL>
 __global__ void __launch_bounds__(128) k_admp_pgrad(PgradArgs<T> g) {
     const PairArgs<T>& a = g.p;
-    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t row = launch_row<ROWS>(a);
     int i = -1, j = -1, nb = 0;
     if (row < a.npairs) {
         i = a.pairs[3 * row];

@@ -27,6 +27,7 @@
 // Each term optionally writes its parameter derivatives (dE/dk, dE/dr0 | dtheta0 | dpsi).
 #pragma once
 #include "common.cuh"
+#include "admp_real.cuh"
 
 namespace dmffb {
 
@@ -54,6 +55,8 @@ struct NbPairArgs {
     double* dsig;          // [ntypes^2] dE/dsigma_ij or null
     double* deps;          // [ntypes^2] dE/deps_ij or null
     double* scal;          // [0] E_coul real space, [1] E_lj, [2..10] box gradient
+    const int32_t* rowmap = nullptr;  // ROWS == 2 launches: indices of the rows with nbond != 0
+    int64_t nrowmap = 0;
 };
 
 // energies and d/dr of one pair; phi = dE_coul / d(q_i q_j)
@@ -99,7 +102,7 @@ __device__ __forceinline__ void nb_eval(TC r, TC qq, TC mc, TC ml, TC sig, TC ep
 
 template <typename T, int ROWS>
 __global__ void __launch_bounds__(128) k_nb_pair(NbPairArgs<T> a) {
-    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t row = launch_row<ROWS>(a);
     int i = -1, j = -1, nb = 0;
     if (row < a.npairs) {
         i = a.pairs[3 * row];

@@ -11,6 +11,7 @@
 // topological scale run in FP64 (m - 1 + g cancels for excluded pairs).
 #pragma once
 #include "common.cuh"
+#include "admp_real.cuh"
 
 namespace dmffb {
 
@@ -33,6 +34,8 @@ struct DispArgs {
     double* scal;        // [0] E_lr real, [1] E_sr, [2..10] box grad lr, [11..19] box grad sr
     double* dlr;         // [3][n] += dE_lr/dc (channel-major), parameter adjoints, or null
     double* dsr;         // [4][n] += dE_sr/d(a, b, q, c6), or null
+    const int32_t* rowmap = nullptr;  // ROWS == 2 launches: indices of the rows with nbond != 0
+    int64_t nrowmap = 0;
 };
 
 // Parameter partials of one pair: dE_lr/dc_i^p and dE_lr/dc_j^p (p = 6, 8, 10; the real-space
@@ -130,7 +133,7 @@ __device__ __forceinline__ void disp_eval(TC r, TC m, const TC ci[3], const TC c
 
 template <typename T, int ROWS, bool TT>
 __global__ void __launch_bounds__(128) k_disp_pair(DispArgs<T> a) {
-    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t row = launch_row<ROWS>(a);
     int i = -1, j = -1, nb = 0;
     if (row < a.npairs) {
         i = a.pairs[3 * row];

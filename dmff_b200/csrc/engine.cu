@@ -145,6 +145,15 @@ struct dmffb_engine {
     bool admp_pgrad = false, have_pgrad = false;
     double *d_dQloc = nullptr, *d_dpa = nullptr, *d_dth = nullptr, *d_dpol = nullptr;
     double* d_dsr = nullptr;  // [4n] dE_sr/d(a, b, q, c6) (dispersion engines)
+    // ---- rows with nbond != 0 (the FP64 scaled-rows launches visit only these)
+    int32_t* d_srows = nullptr;
+    int64_t srows_cap = 0, n_srows = 0;
+    int* d_nsel = nullptr;
+    int* h_nsel = nullptr;  // pinned
+    void* d_cubsel = nullptr;
+    size_t cubsel_bytes = 0;
+    const int32_t* srows_pairs = nullptr;  // the pair list the row map belongs to
+    int64_t srows_npairs = -1, srows_gen = -1, pairs_gen = 0;
     // ---- capacities (dmffb_admp_reconfigure reuses the allocations for systems that fit)
     int n_cap = 0;
     int64_t cov_cap = 0, grid_cap = 0, cgrid_cap = 0;
@@ -385,6 +394,54 @@ __global__ void k_set_thole(int n, const double* pol, const double* thole, T* th
 }
 
 // ------------------------------------------------------------------ engine pieces
+// predicate of the scaled-rows selection: a valid row (i < j) with a topological scale
+struct ScaledRow {
+    const int32_t* p;
+    __device__ __forceinline__ bool operator()(const int32_t r) const {
+        return p[3 * (int64_t)r + 2] != 0 && p[3 * (int64_t)r] < p[3 * (int64_t)r + 1];
+    }
+};
+
+// Indices of the rows with nbond != 0 (stable, so still sorted by i), rebuilt when the pair
+// list changes: the FP64 scaled-rows launches run over these (about one row in a hundred)
+// instead of over every row.
+int scaled_rows(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npairs) {
+    const bool internal = pairs == h->d_pairs;
+    if (internal && h->srows_pairs == pairs && h->srows_npairs == npairs && h->srows_gen == h->pairs_gen)
+        return DMFFB_OK;
+    int st;
+    if (npairs > 0x7fffffff) return fail(h, DMFFB_BAD_ARG, "too many pair rows");
+    if (!h->d_nsel) {
+        if ((st = dalloc(h, &h->d_nsel, sizeof(int)))) return st;
+        if (cudaMallocHost((void**)&h->h_nsel, sizeof(int)) != cudaSuccess) return fail(h, DMFFB_OOM, "cudaMallocHost");
+    }
+    const int64_t cap_need = std::max<int64_t>(npairs, 1);
+    if (cap_need > h->srows_cap) {  // capacity for every row: selection output cannot overflow
+        if (h->d_srows) cudaFree(h->d_srows);
+        h->d_srows = nullptr;
+        h->srows_cap = cap_need + cap_need / 4;
+        if ((st = dalloc(h, &h->d_srows, h->srows_cap * sizeof(int32_t)))) return st;
+    }
+    size_t need = 0;
+    cub::CountingInputIterator<int32_t> it(0);
+    cub::DeviceSelect::If(nullptr, need, it, h->d_srows, h->d_nsel, (int)npairs, ScaledRow{pairs}, s);
+    if (need > h->cubsel_bytes) {
+        if (h->d_cubsel) cudaFree(h->d_cubsel);
+        h->d_cubsel = nullptr;
+        h->cubsel_bytes = need;
+        if ((st = dalloc(h, &h->d_cubsel, need))) return st;
+    }
+    size_t tb = h->cubsel_bytes;
+    CK(cub::DeviceSelect::If(h->d_cubsel, tb, it, h->d_srows, h->d_nsel, (int)npairs, ScaledRow{pairs}, s));
+    CK(cudaMemcpyAsync(h->h_nsel, h->d_nsel, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    h->n_srows = *h->h_nsel;
+    h->srows_pairs = pairs;
+    h->srows_npairs = npairs;
+    h->srows_gen = internal ? h->pairs_gen : -1;
+    return DMFFB_OK;
+}
+
 template <typename T>
 PairArgs<T> pair_args(dmffb_engine* h, const Box& bx, const int32_t* pairs, int64_t npairs, const double* U) {
     PairArgs<T> a;
@@ -553,7 +610,10 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
         if (sizeof(T) == 4) {
             LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_UNSCALED><<<nblk(npairs, 128), 128, 0, s>>>(a));
-            LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(npairs, 128), 128, 0, s>>>(a));
+            a.rowmap = h->d_srows;
+            a.nrowmap = h->n_srows;
+            if (h->n_srows > 0)
+                LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(h->n_srows, 128), 128, 0, s>>>(a));
         } else {
             LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, s>>>(a));
         }
@@ -727,6 +787,8 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
         npairs = h->npairs;
     }
     res->n_pairs = npairs;
+    if (sizeof(T) == 4 && npairs > 0)
+        if ((st = scaled_rows(h, s, pairs, npairs))) return st;
     if (h->timing) CK(cudaEventRecord(h->ev[0], s));
     CK(cudaMemsetAsync(h->d_scal, 0, N_SCAL * sizeof(double), s));
     CK(cudaMemsetAsync(h->d_gpair, 0, (size_t)3 * n * sizeof(T), s));
@@ -757,12 +819,17 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, h->lpol ? U : nullptr);
         const unsigned nbk = nblk(npairs, 128);
         if (sizeof(T) == 4) {
+            const unsigned nbs = nblk(h->n_srows, 128);
             if (h->lpol) {
                 LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(a));
-                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbk, 128, 0, s>>>(a));
+                a.rowmap = h->d_srows;
+                a.nrowmap = h->n_srows;
+                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, s>>>(a));
             } else {
                 LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(a));
-                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbk, 128, 0, s>>>(a));
+                a.rowmap = h->d_srows;
+                a.nrowmap = h->n_srows;
+                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, s>>>(a));
             }
         } else {
             if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nbk, 128, 0, s>>>(a));
@@ -804,12 +871,17 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
             g.dth = h->d_dth;
             const unsigned nbk = nblk(npairs, 128);
             if (sizeof(T) == 4) {
+                const unsigned nbs = nblk(h->n_srows, 128);
                 if (h->lpol) {
                     LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
-                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_SCALED><<<nbk, 128, 0, s>>>(g));
+                    g.p.rowmap = h->d_srows;
+                    g.p.nrowmap = h->n_srows;
+                    if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_SCALED><<<nbs, 128, 0, s>>>(g));
                 } else {
                     LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
-                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_SCALED><<<nbk, 128, 0, s>>>(g));
+                    g.p.rowmap = h->d_srows;
+                    g.p.nrowmap = h->n_srows;
+                    if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_SCALED><<<nbs, 128, 0, s>>>(g));
                 }
             } else {
                 if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true><<<nbk, 128, 0, s>>>(g));
@@ -1018,12 +1090,18 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
     if (npairs > 0) {
         const unsigned nbk = nblk(npairs, 128);
         if (sizeof(T) == 4) {
+            if ((st = scaled_rows(h, s, pairs, npairs))) return st;
+            const unsigned nbs = nblk(h->n_srows, 128);
             if (h->tt) {
                 LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 1, true><<<nbk, 128, 0, s>>>(a));
-                LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, true><<<nbk, 128, 0, s>>>(a));
+                a.rowmap = h->d_srows;
+                a.nrowmap = h->n_srows;
+                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, true><<<nbs, 128, 0, s>>>(a));
             } else {
                 LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 1, false><<<nbk, 128, 0, s>>>(a));
-                LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, false><<<nbk, 128, 0, s>>>(a));
+                a.rowmap = h->d_srows;
+                a.nrowmap = h->n_srows;
+                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, false><<<nbs, 128, 0, s>>>(a));
             }
         } else {
             if (h->tt) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 0, true><<<nbk, 128, 0, s>>>(a));
@@ -1128,8 +1206,11 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
         a.scal = h->d_scal;
         const unsigned nbk = nblk(npairs, 128);
         if (sizeof(T) == 4) {
+            if ((st = scaled_rows(h, s, pairs, npairs))) return st;
             LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 1><<<nbk, 128, 0, s>>>(a));
-            LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 2><<<nbk, 128, 0, s>>>(a));
+            a.rowmap = h->d_srows;
+            a.nrowmap = h->n_srows;
+            if (h->n_srows > 0) LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 2><<<nblk(h->n_srows, 128), 128, 0, s>>>(a));
         } else {
             LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 0><<<nbk, 128, 0, s>>>(a));
         }
@@ -1432,11 +1513,12 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_c, h->d_tta, h->d_ttb, h->d_ttq, h->d_glr, h->d_gsr, h->d_dc,
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
-                    h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr,
+                    h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
                     h->d_cub};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->h_nsel) cudaFreeHost(h->h_nsel);
     for (auto& kv : h->plan_cache) {
         cufftDestroy(kv.second.first);
         cufftDestroy(kv.second.second);
@@ -1513,6 +1595,7 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
         }
         h->have_pairs = false;
         h->csr_from_build = false;
+        h->pairs_gen++;
         dp = h->d_pairs;
         CK(cudaMemcpyAsync(dp, pairs, npairs * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     }
@@ -1564,7 +1647,9 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
         pa.QgT = (T*)h->d_QgT;
         pa.Qg = h->d_Qg;
         LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
-        int st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out);
+        int st;
+        if (sizeof(T) == 4 && npairs > 0 && (st = scaled_rows(h, s, pairs, npairs))) return st;
+        st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out);
         if (st) return st;
         CK(cudaStreamSynchronize(s));
         return DMFFB_OK;
@@ -1735,6 +1820,7 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
         if (st) return st;
         h->npairs = need;
         h->have_pairs = true;
+        h->pairs_gen++;
         h->csr_from_build = false;
         return DMFFB_OK;
     }
@@ -1833,6 +1919,7 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     prof_collect(h);
     h->npairs = tot[0];
     h->have_pairs = true;
+    h->pairs_gen++;
     h->csr_from_build = true;
     return DMFFB_OK;
 }
