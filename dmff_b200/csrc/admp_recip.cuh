@@ -536,6 +536,20 @@ __device__ __forceinline__ void stencil01(const MeshGeom& g, const double* pos, 
     }
 }
 
+// v[k] for a runtime k in 0..5 without indexing a register array (a select chain keeps the
+// stencil in registers instead of the stack)
+template <typename T>
+__device__ __forceinline__ T sel6(const T v[6], int k) {
+    T r = v[0];
+#pragma unroll
+    for (int t = 1; t < 6; ++t) r = (k == t) ? v[t] : r;
+    return r;
+}
+
+// Lane layout of the lean dipole spread / field gather: a warp per atom, lanes 0..29 form five
+// groups of six consecutive z points of one (x, y) stencil column; the 36 columns take eight
+// passes.  A warp's atomics / loads of one pass then touch five runs of six consecutive floats
+// (coalesced in L2) instead of 32 scattered addresses.
 template <typename T>
 __global__ void __launch_bounds__(256) k_spread_dip(SpreadArgs<T> a) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -551,22 +565,26 @@ __global__ void __launch_bounds__(256) k_spread_dip(SpreadArgs<T> a) {
     const T c2 = -(T(B[3]) * mu0 + T(B[4]) * mu1 + T(B[5]) * mu2);
     const T c3 = -(T(B[6]) * mu0 + T(B[7]) * mu1 + T(B[8]) * mu2);
     const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
-    for (int L = lane; L < 36; L += 32) {
-        const int ix = L / 6, iy = L % 6;
-        const T s0 = c1 * Mx[1][ix] * My[0][iy] + c2 * Mx[0][ix] * My[1][iy];
-        const T s1 = c3 * Mx[0][ix] * My[0][iy];
-        const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
-        T* line = a.grid + ((size_t)gx * K1 + gy) * K2;
-        int gz = wrapi(m0[2] - 3, K2);
+    const int grp = lane / 6, iz = lane - 6 * grp;
+    if (grp >= 5) return;
+    const T mz0 = sel6(Mz[0], iz), mz1 = sel6(Mz[1], iz);
+    const int gz = wrapi(m0[2] - 3 + iz, K2);
 #pragma unroll
-        for (int t = 0; t < 6; ++t) {
-            atomicAdd(line + gz, s0 * Mz[0][t] + s1 * Mz[1][t]);
-            gz = (gz + 1 == K2) ? 0 : gz + 1;
+    for (int pass = 0; pass < 8; ++pass) {
+        const int col = grp + 5 * pass;
+        if (col < 36) {
+            const int ix = col / 6, iy = col - 6 * ix;
+            const T mx0 = sel6(Mx[0], ix), mx1 = sel6(Mx[1], ix), my0 = sel6(My[0], iy), my1 = sel6(My[1], iy);
+            const T v = (c1 * mx1 * my0 + c2 * mx0 * my1) * mz0 + c3 * mx0 * my0 * mz1;
+            const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
+            atomicAdd(a.grid + ((size_t)gx * K1 + gy) * K2 + gz, v);
         }
     }
 }
 
-// dE/dmu (Cartesian) of every site from the convolved mesh: out = scale * (-B^T grad_u phi)
+// dE/dmu (Cartesian) of every site from the convolved mesh: out = scale * (-B^T grad_u phi).
+// Lanes take whole (x, y) stencil columns and read their six z points in sequence (one cache
+// line, L1 hits after the first); sel6 keeps the column weights in registers.
 template <typename T>
 __global__ void __launch_bounds__(256) k_gather_field(int n, const double* pos, MeshGeom g, const T* phi, double scale,
                                                       double* out) {
@@ -579,22 +597,27 @@ __global__ void __launch_bounds__(256) k_gather_field(int n, const double* pos, 
     stencil01<T>(g, pos, at, m0, Mx, My, Mz);
     const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
     T p1 = T(0), p2 = T(0), p3 = T(0);
-    for (int L = lane; L < 36; L += 32) {
-        const int ix = L / 6, iy = L % 6;
-        const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
-        const T* line = phi + ((size_t)gx * K1 + gy) * K2;
-        int gz = wrapi(m0[2] - 3, K2);
-        T s0 = T(0), s1 = T(0);
 #pragma unroll
-        for (int t = 0; t < 6; ++t) {
-            const T v = line[gz];
-            s0 += v * Mz[0][t];
-            s1 += v * Mz[1][t];
-            gz = (gz + 1 == K2) ? 0 : gz + 1;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int L = lane + 32 * pass;
+        if (L < 36) {
+            const int ix = L / 6, iy = L - 6 * ix;
+            const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
+            const T* line = phi + ((size_t)gx * K1 + gy) * K2;
+            int gz = wrapi(m0[2] - 3, K2);
+            T s0 = T(0), s1 = T(0);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+                const T v = __ldg(line + gz);
+                s0 += v * Mz[0][t];
+                s1 += v * Mz[1][t];
+                gz = (gz + 1 == K2) ? 0 : gz + 1;
+            }
+            const T mx0 = sel6(Mx[0], ix), mx1 = sel6(Mx[1], ix), my0 = sel6(My[0], iy), my1 = sel6(My[1], iy);
+            p1 += mx1 * my0 * s0;
+            p2 += mx0 * my1 * s0;
+            p3 += mx0 * my0 * s1;
         }
-        p1 += Mx[1][ix] * My[0][iy] * s0;
-        p2 += Mx[0][ix] * My[1][iy] * s0;
-        p3 += Mx[0][ix] * My[0][iy] * s1;
     }
     p1 = warp_sum(p1);
     p2 = warp_sum(p2);
