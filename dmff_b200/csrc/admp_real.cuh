@@ -821,11 +821,11 @@ __global__ void __launch_bounds__(256) k_matvec_csr(PairArgs<T> a, CsrArgs c, do
 // streams them (k_matvec_apply).
 template <typename T>
 struct MvCoef {
-    T c[4];  // udud1, udud0 - udud1, z_x, z_y
+    T c[2];  // udud1, udud0 - udud1 (the pair direction is recomputed from the positions)
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_matvec_coef(PairArgs<T> a, CsrArgs c, MvCoef<T>* coef, T* coefz) {
+__global__ void __launch_bounds__(256) k_matvec_coef(PairArgs<T> a, CsrArgs c, MvCoef<T>* coef) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= c.n) return;
@@ -871,31 +871,34 @@ __global__ void __launch_bounds__(256) k_matvec_coef(PairArgs<T> a, CsrArgs c, M
         MvCoef<T> cf;
         cf.c[0] = udud1;
         cf.c[1] = udud0 - udud1;
-        cf.c[2] = dx * rinv;
-        cf.c[3] = dy * rinv;
         coef[k] = cf;
-        coefz[k] = dz * rinv;
     }
 }
 
+// The CG matvec streams 12 bytes per CSR entry (packed j + two coefficients); the pair
+// direction z is recomputed from the positions, which like U stay cache-resident.
 template <typename T>
-__global__ void __launch_bounds__(256) k_matvec_apply(CsrArgs c, const MvCoef<T>* coef, const T* coefz,
+__global__ void __launch_bounds__(256) k_matvec_apply(CsrArgs c, const MvCoef<T>* coef, const T* pos4, BoxT<T> bx,
                                                       const double* U, double* out) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= c.n) return;
     const int i = w;
+    const T xi = pos4[4 * i], yi = pos4[4 * i + 1], zi = pos4[4 * i + 2];
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
     const int64_t beg = c.off[i], end = c.off[i + 1];
     for (int64_t k = beg + lane; k < end; k += 32) {
         const int j = c.ent[k] & 0x0FFFFFFF;
         const MvCoef<T> cf = coef[k];
-        const T ez = coefz[k];
+        T dx = xi - pos4[4 * j], dy = yi - pos4[4 * j + 1], dz = zi - pos4[4 * j + 2];
+        pbc_shift(bx, dx, dy, dz, (T*)nullptr);
+        const T rinv = d_rsqrt(dx * dx + dy * dy + dz * dz);
+        const T ex = dx * rinv, ey = dy * rinv, ez = dz * rinv;
         const double* Uj = U + 3 * j;
         const T u0 = (T)Uj[0], u1 = (T)Uj[1], u2 = (T)Uj[2];
-        const T dd = cf.c[1] * (cf.c[2] * u0 + cf.c[3] * u1 + ez * u2);
-        acc0 += (double)(cf.c[0] * u0 + dd * cf.c[2]);
-        acc1 += (double)(cf.c[0] * u1 + dd * cf.c[3]);
+        const T dd = cf.c[1] * (ex * u0 + ey * u1 + ez * u2);
+        acc0 += (double)(cf.c[0] * u0 + dd * ex);
+        acc1 += (double)(cf.c[0] * u1 + dd * ey);
         acc2 += (double)(cf.c[0] * u2 + dd * ez);
     }
     acc0 = warp_sum(acc0);

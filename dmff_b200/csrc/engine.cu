@@ -78,7 +78,6 @@ struct dmffb_engine {
     const int32_t* csr_pairs = nullptr;  // the half list the current CSR belongs to
     float* d_posf = nullptr;
     void* d_mvcoef = nullptr;  // [csr_cap] MvCoef<T>
-    void* d_mvz = nullptr;     // [csr_cap] T
     int64_t mv_cap = 0;
     int32_t* d_pcount_f = nullptr;
     void* d_cub2 = nullptr;
@@ -552,10 +551,9 @@ template <typename T>
 int matvec_setup(dmffb_engine* h, cudaStream_t s, const Box& bx, const int32_t* pairs, int64_t npairs) {
     int st;
     if (h->csr_cap > h->mv_cap) {
-        if (h->d_mvcoef) { cudaFree(h->d_mvcoef); cudaFree(h->d_mvz); }
+        if (h->d_mvcoef) cudaFree(h->d_mvcoef);
         h->mv_cap = h->csr_cap;
         if ((st = dalloc(h, &h->d_mvcoef, h->mv_cap * sizeof(MvCoef<T>)))) return st;
-        if ((st = dalloc(h, &h->d_mvz, h->mv_cap * sizeof(T)))) return st;
     }
     PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
     CsrArgs c;
@@ -563,7 +561,7 @@ int matvec_setup(dmffb_engine* h, cudaStream_t s, const Box& bx, const int32_t* 
     c.off = h->d_csr_off;
     c.ent = h->d_csr_ent;
     LAUNCH(h, s, KC_PAIR_MATVEC, k_matvec_coef<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
-                                     a, c, (MvCoef<T>*)h->d_mvcoef, (T*)h->d_mvz));
+                                     a, c, (MvCoef<T>*)h->d_mvcoef));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
@@ -633,7 +631,7 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
             sm = h->s2;
         }
         LAUNCH(h, sm, KC_PAIR_MATVEC, k_matvec_apply<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, sm>>>(
-                                          c, (const MvCoef<T>*)h->d_mvcoef, (const T*)h->d_mvz, U, h->d_fmv));
+                                          c, (const MvCoef<T>*)h->d_mvcoef, (const T*)h->d_posT, boxT<T>(bx), U, h->d_fmv));
         if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
     const double* recip = nullptr;
@@ -1508,7 +1506,7 @@ void dmffb_destroy(dmffb_engine* h) {
     void* ptrs[] = {h->d_axis_type, h->d_axis_idx, h->d_cov_ptr, h->d_cov_j, h->d_cov_nb, h->d_Qloc, h->d_pol,
                     h->d_thole, h->d_polsix, h->d_pos, h->d_U, h->d_forces, h->d_posT, h->d_Qg, h->d_QgT,
                     h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
-                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_mvz, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
+                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
                     h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
                     h->d_c, h->d_tta, h->d_ttb, h->d_ttq, h->d_glr, h->d_gsr, h->d_dc,
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
