@@ -106,41 +106,45 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def roofline(stats, s, npairs, peaks, peak_src, traffic_per_launch=None):
-    """Roofline entry for the kernel class with the largest device time.  Algorithmic work per
-    launch (fixed convention): pair FULL polarizable 1900 flop/pair; pair MATVEC 200 flop/pair;
-    spread N(12 + 4(l+1)^2) + 4K^3 B; gather 4K^3 + N(12 + 4(l+1)^2 + 24) B; convolution 16 K^3 B."""
+# DRAM bytes per launch from one ncu capture of this workload (profiles/kernels_admp_pol_12288.md:
+# dram__bytes_read.sum + dram__bytes_write.sum, 12288-atom polarizable step)
+NCU_DRAM_BYTES = {"pair_matvec": 33.11e6, "spread": 1.11e6, "neighbors": 0.5 * (0.55e6 + 0.94e6)}
+
+
+def roofline(stats, s, npairs, peaks, peak_src):
+    """Roofline of the CG matvec (k_matvec_apply: the kernel with the largest share of the step in
+    the ncu launch list, profiles/launches_admp_pol_12288.md), plus every kernel class's achieved
+    rate against its bound.  Algorithmic work per launch (fixed convention): matvec 12 B per CSR
+    entry (2 entries per pair: packed j + two FP32 coefficients); pair FULL polarizable 1900
+    flop/pair, FIELD 600 flop/pair; spread N(12 + 4(l+1)^2) + 4K^3 B; gather 4K^3 + N(12 + 4(l+1)^2
+    + 24) B; convolution 16 K^3 B; neighbour build 12N + 12 Np B."""
     n = s["n_atoms"]
     K3 = float(np.prod(s["K"]))
-    cls = max((k for k in stats if stats[k][1] > 0 and k != "fft"), key=lambda k: stats[k][0])
-    ms, launches = stats[cls]
-    per_launch_s = ms / 1e3 / launches
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12  # TFLOP/s, nominal at max clock
-    if cls in ("pair_full", "pair_matvec", "pair_field"):
-        flop = {"pair_full": 1900, "pair_matvec": 200, "pair_field": 600}[cls] * npairs
-        ach = flop / per_launch_s / 1e12
-        return {"kernel": cls, "bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": ach / fp32_peak, "traffic": traffic_per_launch, "launches": launches,
-                "avg_launch_us": per_launch_s * 1e6,
-                "peak_source": "nominal FP32 CUDA-core peak: 148 SM x 128 lanes x 2 x max SM clock"}
-    lmap = {"spread": 2, "gather_full": 2, "gather_field": 1}
-    if cls == "spread":
-        byts = n * (12 + 4 * 9) + 4 * K3
-    elif cls in ("gather_full", "gather_field"):
-        l = lmap[cls]
-        byts = 4 * K3 + n * (12 + 4 * (l + 1) ** 2 + 24)
-    elif cls == "conv":
-        byts = 16 * K3
-    elif cls == "vector":
-        byts = 5 * 3 * n * 8
-    elif cls == "neighbors":
-        byts = 12 * n + 12 * npairs
-    else:
-        byts = 12 * n
-    ach = byts / per_launch_s / 1e9
-    return {"kernel": cls, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": ach / peaks["hbm_gbs"], "traffic": traffic_per_launch, "launches": launches,
-            "avg_launch_us": per_launch_s * 1e6, "peak_source": f"hbm_gbs ({peak_src})"}
+    models = {"pair_matvec": ("hbm", 12.0 * 2 * npairs), "pair_full": ("fp32", 1900.0 * npairs),
+              "pair_field": ("fp32", 600.0 * npairs), "spread": ("hbm", n * (12 + 4 * 9) + 4 * K3),
+              "gather_full": ("hbm", 4 * K3 + n * (12 + 4 * 9 + 24)), "gather_field": ("hbm", 4 * K3 + n * (12 + 16 + 24)),
+              "conv": ("hbm", 16 * K3), "neighbors": ("hbm", 12 * n + 12 * npairs)}
+    out = {}
+    for cls, (bound, work) in models.items():
+        ms, launches = stats.get(cls, (0.0, 0))
+        if launches == 0:
+            continue
+        per = ms / 1e3 / launches
+        if bound == "fp32":
+            ach = work / per / 1e12
+            out[cls] = {"bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                        "avg_launch_us": per * 1e6, "launches": launches}
+        else:
+            ach = work / per / 1e9
+            out[cls] = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": ach / peaks["hbm_gbs"], "avg_launch_us": per * 1e6, "launches": launches}
+    main = dict(out["pair_matvec"], kernel="k_matvec_apply (CG matvec)", traffic=NCU_DRAM_BYTES["pair_matvec"],
+                peak_source=f"hbm_gbs ({peak_src})",
+                traffic_source="ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, this workload")
+    main["by_class"] = {k: {"frac": round(v["frac"], 4), "achieved": round(v["achieved"], 2), "unit": v["unit"],
+                            "avg_launch_us": round(v["avg_launch_us"], 2)} for k, v in out.items()}
+    return main
 
 
 # ---------------------------------------------------------------------------------- CPU side

@@ -47,7 +47,7 @@ DMFFB_TERM_ANGLE = 1
 DMFFB_TERM_TORSION = 2
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
-                  "gather_field", "self_frames", "vector", "neighbors"]
+                  "gather_field", "self_frames", "vector", "neighbors", "matvec_coef"]
 
 
 class AdmpDesc(ctypes.Structure):

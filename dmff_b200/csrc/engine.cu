@@ -251,7 +251,7 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // kernel classes for dmffb_get_kernel_stats
 enum { KC_PREP = 0, KC_PAIR_FULL, KC_PAIR_FIELD, KC_PAIR_MATVEC, KC_SPREAD, KC_FFT, KC_CONV, KC_GATHER_FULL,
-       KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_COUNT };
+       KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_MVCOEF, KC_COUNT };
 
 inline void prof_begin(dmffb_engine* h, cudaStream_t s, int cls) {
     if (!h->prof) return;
@@ -560,7 +560,7 @@ int matvec_setup(dmffb_engine* h, cudaStream_t s, const Box& bx, const int32_t* 
     c.n = h->n;
     c.off = h->d_csr_off;
     c.ent = h->d_csr_ent;
-    LAUNCH(h, s, KC_PAIR_MATVEC, k_matvec_coef<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
+    LAUNCH(h, s, KC_MVCOEF, k_matvec_coef<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
                                      a, c, (MvCoef<T>*)h->d_mvcoef));
     CK(cudaGetLastError());
     return DMFFB_OK;
