@@ -164,3 +164,86 @@ def stream_stats(reqs):
             "atom_evals_per_s": atoms / (t_last - t_first), "p50_ms": float(np.percentile(lat, 50) * 1e3),
             "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3), "failed": bad,
             "not_converged": sum(1 for r in reqs if r.status == L.DMFFB_NOT_CONVERGED)}
+
+
+# ----------------------------------------------------------------------------------- replicas
+def assign_requests(atoms, n_ranks):
+    """Rank of every request for an ``n_ranks``-replica deployment: in arrival order, each request
+    goes to the rank with the fewest atoms assigned so far (ties to the lower rank).  Deterministic,
+    so every rank computes the same assignment from the same stream without communicating."""
+    load = [0] * n_ranks
+    out = []
+    for a in atoms:
+        r = min(range(n_ranks), key=lambda k: (load[k], k))
+        out.append(r)
+        load[r] += int(a)
+    return out
+
+
+def serve_replicated(systems, arrivals, run_local, group=None, timeout_s=600.0):
+    """Serve one request stream on all ranks of a process group, one replica (server) per rank.
+
+    ``run_local(systems, arrivals) -> list of per-request dicts`` runs this rank's share (its own
+    GPU and server; no device data crosses ranks: the path has no exchange step).  Per-request
+    records (``index``, ``n_atoms``, ``latency`` or ``error``) are gathered on every rank over
+    ``group`` (a gloo group: objects, not device tensors).  Requests whose rank raised are
+    re-assigned over the ranks that did not and run in a second round.  Returns (records sorted by
+    request index, summary dict)."""
+    import torch.distributed as dist
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    owner = assign_requests([s["n_atoms"] for s in systems], world)
+    mine = [k for k in range(len(systems)) if owner[k] == rank]
+
+    def run(indices):
+        try:
+            recs = run_local([systems[k] for k in indices], [arrivals[k] for k in indices])
+            for k, r in zip(indices, recs):
+                r["index"] = k
+            return {"rank": rank, "ok": True, "records": recs}
+        except Exception as e:  # a failed replica reports instead of leaving the group
+            return {"rank": rank, "ok": False, "error": f"{type(e).__name__}: {e}", "indices": list(indices)}
+
+    def gather(obj):
+        got = [None] * world
+        dist.all_gather_object(got, obj, group=group)
+        return got
+
+    first = gather(run(mine))
+    records = [r for g in first if g["ok"] for r in g["records"]]
+    failed_ranks = [g["rank"] for g in first if not g["ok"]]
+    retry = sorted(k for g in first if not g["ok"] for k in g["indices"])
+    alive = [r for r in range(world) if r not in failed_ranks]
+    redistributed = 0
+    if retry and alive:
+        sub = assign_requests([systems[k]["n_atoms"] for k in retry], len(alive))
+        mine2 = [k for k, a in zip(retry, sub) if alive[a] == rank]
+        second = gather(run(mine2) if rank in alive else {"rank": rank, "ok": True, "records": []})
+        for g in second:
+            if g["ok"]:
+                records += g["records"]
+        redistributed = len(retry)
+    records.sort(key=lambda r: r["index"])
+    done = {r["index"] for r in records}
+    summary = {"ranks": world, "requests": len(systems), "completed": len(done),
+               "failed_ranks": failed_ranks, "redistributed": redistributed,
+               "errors": [g["error"] for g in first if not g["ok"]],
+               "atoms": int(sum(r["n_atoms"] for r in records))}
+    return records, summary
+
+
+def server_run_local(**server_kw):
+    """``run_local`` for ``serve_replicated``: this rank's share on an ``AdmpServer`` on its GPU
+    (keyword arguments as ``AdmpServer``; capacity defaults to the share's largest request)."""
+    def run_local(systems, arrivals):
+        if not systems:
+            return []
+        kw = dict(server_kw)
+        kw.setdefault("capacity_atoms", max(s["n_atoms"] for s in systems))
+        srv = AdmpServer(**kw)
+        try:
+            reqs, _ = srv.run_stream(systems, arrivals)
+        finally:
+            srv.close()
+        return [{"n_atoms": r.n_atoms, "latency": r.latency, "energy": r.energy, "status": r.status,
+                 "box_grad": r.box_grad.tolist()} for r in reqs]
+    return run_local
