@@ -1796,16 +1796,22 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     make_box(box, bx);
     const double* m = bx.h;
     const double V = fabs(det3(m));
-    int nc[3];
-    bool cells = true;
+    int nc[3], nc2[3];
+    bool cells = true, fine = true;  // fine: half-width cells with the 5^3 stencil
     for (int k = 0; k < 3; ++k) {
         const double* u = m + 3 * ((k + 1) % 3);
         const double* w = m + 3 * ((k + 2) % 3);
         const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
-        nc[k] = (int)floor(V / sqrt(cx * cx + cy * cy + cz * cz) / h->rc);
+        const double width = V / sqrt(cx * cx + cy * cy + cz * cz);
+        nc[k] = (int)floor(width / h->rc);
         if (nc[k] > 64) nc[k] = 64;
         if (nc[k] < 3) cells = false;
+        nc2[k] = (int)floor(width / (0.5 * h->rc));
+        if (nc2[k] > 64) nc2[k] = 64;
+        if (nc2[k] < 5) fine = false;
     }
+    if (fine && cells)
+        for (int k = 0; k < 3; ++k) nc[k] = nc2[k];
     if (!cells) {  // small boxes: the generic builder, CSR later from the rows
         int64_t need = 0;
         int st = dmffb_build_neighbors(h, stream, pos, box, h->rc, h->d_pairs, h->pair_cap, &need);
@@ -1886,7 +1892,8 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.posf = h->d_posf;
     b.count_f = h->d_pcount_f;
     b.off_f = h->d_csr_off;
-    LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
+    if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
+    else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
     CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
     tb = h->cub_bytes;
@@ -1911,7 +1918,8 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.a.cap = h->pair_cap;
     b.ent = h->d_csr_ent;
     b.cap_f = h->csr_cap;
-    LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
+    if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<1, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
+    else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     prof_collect(h);

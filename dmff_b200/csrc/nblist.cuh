@@ -333,6 +333,124 @@ __global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
     }
 }
 
+// k_pairs_warp2 over a finer cell grid: cells at least rc / S wide and a (2S + 1)^3 stencil
+// (S = 2: 125 cells of half width, about 0.58 of the 27-cell search volume).  The warp first
+// lays the stencil's cells out as one concatenated candidate list (cell starts and a prefix sum of
+// their counts in shared memory, in the dx, dy, dz order of the 27-cell scan), then walks it in
+// full 32-lane batches; each lane finds its candidate's cell by advancing a cursor (lanes move
+// forward monotonically).  Rows come out grouped by i like the coarse scan's.
+constexpr int kNbWarps = 8;  // warps per block of k_pairs_warp3
+
+template <int PASS, int S>
+__global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
+    constexpr int W = 2 * S + 1, NQ = W * W * W;
+    __shared__ int s_beg[kNbWarps][NQ];
+    __shared__ int s_off[kNbWarps][NQ + 1];
+    const NbArgs& a = b.a;
+    const int wl = threadIdx.x >> 5;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= a.n) return;  // whole warps leave together
+    const double* pi = a.pos + 3 * i;
+    const float pix = b.posf[4 * i], piy = b.posf[4 * i + 1], piz = b.posf[4 * i + 2];
+    float hf[9], hif[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { hf[k] = (float)a.box.h[k]; hif[k] = (float)a.box.hinv[k]; }
+    const float rlo = (float)(a.rc - 2e-3), rhi = (float)(a.rc + 2e-3);
+    const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
+    int c3[3];
+    cell_of(a.box, a.nc, pi, c3);
+    // stencil cells -> (start, count), prefix-summed in q order
+    int carry = 0;
+    if (lane == 0) s_off[wl][0] = 0;
+    for (int q0 = 0; q0 < NQ; q0 += 32) {
+        const int q = q0 + lane;
+        int cnt = 0;
+        if (q < NQ) {
+            const int dx = q / (W * W) - S, dy = (q / W) % W - S, dz = q % W - S;
+            const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
+            const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
+            const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
+            const int cc = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+            const int cs = a.cell_start[cc];
+            cnt = a.cell_start[cc + 1] - cs;
+            s_beg[wl][q] = cs;
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (q < NQ) s_off[wl][q + 1] = carry + incl;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+    const int total = carry;
+    int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1) ? b.off_f[i] : 0;
+    int cnt_h = 0, cnt_f = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    int qc = 0;
+    for (int base = 0; base < total; base += 32) {
+        const int t = base + lane;
+        bool keep = false;
+        int j = -1;
+        if (t < total) {
+            while (t >= s_off[wl][qc + 1]) ++qc;
+            j = a.cell_atoms[s_beg[wl][qc] + (t - s_off[wl][qc])];
+            if (j != i) {
+                const float d0 = b.posf[4 * j] - pix, d1 = b.posf[4 * j + 1] - piy, d2 = b.posf[4 * j + 2] - piz;
+                bool amb = false;
+                float sf[3];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    float tt = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
+                    float nn = floorf(tt + 0.5f);
+                    sf[q] = tt - nn;
+                    amb |= fabsf(sf[q]) > 0.4999f;
+                }
+                const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
+                const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
+                const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
+                const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
+                if (!amb && r2 < rlo2) keep = true;
+                else if (!amb && r2 > rhi2) keep = false;
+                else keep = j > i ? within_rc(a.box, pi, a.pos + 3 * j, a.rc)
+                                  : within_rc(a.box, a.pos + 3 * j, pi, a.rc);
+            }
+        }
+        const bool up = keep && j > i;
+        const unsigned mf = __ballot_sync(0xffffffffu, keep);
+        const unsigned mh = __ballot_sync(0xffffffffu, up);
+        if (PASS == 1) {
+            if (keep) {
+                const int nbd = j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i);
+                int sidx = nbd - 1;
+                if (sidx < 0) sidx += 6;
+                const int64_t sf_ = out_f + __popc(mf & lt);
+                if (sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
+                if (up) {
+                    const int64_t sh = out_h + __popc(mh & lt);
+                    if (sh < a.cap) {
+                        a.pairs[3 * sh] = i;
+                        a.pairs[3 * sh + 1] = j;
+                        a.pairs[3 * sh + 2] = nbd;
+                    }
+                }
+            }
+            out_f += __popc(mf);
+            out_h += __popc(mh);
+        } else {
+            cnt_f += __popc(mf);
+            cnt_h += __popc(mh);
+        }
+    }
+    if (PASS == 0 && lane == 0) {
+        a.count[i] = cnt_h;
+        b.count_f[i] = cnt_f;
+    }
+}
+
 static __global__ void k_pos_f32(int n, const double* pos, float* posf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
