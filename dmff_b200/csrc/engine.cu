@@ -1890,34 +1890,40 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.a.count = h->d_pcount;
     b.a.offset = h->d_poff;
     b.posf = h->d_posf;
-    b.count_f = h->d_pcount_f;
-    b.off_f = h->d_csr_off;
+    // the full CSR feeds only the polarizable dipole solve; other engines take the half rows alone
+    const bool want_csr = h->kind == 0 && h->lpol;
+    b.count_f = want_csr ? h->d_pcount_f : nullptr;
+    b.off_f = want_csr ? h->d_csr_off : nullptr;
+    b.ent = nullptr;
+    b.cap_f = 0;
     if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
-    CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
     tb = h->cub_bytes;
     LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount, h->d_poff + 1, n, s));
-    tb = h->cub_bytes;
-    LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount_f, h->d_csr_off + 1, n, s));
     int64_t tot[2] = {0, 0};
+    if (want_csr) {
+        CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
+        tb = h->cub_bytes;
+        LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount_f, h->d_csr_off + 1, n, s));
+        CK(cudaMemcpyAsync(&tot[1], h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    }
     CK(cudaMemcpyAsync(&tot[0], h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(&tot[1], h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     if (tot[0] > h->pair_cap) {
         if (h->d_pairs) cudaFree(h->d_pairs);
         h->pair_cap = (int64_t)(tot[0] * 1.3) + 64;  // headroom as in nblist.py:37-38
         if ((st = dalloc(h, &h->d_pairs, h->pair_cap * 3 * sizeof(int32_t)))) return st;
     }
-    if (tot[1] > h->csr_cap) {
+    if (want_csr && tot[1] > h->csr_cap) {
         if (h->d_csr_ent) cudaFree(h->d_csr_ent);
         h->csr_cap = (int64_t)(tot[1] * 1.3) + 1024;
         if ((st = dalloc(h, &h->d_csr_ent, h->csr_cap * sizeof(int32_t)))) return st;
     }
     b.a.pairs = h->d_pairs;
     b.a.cap = h->pair_cap;
-    b.ent = h->d_csr_ent;
-    b.cap_f = h->csr_cap;
+    b.ent = want_csr ? h->d_csr_ent : nullptr;
+    b.cap_f = want_csr ? h->csr_cap : 0;
     if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<1, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaGetLastError());
@@ -1926,7 +1932,7 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     h->npairs = tot[0];
     h->have_pairs = true;
     h->pairs_gen++;
-    h->csr_from_build = true;
+    h->csr_from_build = want_csr;
     return DMFFB_OK;
 }
 

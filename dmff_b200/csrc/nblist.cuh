@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256) k_pairs_warp(NbArgs a) {
 struct Nb2Args {
     NbArgs a;
     const float* posf;      // [n*4]
-    int32_t* count_f;       // [n] pass 0: full-list counts
+    int32_t* count_f;       // [n] pass 0: full-list counts (null: half rows only, no CSR)
     const int64_t* off_f;   // [n+1] pass 1
     int32_t* ent;           // [cap_f]
     int64_t cap_f;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
     const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
     int c3[3];
     cell_of(a.box, a.nc, pi, c3);
-    int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1) ? b.off_f[i] : 0;
+    int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1 && b.off_f) ? b.off_f[i] : 0;
     int cnt_h = 0, cnt_f = 0;
     const unsigned lt = (1u << lane) - 1u;
     for (int dx = -1; dx <= 1; ++dx) {
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
                             int sidx = nbd - 1;
                             if (sidx < 0) sidx += 6;
                             const int64_t sf_ = out_f + __popc(mf & lt);
-                            if (sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
+                            if (b.ent && sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
                             if (up) {
                                 const int64_t sh = out_h + __popc(mh & lt);
                                 if (sh < a.cap) {
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
     }
     if (PASS == 0 && lane == 0) {
         a.count[i] = cnt_h;
-        b.count_f[i] = cnt_f;
+        if (b.count_f) b.count_f[i] = cnt_f;
     }
 }
 
@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
     }
     __syncwarp();
     const int total = carry;
-    int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1) ? b.off_f[i] : 0;
+    int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1 && b.off_f) ? b.off_f[i] : 0;
     int cnt_h = 0, cnt_f = 0;
     const unsigned lt = (1u << lane) - 1u;
     int qc = 0;
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
                 int sidx = nbd - 1;
                 if (sidx < 0) sidx += 6;
                 const int64_t sf_ = out_f + __popc(mf & lt);
-                if (sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
+                if (b.ent && sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
                 if (up) {
                     const int64_t sh = out_h + __popc(mh & lt);
                     if (sh < a.cap) {
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
     }
     if (PASS == 0 && lane == 0) {
         a.count[i] = cnt_h;
-        b.count_f[i] = cnt_f;
+        if (b.count_f) b.count_f[i] = cnt_f;
     }
 }
 
