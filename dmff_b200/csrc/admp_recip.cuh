@@ -113,6 +113,7 @@ struct SpreadArgs {
     MeshGeom g;
     T* grid;
     int perm_mul;  // warps visit atoms in the order (w * perm_mul) mod n, gcd(perm_mul, n) = 1
+    double* zero_scal[3] = {nullptr, nullptr, nullptr};  // scalars thread 0 of block 0 sets to 0 (may be null)
 };
 
 template <typename T>
@@ -203,6 +204,8 @@ struct ConvArgs {
     int kind;
     double* scal;        // [0] energy, [1..6] sum E_k (dlnC/dk2) k k  (xx,yy,zz,xy,xz,yz)
     int want_energy;
+    T* zero_real = nullptr;  // real grid of nzero elements the kernel sets to 0 (may be null)
+    int64_t nzero = 0;
 };
 
 // influence function C(k^2) and d ln C / d k^2
@@ -286,6 +289,8 @@ __global__ void __launch_bounds__(256) k_conv(ConvArgs<T> a) {
         s[0] = (T)(re * G);
         s[1] = (T)(im * G);
     }
+    // the spread input of this pass has been transformed: clear it for the next spread
+    for (int64_t i = idx; i < a.nzero; i += (int64_t)gridDim.x * blockDim.x) a.zero_real[i] = T(0);
     if (a.want_energy) block_reduce_add<7>(red, a.scal);
 }
 
@@ -554,6 +559,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_spread_dip(SpreadArgs<T> a) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
     if (warp >= a.n) return;
     const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
     int m0[3];

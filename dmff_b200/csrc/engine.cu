@@ -83,6 +83,7 @@ struct dmffb_engine {
     void* d_cub2 = nullptr;
     size_t cub2_bytes = 0;
     void* d_grid = nullptr;
+    void* d_grid2 = nullptr;  // spread target of the dipole-only field pass, kept zero between passes
     void* d_cgrid = nullptr;
     double* d_bmod = nullptr;
     cufftHandle plan_f = 0, plan_b = 0;
@@ -296,23 +297,30 @@ inline void prof_collect(dmffb_engine* h) {
     } while (0)
 
 // ------------------------------------------------------------------ small vector kernels
+// out = recip + fT + mv + (1/pol + self) U [+ self * permanent dipole]; with dot_out, also
+// accumulates dot(dotv, out) into *dot_out (the p.Ap of a CG step)
 template <typename T>
 __global__ void k_field_combine(int n, const double* recip, const T* fT, const double* mv, const double* U,
-                                const double* Qg, const double* pol, double self1, int include_perm, double* out) {
+                                const double* Qg, const double* pol, double self1, int include_perm, double* out,
+                                const double* dotv, double* dot_out) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= 3 * n) return;
-    const int a = k / 3, c = k % 3;
-    double p = pol[a];
-    p = p < 1e-8 ? 1e-8 : p;
-    double v = recip ? recip[k] : 0.0;
-    if (fT) v += (double)fT[k];
-    if (mv) v += mv[k];
-    if (U) v += (DMFFB_DIELECTRIC / p + self1) * U[k];
-    if (include_perm) {
-        const int hidx = c == 0 ? 2 : (c == 1 ? 3 : 1);
-        v += self1 * Qg[9 * a + hidx];
+    double d[1] = {0.0};
+    if (k < 3 * n) {
+        const int a = k / 3, c = k % 3;
+        double p = pol[a];
+        p = p < 1e-8 ? 1e-8 : p;
+        double v = recip ? recip[k] : 0.0;
+        if (fT) v += (double)fT[k];
+        if (mv) v += mv[k];
+        if (U) v += (DMFFB_DIELECTRIC / p + self1) * U[k];
+        if (include_perm) {
+            const int hidx = c == 0 ? 2 : (c == 1 ? 3 : 1);
+            v += self1 * Qg[9 * a + hidx];
+        }
+        out[k] = v;
+        if (dot_out) d[0] = dotv[k] * v;
     }
-    out[k] = v;
+    if (dot_out) block_reduce_add<1>(d, dot_out);
 }
 
 // CG helpers; scalars live in s[]: [0] rz(even) [1] rz(odd) [2] pAp [3] rr
@@ -474,10 +482,14 @@ int lmax_eff(const dmffb_engine* h) { return (h->lmax == 0 && h->lpol) ? 1 : h->
 // reciprocal pass: spread (Qg and/or U) -> FFT -> convolution -> inverse FFT -> gather
 template <typename T>
 int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, bool use_Qg, const double* U,
-               int mode, double* field_out, int field_acc) {
+               int mode, double* field_out, int field_acc, double* const* zero_scal = nullptr) {
     const MeshGeom g = mesh_geom(bx, h->K);
     const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
-    CK(cudaMemsetAsync(h->d_grid, 0, K3 * sizeof(T), s));
+    // the dipole-only field pass (the CG matvec) spreads into d_grid2, which the convolution
+    // clears again once the forward transform has read it: no memset per pass
+    const bool dip = mode == GATHER_FIELD && !use_Qg && U;
+    void* spread_grid = dip ? h->d_grid2 : h->d_grid;
+    if (!dip) CK(cudaMemsetAsync(h->d_grid, 0, K3 * sizeof(T), s));
     SpreadArgs<T> sa;
     sa.n = h->n;
     sa.pos = pos;
@@ -486,18 +498,20 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     sa.q1 = nullptr;
     sa.lmax = lmax_eff(h);
     sa.g = g;
-    sa.grid = (T*)h->d_grid;
+    sa.grid = (T*)spread_grid;
     sa.perm_mul = h->perm_mul;
-    if (mode == GATHER_FIELD && !use_Qg && U)
+    if (zero_scal)
+        for (int k = 0; k < 3; ++k) sa.zero_scal[k] = zero_scal[k];
+    if (dip)
         LAUNCH(h, s, KC_SPREAD, k_spread_dip<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
     else
         LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
     CKFFT(cufftSetStream(h->plan_f, s));
     CKFFT(cufftSetStream(h->plan_b, s));
     if (sizeof(T) == 4) {
-        FFTCALL(h, s, cufftExecR2C(h->plan_f, (cufftReal*)h->d_grid, (cufftComplex*)h->d_cgrid));
+        FFTCALL(h, s, cufftExecR2C(h->plan_f, (cufftReal*)spread_grid, (cufftComplex*)h->d_cgrid));
     } else {
-        FFTCALL(h, s, cufftExecD2Z(h->plan_f, (cufftDoubleReal*)h->d_grid, (cufftDoubleComplex*)h->d_cgrid));
+        FFTCALL(h, s, cufftExecD2Z(h->plan_f, (cufftDoubleReal*)spread_grid, (cufftDoubleComplex*)h->d_cgrid));
     }
     ConvArgs<T> ca;
     for (int k = 0; k < 3; ++k) ca.K[k] = h->K[k];
@@ -511,6 +525,10 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     ca.kind = CK_COUL;
     ca.scal = h->d_scal + S_RECIP;
     ca.want_energy = (mode == GATHER_FULL) ? 1 : 0;
+    if (dip) {
+        ca.zero_real = (T*)h->d_grid2;
+        ca.nzero = K3;
+    }
     const int64_t nk = (int64_t)h->K[0] * h->K[1] * ca.Kh;
     LAUNCH(h, s, KC_CONV, k_conv<T><<<nblk(nk, 256), 256, 0, s>>>(ca));
     if (sizeof(T) == 4) {
@@ -599,10 +617,17 @@ int build_csr(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npa
     return DMFFB_OK;
 }
 
-// dE/dU at U (include_perm) or its linear part A U (!include_perm), into out
+// dE/dU at U (include_perm) or its linear part A U (!include_perm), into out.  With dot_out,
+// dot(dotv, out) is accumulated into *dot_out; zero_scal names three scalars set to 0 before
+// the combine (by the first kernel of the reciprocal pass when there is one)
 template <typename T>
 int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
-               int64_t npairs, const double* U, bool include_perm, double* out) {
+               int64_t npairs, const double* U, bool include_perm, double* out, const double* dotv = nullptr,
+               double* dot_out = nullptr, double* const* zero_scal = nullptr) {
+    const bool recip_on = h->lpme && h->have_plans;
+    if (zero_scal && !recip_on)
+        for (int k = 0; k < 3; ++k)
+            if (zero_scal[k]) CK(cudaMemsetAsync(zero_scal[k], 0, sizeof(double), s));
     if (include_perm) CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
     if (include_perm && npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
@@ -635,8 +660,8 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
         if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
     const double* recip = nullptr;
-    if (h->lpme && h->have_plans) {
-        int st = recip_pass<T>(h, s, pos, bx, include_perm, U, GATHER_FIELD, h->d_fr, 0);
+    if (recip_on) {
+        int st = recip_pass<T>(h, s, pos, bx, include_perm, U, GATHER_FIELD, h->d_fr, 0, zero_scal);
         if (st) return st;
         recip = h->d_fr;
     }
@@ -645,7 +670,7 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     const double self1 = h->lpme ? -2.0 * DMFFB_DIELECTRIC * (k / 1.7724538509055159) * 2.0 * k * k / 3.0 : 0.0;
     LAUNCH(h, s, KC_VEC, k_field_combine<T><<<nblk(3 * h->n, 256), 256, 0, s>>>(
                              h->n, recip, include_perm ? (const T*)h->d_fieldT : nullptr, U ? h->d_fmv : nullptr, U,
-                             h->d_Qg, h->d_pol, self1, include_perm ? 1 : 0, out));
+                             h->d_Qg, h->d_pol, self1, include_perm ? 1 : 0, out, dotv, dot_out));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
@@ -686,7 +711,10 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         res->residual_rms = conv && h->steps_pol <= 0 ? h->h_scal[0] : -1.0;
         return DMFFB_OK;
     }
-    // CG on A U = -b
+    // CG on A U = -b.  The dipole-only field passes keep d_grid2 zero between passes; clear it
+    // here so that an earlier solve that stopped part-way leaves nothing behind
+    if (h->lpme && h->have_plans)
+        CK(cudaMemsetAsync(h->d_grid2, 0, (size_t)h->K[0] * h->K[1] * h->K[2] * sizeof(T), s));
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b))) return st;
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
     LAUNCH(h, s, KC_VEC, k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_Ap, h->d_pol, h->d_r, h->d_z, h->d_p));
@@ -699,10 +727,10 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     // one CG iteration; slot = parity of the r.z scalar it reads
     auto iteration = [&](int slot) -> int {
         int st2;
-        if ((st2 = field_eval<T>(h, s, pos, bx, pairs, npairs, h->d_p, false, h->d_Ap))) return st2;
-        CK(cudaMemsetAsync(sc + 2, 0, 2 * sizeof(double), s));  // pAp, rr
-        CK(cudaMemsetAsync(sc + (1 - slot), 0, sizeof(double), s));
-        LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_p, h->d_Ap, nullptr, nullptr, sc + 2, nullptr));
+        // Ap = A p with p.Ap reduced into sc[2]; pAp, rr and the r.z slot this step writes are
+        // cleared at the head of the pass (the previous step has read them by then)
+        double* const zs[3] = {sc + 2, sc + 3, sc + (1 - slot)};
+        if ((st2 = field_eval<T>(h, s, pos, bx, pairs, npairs, h->d_p, false, h->d_Ap, h->d_p, sc + 2, zs))) return st2;
         LAUNCH(h, s, KC_VEC, k_cg_update<<<nb3, 256, 0, s>>>(n, sc, slot, U, h->d_r, h->d_z, h->d_p, h->d_Ap,
                                                            h->d_pol, sc + (1 - slot), sc + 3));
         LAUNCH(h, s, KC_VEC, k_cg_p<<<nb3, 256, 0, s>>>(n, sc, slot, 1 - slot, h->d_z, h->d_p));
@@ -747,7 +775,7 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         for (int k = 0; k < check_every; k += 2) {
             if (graphs) {
                 CK(cudaGraphLaunch(h->cg_exec, s));
-                h->n_launch += 2 * 8;
+                h->n_launch += 2 * 7;
                 h->n_fft += 4;
             } else {
                 if ((st = iteration(0))) return st;
@@ -1351,8 +1379,11 @@ int setup_mesh(dmffb_engine* h) {
     if (K3 > h->grid_cap) {
         if (h->d_grid) cudaFree(h->d_grid);
         h->d_grid = nullptr;
+        if (h->d_grid2) cudaFree(h->d_grid2);
+        h->d_grid2 = nullptr;
         h->grid_cap = K3;
         if ((st = dalloc(h, &h->d_grid, K3 * ts))) return st;
+        if ((st = dalloc(h, &h->d_grid2, K3 * ts))) return st;
     }
     if (Kc > h->cgrid_cap) {
         if (h->d_cgrid) cudaFree(h->d_cgrid);
@@ -1506,7 +1537,7 @@ void dmffb_destroy(dmffb_engine* h) {
     void* ptrs[] = {h->d_axis_type, h->d_axis_idx, h->d_cov_ptr, h->d_cov_j, h->d_cov_nb, h->d_Qloc, h->d_pol,
                     h->d_thole, h->d_polsix, h->d_pos, h->d_U, h->d_forces, h->d_posT, h->d_Qg, h->d_QgT,
                     h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
-                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
+                    h->d_Ap, h->d_fr, h->d_gQ, h->d_fmv, h->d_posf, h->d_pcount_f, h->d_mvcoef, h->d_csr_off, h->d_csr_ent, h->d_csr_deg, h->d_cub2, h->d_grid, h->d_grid2, h->d_cgrid, h->d_bmod, h->d_pairs, h->d_atom_cell,
                     h->d_cell_count, h->d_cell_start, h->d_cell_cursor, h->d_cell_atoms, h->d_pcount, h->d_poff,
                     h->d_c, h->d_tta, h->d_ttb, h->d_ttq, h->d_glr, h->d_gsr, h->d_dc,
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,

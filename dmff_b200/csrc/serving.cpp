@@ -125,12 +125,13 @@ extern "C" {
 
 int64_t dmffb_request_footprint(int32_t n_atoms, double rc, const int32_t K[3], double box_volume, int32_t lpol) {
     // accounting convention: per-atom engine arrays, neighbour rows + both-direction CSR with the
-    // matvec pair tensors, and the mesh with its complex transform and cuFFT work area
+    // matvec pair tensors, and the mesh with its complex transform, cuFFT work area and (with
+    // polarization) the second real grid of the dipole field pass
     const double n = n_atoms;
     const double dens = box_volume > 0 ? n / box_volume : 0.1;
     const double half_pairs = n * dens * (4.0 / 3.0) * M_PI * rc * rc * rc / 2.0;
     const double K3 = (double)K[0] * K[1] * K[2];
-    const double bytes = n * (600.0 + (lpol ? 160.0 : 0.0)) + half_pairs * 92.0 + 16.0 * K3;
+    const double bytes = n * (600.0 + (lpol ? 160.0 : 0.0)) + half_pairs * 92.0 + (lpol ? 20.0 : 16.0) * K3;
     return (int64_t)bytes;
 }
 
