@@ -636,4 +636,119 @@ __global__ void __launch_bounds__(256) k_gather_field(int n, const double* pos, 
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Stencil cache for the CG loop.  Positions are fixed during the dipole solve, so the wrapped
+// first stencil point (m0 - 3 per dimension) and the value / first-derivative B-spline weights
+// of every atom are computed once per evaluation (k_stencil_prep, with the same arithmetic as
+// stencil01) and read by the cached dipole spread and field gather, instead of every lane
+// recomputing three spline sets and two integer wraps per pass in every iteration.
+// Weights per atom: Mx0[6] Mx1[6] My0[6] My1[6] Mz0[6] Mz1[6].
+template <typename T>
+struct StencilCache {
+    const int4* org;  // wrapped first stencil point per dimension (w unused)
+    const T* w;       // [n * 36]
+};
+
+// g + d wrapped into [0, K) for g in [0, K), d >= 0
+__device__ __forceinline__ int wrap_up(int g, int K) {
+    while (g >= K) g -= K;
+    return g;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_stencil_prep(int n, const double* pos, MeshGeom g, int4* org, T* w) {
+    const int at = blockIdx.x * blockDim.x + threadIdx.x;
+    if (at >= n) return;
+    int m0[3];
+    T Mx[2][6], My[2][6], Mz[2][6];
+    stencil01<T>(g, pos, at, m0, Mx, My, Mz);
+    org[at] = make_int4(wrapi(m0[0] - 3, g.K[0]), wrapi(m0[1] - 3, g.K[1]), wrapi(m0[2] - 3, g.K[2]), 0);
+    T* o = w + 36 * (size_t)at;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        o[j] = Mx[0][j];
+        o[6 + j] = Mx[1][j];
+        o[12 + j] = My[0][j];
+        o[18 + j] = My[1][j];
+        o[24 + j] = Mz[0][j];
+        o[30 + j] = Mz[1][j];
+    }
+}
+
+// k_spread_dip with the cached stencil (same lane layout and per-point arithmetic)
+template <typename T>
+__global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, StencilCache<T> st) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
+    if (warp >= a.n) return;
+    const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
+    const int grp = lane / 6, iz = lane - 6 * grp;
+    if (grp >= 5) return;
+    const int4 o = st.org[at];
+    const T* w = st.w + 36 * (size_t)at;
+    const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
+    const double* B = a.g.B;
+    const T c1 = -(T(B[0]) * mu0 + T(B[1]) * mu1 + T(B[2]) * mu2);
+    const T c2 = -(T(B[3]) * mu0 + T(B[4]) * mu1 + T(B[5]) * mu2);
+    const T c3 = -(T(B[6]) * mu0 + T(B[7]) * mu1 + T(B[8]) * mu2);
+    const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
+    const T mz0 = __ldg(w + 24 + iz), mz1 = __ldg(w + 30 + iz);
+    const int gz = wrap_up(o.z + iz, K2);
+#pragma unroll
+    for (int pass = 0; pass < 8; ++pass) {
+        const int col = grp + 5 * pass;
+        if (col < 36) {
+            const int ix = col / 6, iy = col - 6 * ix;
+            const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy), my1 = __ldg(w + 18 + iy);
+            const T v = (c1 * mx1 * my0 + c2 * mx0 * my1) * mz0 + c3 * mx0 * my0 * mz1;
+            const int gx = wrap_up(o.x + ix, K0), gy = wrap_up(o.y + iy, K1);
+            atomicAdd(a.grid + ((size_t)gx * K1 + gy) * K2 + gz, v);
+        }
+    }
+}
+
+// k_gather_field with the cached stencil; lanes take the spread's layout (five columns of six z
+// points per pass, eight passes), so every lane issues eight independent mesh loads
+template <typename T>
+__global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache<T> st, MeshGeom g, const T* phi,
+                                                             double scale, double* out) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int at = warp;
+    const int grp = lane / 6, iz = lane - 6 * grp;
+    T p1 = T(0), p2 = T(0), p3 = T(0);
+    if (grp < 5) {
+        const int4 o = st.org[at];
+        const T* w = st.w + 36 * (size_t)at;
+        const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
+        const T mz0 = __ldg(w + 24 + iz), mz1 = __ldg(w + 30 + iz);
+        const int gz = wrap_up(o.z + iz, K2);
+#pragma unroll
+        for (int pass = 0; pass < 8; ++pass) {
+            const int col = grp + 5 * pass;
+            if (col < 36) {
+                const int ix = col / 6, iy = col - 6 * ix;
+                const int gx = wrap_up(o.x + ix, K0), gy = wrap_up(o.y + iy, K1);
+                const T v = __ldg(phi + ((size_t)gx * K1 + gy) * K2 + gz);
+                const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy), my1 = __ldg(w + 18 + iy);
+                const T t0 = mz0 * v;
+                p1 += mx1 * my0 * t0;
+                p2 += mx0 * my1 * t0;
+                p3 += mx0 * my0 * (mz1 * v);
+            }
+        }
+    }
+    p1 = warp_sum(p1);
+    p2 = warp_sum(p2);
+    p3 = warp_sum(p3);
+    if (lane == 0) {
+        const double* B = g.B;
+        const double P1 = scale * (double)p1, P2 = scale * (double)p2, P3 = scale * (double)p3;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[3 * at + c] = -(P1 * B[c] + P2 * B[3 + c] + P3 * B[6 + c]);
+    }
+}
+
 }  // namespace dmffb

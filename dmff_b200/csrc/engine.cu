@@ -154,6 +154,11 @@ struct dmffb_engine {
     size_t cubsel_bytes = 0;
     const int32_t* srows_pairs = nullptr;  // the pair list the row map belongs to
     int64_t srows_npairs = -1, srows_gen = -1, pairs_gen = 0;
+    // ---- per-atom mesh stencils of the evaluation in progress (cached dipole spread / gather)
+    int4* d_stc_org = nullptr;
+    void* d_stc_w = nullptr;
+    int64_t stc_cap = 0;
+    bool stencils_ready = false;
     // ---- capacities (dmffb_admp_reconfigure reuses the allocations for systems that fit)
     int n_cap = 0;
     int64_t cov_cap = 0, grid_cap = 0, cgrid_cap = 0;
@@ -480,6 +485,35 @@ PairArgs<T> pair_args(dmffb_engine* h, const Box& bx, const int32_t* pairs, int6
 int lmax_eff(const dmffb_engine* h) { return (h->lmax == 0 && h->lpol) ? 1 : h->lmax; }
 
 // reciprocal pass: spread (Qg and/or U) -> FFT -> convolution -> inverse FFT -> gather
+// per-atom wrapped stencil origins and spline weights at these positions, for the cached dipole
+// spread and field gather of the dipole solve
+template <typename T>
+int stencil_prep(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx) {
+    const int n = h->n;
+    int st;
+    if (n > h->stc_cap) {
+        if (h->d_stc_org) cudaFree(h->d_stc_org);
+        if (h->d_stc_w) cudaFree(h->d_stc_w);
+        h->d_stc_org = nullptr;
+        h->d_stc_w = nullptr;
+        h->stc_cap = n;
+        if ((st = dalloc(h, &h->d_stc_org, (size_t)n * sizeof(int4)))) return st;
+        if ((st = dalloc(h, &h->d_stc_w, (size_t)n * 36 * sizeof(double)))) return st;
+    }
+    LAUNCH(h, s, KC_VEC, k_stencil_prep<T><<<nblk(n, 128), 128, 0, s>>>(n, pos, mesh_geom(bx, h->K), h->d_stc_org,
+                                                                        (T*)h->d_stc_w));
+    h->stencils_ready = true;
+    return DMFFB_OK;
+}
+
+template <typename T>
+StencilCache<T> stencil_cache(dmffb_engine* h) {
+    StencilCache<T> c;
+    c.org = h->d_stc_org;
+    c.w = (const T*)h->d_stc_w;
+    return c;
+}
+
 template <typename T>
 int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, bool use_Qg, const double* U,
                int mode, double* field_out, int field_acc, double* const* zero_scal = nullptr) {
@@ -502,7 +536,9 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     sa.perm_mul = h->perm_mul;
     if (zero_scal)
         for (int k = 0; k < 3; ++k) sa.zero_scal[k] = zero_scal[k];
-    if (dip)
+    if (dip && h->stencils_ready)
+        LAUNCH(h, s, KC_SPREAD, k_spread_dip_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa, stencil_cache<T>(h)));
+    else if (dip)
         LAUNCH(h, s, KC_SPREAD, k_spread_dip<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
     else
         LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
@@ -555,7 +591,10 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     ga.scal = h->d_scal + S_GATHER;
     ga.want_box = 1;
     ga.mode = mode;
-    if (mode == GATHER_FIELD && !field_acc)
+    if (mode == GATHER_FIELD && !field_acc && h->stencils_ready)
+        LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
+                                          h->n, stencil_cache<T>(h), g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, field_out));
+    else if (mode == GATHER_FIELD && !field_acc)
         LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
                                           h->n, pos, g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, field_out));
     else
@@ -713,8 +752,15 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     }
     // CG on A U = -b.  The dipole-only field passes keep d_grid2 zero between passes; clear it
     // here so that an earlier solve that stopped part-way leaves nothing behind
-    if (h->lpme && h->have_plans)
+    // the stencil cache holds for these positions only: it is dropped when the solve returns
+    struct StencilScope {
+        dmffb_engine* h;
+        ~StencilScope() { h->stencils_ready = false; }
+    } stencil_scope{h};
+    if (h->lpme && h->have_plans) {
         CK(cudaMemsetAsync(h->d_grid2, 0, (size_t)h->K[0] * h->K[1] * h->K[2] * sizeof(T), s));
+        if ((st = stencil_prep<T>(h, s, pos, bx))) return st;
+    }
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b))) return st;
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
     LAUNCH(h, s, KC_VEC, k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_Ap, h->d_pol, h->d_r, h->d_z, h->d_p));
@@ -1543,7 +1589,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub};
+                    h->d_cub, h->d_stc_org, h->d_stc_w};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);

@@ -131,7 +131,7 @@ int64_t dmffb_request_footprint(int32_t n_atoms, double rc, const int32_t K[3], 
     const double dens = box_volume > 0 ? n / box_volume : 0.1;
     const double half_pairs = n * dens * (4.0 / 3.0) * M_PI * rc * rc * rc / 2.0;
     const double K3 = (double)K[0] * K[1] * K[2];
-    const double bytes = n * (600.0 + (lpol ? 160.0 : 0.0)) + half_pairs * 92.0 + (lpol ? 20.0 : 16.0) * K3;
+    const double bytes = n * (600.0 + (lpol ? 320.0 : 0.0)) + half_pairs * 92.0 + (lpol ? 20.0 : 16.0) * K3;
     return (int64_t)bytes;
 }
 
