@@ -683,11 +683,11 @@ __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, Sten
     if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
     if (warp >= a.n) return;
     const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
+    const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
     const int grp = lane / 6, iz = lane - 6 * grp;
     if (grp >= 5) return;
     const int4 o = st.org[at];
     const T* w = st.w + 36 * (size_t)at;
-    const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
     const double* B = a.g.B;
     const T c1 = -(T(B[0]) * mu0 + T(B[1]) * mu1 + T(B[2]) * mu2);
     const T c2 = -(T(B[3]) * mu0 + T(B[4]) * mu1 + T(B[5]) * mu2);
@@ -708,18 +708,30 @@ __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, Sten
     }
 }
 
+// Field terms folded into the gather: out = recip [+ mv] [+ (1/pol + self1) U]; with dot_out,
+// sum U . out is reduced into *dot_out; *zero1 is cleared by thread 0 of block 0.
+struct FieldCombine {
+    const double* mv = nullptr;  // real-space matvec field (may be null)
+    const double* U = nullptr;   // dipoles of the diagonal term (null: no diagonal term)
+    const double* pol = nullptr;
+    double self1 = 0.0;
+    double* dot_out = nullptr;
+    double* zero1 = nullptr;
+};
+
 // k_gather_field with the cached stencil; lanes take the spread's layout (five columns of six z
 // points per pass, eight passes), so every lane issues eight independent mesh loads
 template <typename T>
 __global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache<T> st, MeshGeom g, const T* phi,
-                                                             double scale, double* out) {
+                                                             double scale, double* out, FieldCombine cmb) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const int at = warp;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && cmb.zero1) *cmb.zero1 = 0.0;
+    const bool active = warp < n;
+    const int at = active ? warp : 0;
     const int grp = lane / 6, iz = lane - 6 * grp;
     T p1 = T(0), p2 = T(0), p3 = T(0);
-    if (grp < 5) {
+    if (active && grp < 5) {
         const int4 o = st.org[at];
         const T* w = st.w + 36 * (size_t)at;
         const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
@@ -743,12 +755,26 @@ __global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache
     p1 = warp_sum(p1);
     p2 = warp_sum(p2);
     p3 = warp_sum(p3);
-    if (lane == 0) {
+    double d[1] = {0.0};
+    if (active && lane == 0) {
         const double* B = g.B;
         const double P1 = scale * (double)p1, P2 = scale * (double)p2, P3 = scale * (double)p3;
+        double pp = 0.0;
+        if (cmb.U) {
+            pp = cmb.pol[at];
+            pp = pp < 1e-8 ? 1e-8 : pp;
+            pp = DMFFB_DIELECTRIC / pp + cmb.self1;
+        }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) out[3 * at + c] = -(P1 * B[c] + P2 * B[3 + c] + P3 * B[6 + c]);
+        for (int c = 0; c < 3; ++c) {
+            double v = -(P1 * B[c] + P2 * B[3 + c] + P3 * B[6 + c]);
+            if (cmb.mv) v += cmb.mv[3 * at + c];
+            if (cmb.U) v += pp * cmb.U[3 * at + c];
+            out[3 * at + c] = v;
+            if (cmb.dot_out) d[0] += cmb.U[3 * at + c] * v;
+        }
     }
+    if (cmb.dot_out) block_reduce_add<1>(d, cmb.dot_out);
 }
 
 }  // namespace dmffb

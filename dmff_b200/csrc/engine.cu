@@ -110,6 +110,7 @@ struct dmffb_engine {
     double kstat_ms[16] = {0};
     int64_t kstat_n[16] = {0};
     int64_t n_launch = 0, n_fft = 0;
+    int64_t cg_graph_launches = 0, cg_graph_ffts = 0;  // per replay of the two-iteration CG graph
     // ---- last result book-keeping
     Box last_box;
     const double* cur_pos = nullptr;  // FP64 positions of the evaluation in flight
@@ -353,16 +354,20 @@ __global__ void k_cg_init(int n, const double* b, const double* Ax, const double
     p[k] = z[k];
 }
 
+// Ap may come in two parts (Ap + Ap2, p.Ap = s[2] + s[5]); s[5] stays 0 when Ap2 is null
 __global__ void k_cg_update(int n, const double* s, int slot, double* x, double* r, double* z, const double* p,
-                            const double* Ap, const double* pol, double* rz_new, double* rr) {
+                            const double* Ap, const double* pol, double* rz_new, double* rr,
+                            const double* Ap2 = nullptr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const double alpha = s[2] != 0.0 ? s[slot] / s[2] : 0.0;
+    const double pAp = s[2] + s[5];
+    const double alpha = pAp != 0.0 ? s[slot] / pAp : 0.0;
     double v[1] = {0.0}, w[1] = {0.0};
     if (k < 3 * n) {
         double pp = pol[k / 3];
         pp = pp < 1e-8 ? 1e-8 : pp;
         x[k] += alpha * p[k];
-        const double rv = r[k] - alpha * Ap[k];
+        const double ap = Ap2 ? Ap[k] + Ap2[k] : Ap[k];
+        const double rv = r[k] - alpha * ap;
         r[k] = rv;
         const double zv = rv * pp / DMFFB_DIELECTRIC;
         z[k] = zv;
@@ -373,8 +378,10 @@ __global__ void k_cg_update(int n, const double* s, int slot, double* x, double*
     block_reduce_add<1>(w, rr);
 }
 
-__global__ void k_cg_p(int n, const double* s, int slot_old, int slot_new, const double* z, double* p) {
+__global__ void k_cg_p(int n, const double* s, int slot_old, int slot_new, const double* z, double* p,
+                       double* zero = nullptr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0 && zero) *zero = 0.0;
     if (k >= 3 * n) return;
     const double beta = s[slot_old] != 0.0 ? s[slot_new] / s[slot_old] : 0.0;
     p[k] = z[k] + beta * p[k];
@@ -593,12 +600,95 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     ga.mode = mode;
     if (mode == GATHER_FIELD && !field_acc && h->stencils_ready)
         LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
-                                          h->n, stencil_cache<T>(h), g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, field_out));
+                                          h->n, stencil_cache<T>(h), g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, field_out,
+                                          FieldCombine()));
     else if (mode == GATHER_FIELD && !field_acc)
         LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
                                           h->n, pos, g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, field_out));
     else
         LAUNCH(h, s, (mode == GATHER_FULL ? KC_GATHER_FULL : KC_GATHER_FIELD), k_gather<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(ga));
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
+// One CG step's direction update and matvec A p on the PME path with the stencil cache: k_cg_p
+// forms p = z + beta p (beta from the previous step's r.z) and clears sc[5]; the real-space
+// matvec forks onto the side stream, writes d_fmv and reduces p.fmv into sc[5], overlapping the
+// whole reciprocal pass; the dipole spread clears sc[2] and sc[3] (rr); the gather writes
+// d_Ap = recip + diagonal p, reduces p.d_Ap into sc[2] and clears sc[1 - slot], the r.z slot
+// this step's update writes.  A p = d_Ap + d_fmv; the caller joins the side stream
+// (h->e_join) before the update reads them.
+template <typename T>
+int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, int slot) {
+    const MeshGeom g = mesh_geom(bx, h->K);
+    SpreadArgs<T> sa;
+    sa.n = h->n;
+    sa.pos = nullptr;
+    sa.Qg = nullptr;
+    sa.U = h->d_p;
+    sa.q1 = nullptr;
+    sa.lmax = 1;
+    sa.g = g;
+    sa.grid = (T*)h->d_grid2;
+    sa.perm_mul = h->perm_mul;
+    sa.zero_scal[0] = sc + 2;
+    sa.zero_scal[1] = sc + 3;
+    LAUNCH(h, s, KC_VEC, k_cg_p<<<nblk(3 * h->n, 256), 256, 0, s>>>(h->n, sc, 1 - slot, slot, h->d_z, h->d_p, sc + 5));
+    const bool fork = h->s2 && !h->prof;
+    {
+        CsrArgs c;
+        c.n = h->n;
+        c.off = h->d_csr_off;
+        c.ent = h->d_csr_ent;
+        cudaStream_t sm = s;
+        if (fork) {
+            CK(cudaEventRecord(h->e_fork, s));
+            CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
+            sm = h->s2;
+        }
+        LAUNCH(h, sm, KC_PAIR_MATVEC, k_matvec_apply<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, sm>>>(
+                                          c, (const MvCoef<T>*)h->d_mvcoef, (const T*)h->d_posT, boxT<T>(bx), h->d_p, h->d_fmv,
+                                          sc + 5));
+        if (fork) CK(cudaEventRecord(h->e_join, h->s2));
+    }
+    LAUNCH(h, s, KC_SPREAD, k_spread_dip_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa, stencil_cache<T>(h)));
+    const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
+    CKFFT(cufftSetStream(h->plan_f, s));
+    CKFFT(cufftSetStream(h->plan_b, s));
+    if (sizeof(T) == 4)
+        FFTCALL(h, s, cufftExecR2C(h->plan_f, (cufftReal*)h->d_grid2, (cufftComplex*)h->d_cgrid));
+    else
+        FFTCALL(h, s, cufftExecD2Z(h->plan_f, (cufftDoubleReal*)h->d_grid2, (cufftDoubleComplex*)h->d_cgrid));
+    ConvArgs<T> ca;
+    for (int k = 0; k < 3; ++k) ca.K[k] = h->K[k];
+    ca.Kh = h->K[2] / 2 + 1;
+    ca.S = (T*)h->d_cgrid;
+    ca.bmod = h->d_bmod;
+    for (int k = 0; k < 9; ++k) ca.hinv[k] = bx.hinv[k];
+    ca.V = fabs(det3(bx.h));
+    ca.kappa = h->kappa;
+    ca.escale = DMFFB_DIELECTRIC;
+    ca.kind = CK_COUL;
+    ca.scal = h->d_scal + S_RECIP;
+    ca.want_energy = 0;
+    ca.zero_real = (T*)h->d_grid2;
+    ca.nzero = K3;
+    const int64_t nk = (int64_t)h->K[0] * h->K[1] * ca.Kh;
+    LAUNCH(h, s, KC_CONV, k_conv<T><<<nblk(nk, 256), 256, 0, s>>>(ca));
+    if (sizeof(T) == 4)
+        FFTCALL(h, s, cufftExecC2R(h->plan_b, (cufftComplex*)h->d_cgrid, (cufftReal*)h->d_grid));
+    else
+        FFTCALL(h, s, cufftExecZ2D(h->plan_b, (cufftDoubleComplex*)h->d_cgrid, (cufftDoubleReal*)h->d_grid));
+    FieldCombine cmb;
+    const double k = h->kappa;
+    cmb.U = h->d_p;
+    cmb.pol = h->d_pol;
+    cmb.self1 = -2.0 * DMFFB_DIELECTRIC * (k / 1.7724538509055159) * 2.0 * k * k / 3.0;
+    cmb.dot_out = sc + 2;
+    cmb.zero1 = sc + (1 - slot);
+    LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
+                                      h->n, stencil_cache<T>(h), g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, h->d_Ap,
+                                      cmb));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
@@ -771,8 +861,16 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     bool conv = false;
     double rms = 0.0, rms_b = 0.0;
     // one CG iteration; slot = parity of the r.z scalar it reads
+    const bool fused = h->lpme && h->have_plans && h->stencils_ready;
     auto iteration = [&](int slot) -> int {
         int st2;
+        if (fused) {
+            if ((st2 = cg_matvec_fused<T>(h, s, bx, sc, slot))) return st2;
+            if (h->s2 && !h->prof) CK(cudaStreamWaitEvent(s, h->e_join, 0));
+            LAUNCH(h, s, KC_VEC, k_cg_update<<<nb3, 256, 0, s>>>(n, sc, slot, U, h->d_r, h->d_z, h->d_p, h->d_Ap,
+                                                               h->d_pol, sc + (1 - slot), sc + 3, h->d_fmv));
+            return DMFFB_OK;
+        }
         // Ap = A p with p.Ap reduced into sc[2]; pAp, rr and the r.z slot this step writes are
         // cleared at the head of the pass (the previous step has read them by then)
         double* const zs[3] = {sc + 2, sc + 3, sc + (1 - slot)};
@@ -793,10 +891,16 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         if (!h->cg_exec || key != h->cg_key) {
             if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
             cudaGraph_t g;
+            const int64_t l0 = h->n_launch, f0 = h->n_fft;
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             int st0 = iteration(0);
             int st1 = st0 ? st0 : iteration(1);
             cudaError_t ce = cudaStreamEndCapture(s, &g);
+            // captured launches run on replay: count them there
+            h->cg_graph_launches = h->n_launch - l0;
+            h->cg_graph_ffts = h->n_fft - f0;
+            h->n_launch = l0;
+            h->n_fft = f0;
             if (st1) return st1;
             if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(ce));
             ce = cudaGraphInstantiate(&h->cg_exec, g, 0);
@@ -821,8 +925,8 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         for (int k = 0; k < check_every; k += 2) {
             if (graphs) {
                 CK(cudaGraphLaunch(h->cg_exec, s));
-                h->n_launch += 2 * 7;
-                h->n_fft += 4;
+                h->n_launch += h->cg_graph_launches;
+                h->n_fft += h->cg_graph_ffts;
             } else {
                 if ((st = iteration(0))) return st;
                 if ((st = iteration(1))) return st;
