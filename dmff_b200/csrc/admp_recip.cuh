@@ -719,8 +719,9 @@ struct FieldCombine {
     double* zero1 = nullptr;
 };
 
-// k_gather_field with the cached stencil; lanes take the spread's layout (five columns of six z
-// points per pass, eight passes), so every lane issues eight independent mesh loads
+// k_gather_field with the cached stencil: lanes own whole (x, y) columns (lanes 0..31, then
+// lanes 0..3) and read the column's six z points in sequence (one or two sectors, L1 hits after
+// the first), contracting them with the warp-uniform z weights.
 template <typename T>
 __global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache<T> st, MeshGeom g, const T* phi,
                                                              double scale, double* out, FieldCombine cmb) {
@@ -729,26 +730,38 @@ __global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache
     if (blockIdx.x == 0 && threadIdx.x == 0 && cmb.zero1) *cmb.zero1 = 0.0;
     const bool active = warp < n;
     const int at = active ? warp : 0;
-    const int grp = lane / 6, iz = lane - 6 * grp;
     T p1 = T(0), p2 = T(0), p3 = T(0);
-    if (active && grp < 5) {
+    if (active) {
         const int4 o = st.org[at];
         const T* w = st.w + 36 * (size_t)at;
         const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
-        const T mz0 = __ldg(w + 24 + iz), mz1 = __ldg(w + 30 + iz);
-        const int gz = wrap_up(o.z + iz, K2);
+        T mz0[6], mz1[6];
 #pragma unroll
-        for (int pass = 0; pass < 8; ++pass) {
-            const int col = grp + 5 * pass;
-            if (col < 36) {
-                const int ix = col / 6, iy = col - 6 * ix;
+        for (int t = 0; t < 6; ++t) {
+            mz0[t] = __ldg(w + 24 + t);
+            mz1[t] = __ldg(w + 30 + t);
+        }
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            const int L = lane + 32 * pass;
+            if (L < 36) {
+                const int ix = L / 6, iy = L - 6 * ix;
                 const int gx = wrap_up(o.x + ix, K0), gy = wrap_up(o.y + iy, K1);
-                const T v = __ldg(phi + ((size_t)gx * K1 + gy) * K2 + gz);
-                const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy), my1 = __ldg(w + 18 + iy);
-                const T t0 = mz0 * v;
-                p1 += mx1 * my0 * t0;
-                p2 += mx0 * my1 * t0;
-                p3 += mx0 * my0 * (mz1 * v);
+                const T* line = phi + ((size_t)gx * K1 + gy) * K2;
+                int gz = o.z;
+                T s0 = T(0), s1 = T(0);
+#pragma unroll
+                for (int t = 0; t < 6; ++t) {
+                    const T v = __ldg(line + gz);
+                    s0 += v * mz0[t];
+                    s1 += v * mz1[t];
+                    gz = (gz + 1 == K2) ? 0 : gz + 1;
+                }
+                const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy),
+                        my1 = __ldg(w + 18 + iy);
+                p1 += mx1 * my0 * s0;
+                p2 += mx0 * my1 * s0;
+                p3 += mx0 * my0 * s1;
             }
         }
     }
