@@ -246,7 +246,9 @@ def bench_serving(args, systems, dev):
     # plain path: FP64, one slot, graphs off, every 5th request back to back
     sub = systems[::5]
     plain = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp64", use_graphs=False, cg_tol=1e-6, device=dev)
-    plain.prewarm([ServingRequest(s) for s in warm[:1]])
+    # the same warm-up as the server: one request per mesh shape, so that neither timed run
+    # includes cuFFT plan creation
+    plain.prewarm([ServingRequest(s) for s in warm])
     preqs, pst = plain.run_stream(sub, np.zeros(len(sub)))
     plain.close()
     out["plain_fp64"] = dict(pst, sample="every 5th request of the stream, one at a time")
