@@ -164,6 +164,8 @@ struct dmffb_engine {
     int n_cap = 0;
     int64_t cov_cap = 0, grid_cap = 0, cgrid_cap = 0;
     int bmod_cap = 0;
+    uint32_t* d_nbmask = nullptr;  // candidate keep masks of the neighbour count pass
+    int64_t nbmask_cap = 0;
     std::map<std::array<int, 3>, std::pair<cufftHandle, cufftHandle>> plan_cache;  // mesh -> (R2C, C2R)
 };
 
@@ -1693,7 +1695,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub, h->d_stc_org, h->d_stc_w};
+                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2077,6 +2079,21 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.off_f = want_csr ? h->d_csr_off : nullptr;
     b.ent = nullptr;
     b.cap_f = 0;
+    if (fine) {
+        // keep masks for the fill pass: room for 1.5x the mean candidate count (125 cells of the
+        // stencil) per atom, at most 1 GiB; atoms with more candidates repeat the distance tests
+        const double mean_cand = 125.0 * (double)n / (double)ncell;
+        int64_t stride = (int64_t)ceil(1.5 * mean_cand / 32.0) + 2;
+        if ((int64_t)n * stride * 4 > ((int64_t)1 << 30)) stride = 0;
+        if (stride > 0 && (int64_t)n * stride > h->nbmask_cap) {
+            if (h->d_nbmask) cudaFree(h->d_nbmask);
+            h->d_nbmask = nullptr;
+            h->nbmask_cap = (int64_t)n * stride;
+            if ((st = dalloc(h, &h->d_nbmask, h->nbmask_cap * sizeof(uint32_t)))) return st;
+        }
+        b.mask = stride > 0 ? h->d_nbmask : nullptr;
+        b.mask_stride = (int)stride;
+    }
     if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));

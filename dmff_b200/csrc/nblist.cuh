@@ -241,6 +241,11 @@ struct Nb2Args {
     const int64_t* off_f;   // [n+1] pass 1
     int32_t* ent;           // [cap_f]
     int64_t cap_f;
+    // keep masks of the candidate batches (k_pairs_warp3): pass 0 stores one word per batch of 32
+    // candidates at mask[i * mask_stride + batch] when the atom's batches fit the stride; pass 1
+    // reads them instead of repeating the distance tests (null: no masks)
+    uint32_t* mask = nullptr;
+    int mask_stride = 0;
 };
 
 template <int PASS>
@@ -391,11 +396,22 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
     int cnt_h = 0, cnt_f = 0;
     const unsigned lt = (1u << lane) - 1u;
     int qc = 0;
+    // both passes see the same candidate list, so the masks are complete exactly when it fits
+    const bool use_mask = b.mask && (total + 31) / 32 <= b.mask_stride;
+    uint32_t* mrow = use_mask ? b.mask + (size_t)i * b.mask_stride : nullptr;
     for (int base = 0; base < total; base += 32) {
         const int t = base + lane;
         bool keep = false;
         int j = -1;
-        if (t < total) {
+        if (PASS == 1 && use_mask) {
+            const uint32_t mk = mrow[base >> 5];
+            if (mk == 0u) continue;  // warp-uniform: no candidate of this batch is kept
+            if ((mk >> lane) & 1u) {
+                while (t >= s_off[wl][qc + 1]) ++qc;
+                j = a.cell_atoms[s_beg[wl][qc] + (t - s_off[wl][qc])];
+                keep = true;
+            }
+        } else if (t < total) {
             while (t >= s_off[wl][qc + 1]) ++qc;
             j = a.cell_atoms[s_beg[wl][qc] + (t - s_off[wl][qc])];
             if (j != i) {
@@ -422,6 +438,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
         const bool up = keep && j > i;
         const unsigned mf = __ballot_sync(0xffffffffu, keep);
         const unsigned mh = __ballot_sync(0xffffffffu, up);
+        if (PASS == 0 && use_mask && lane == 0) mrow[base >> 5] = mf;
         if (PASS == 1) {
             if (keep) {
                 const int nbd = j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i);

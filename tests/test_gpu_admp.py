@@ -106,6 +106,33 @@ def test_internal_pairs_equal_given_pairs(c0_small):
     assert rel_force_rms(F.cpu().numpy(), ref["F"]) <= 1e-8
 
 
+@pytest.mark.parametrize("pol", [False, True])
+def test_internal_pairs_clustered_box(pol):
+    """Every molecule of one octant and about 1/8 of the others (4x the mean density in that
+    octant, liquid contacts everywhere): the dense octant's candidate lists exceed the neighbour
+    count pass's mask stride and the fill pass repeats the distance tests, while the rest use the
+    stored masks.  The engine-built list must give the oracle's pair count and the same FP64
+    energy and forces as the oracle's rows fed in."""
+    full = water_box(1000, 31.0, seed=21, lmax=2, pol=pol, rc=6.0)
+    mol = full["pos"].reshape(-1, 3, 3)
+    c = mol[:, 0, :] % 31.0
+    rng = np.random.default_rng(5)
+    keep = np.all(c < 15.5, axis=1) | (rng.random(len(mol)) < 0.125)
+    s = water_box(int(keep.sum()), 31.0, seed=21, lmax=2, pol=pol, rc=6.0)
+    s["pos"] = mol[keep].reshape(-1, 3).copy()
+    pr = oracle_pairs(s)
+    eng = make_engine(s, precision="fp64", cg_tol=1e-8)
+    p = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
+    eng.U.zero_()
+    res_i, F_i, _ = eng.compute(p, s["box"])  # engine-built cell list
+    E_i, F_i = res_i.energy, F_i.cpu().numpy().copy()
+    eng.U.zero_()
+    res_g, F_g, _ = eng.compute(p, s["box"], pairs=torch.tensor(pr, dtype=torch.int32, device="cuda"))
+    assert res_i.n_pairs == len(pr)
+    assert abs(E_i - res_g.energy) <= 1e-9 * abs(res_g.energy)
+    assert rel_force_rms(F_i, F_g.cpu().numpy()) <= 1e-8
+
+
 @pytest.mark.parametrize("xml,key,dec", [("admp.xml", "dimer_pol_lmax2_steppol5", 1),
                                          ("admp_mono.xml", "dimer_pol_lmax0_steppol5", 2),
                                          ("admp_nonpol.xml", "dimer_nonpol_lmax2", 2)])
