@@ -737,13 +737,15 @@ int build_csr(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npa
         if ((st = dalloc(h, &h->d_csr_ent, h->csr_cap * sizeof(int32_t)))) return st;
     }
     CK(cudaMemsetAsync(h->d_csr_deg, 0, n * sizeof(int32_t), s));
-    LAUNCH(h, s, KC_VEC, k_csr_count<<<nblk(npairs, 256), 256, 0, s>>>(npairs, pairs, n, h->d_csr_deg));
+    if (npairs > 0)
+        LAUNCH(h, s, KC_VEC, k_csr_count<<<nblk(npairs, 256), 256, 0, s>>>(npairs, pairs, n, h->d_csr_deg));
     CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
     size_t tb = h->cub2_bytes;
     LAUNCH(h, s, KC_VEC, cub::DeviceScan::InclusiveSum(h->d_cub2, tb, h->d_csr_deg, h->d_csr_off + 1, n, s));
     CK(cudaMemsetAsync(h->d_csr_deg, 0, n * sizeof(int32_t), s));
-    LAUNCH(h, s, KC_VEC, k_csr_fill<<<nblk(npairs, 256), 256, 0, s>>>(npairs, pairs, n, h->d_csr_off, h->d_csr_deg,
-                                                                      h->d_csr_ent));
+    if (npairs > 0)
+        LAUNCH(h, s, KC_VEC, k_csr_fill<<<nblk(npairs, 256), 256, 0, s>>>(npairs, pairs, n, h->d_csr_off, h->d_csr_deg,
+                                                                          h->d_csr_ent));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }

@@ -31,6 +31,23 @@ def _dev(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
+_EMPTY_ROWS = {}
+
+
+def _pairs_arg(pairs, device):
+    """(pointer, row count) for the C ABI.  None means "use the engine's own neighbour list"; an
+    explicitly empty list must still reach the engine as a non-null pointer with 0 rows (an empty
+    CUDA tensor's data pointer is null), so it points at a one-row scratch buffer."""
+    if pairs is None:
+        return None, 0
+    if pairs.shape[0] == 0:
+        key = str(device)
+        if key not in _EMPTY_ROWS:
+            _EMPTY_ROWS[key] = torch.zeros((1, 3), dtype=torch.int32, device=device)
+        return _dev(_EMPTY_ROWS[key]), 0
+    return _dev(pairs), pairs.shape[0]
+
+
 class AdmpEngine:
     """One ADMP multipolar PME system on one GPU.
 
@@ -155,7 +172,7 @@ class AdmpEngine:
         s = stream if stream is not None else torch.cuda.current_stream(self.device)
         st = self.lib.dmffb_admp_compute(
             self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p),
-            _dev(pairs), 0 if pairs is None else pairs.shape[0], _dev(U) if self.lpol else None, _dev(forces),
+            *_pairs_arg(pairs, self.device), _dev(U) if self.lpol else None, _dev(forces),
             ctypes.byref(res))
         self._check(st, allow=(L.DMFFB_NOT_CONVERGED,))
         return res, forces, U
@@ -181,8 +198,8 @@ class AdmpEngine:
         b = self._box(box)
         s = torch.cuda.current_stream(self.device)
         self._check(self.lib.dmffb_admp_field(
-            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p), _dev(pairs),
-            0 if pairs is None else pairs.shape[0], _dev(U), _dev(out)))
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p),
+            *_pairs_arg(pairs, self.device), _dev(U), _dev(out)))
         return out
 
     def set_param_grads(self, on=True):
@@ -317,8 +334,8 @@ class DispEngine:
         res = L.DispResult()
         s = torch.cuda.current_stream(self.device)
         self._check(self.lib.dmffb_disp_compute(
-            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p), _dev(pairs),
-            0 if pairs is None else pairs.shape[0], _dev(self.f_lr), _dev(self.f_sr), ctypes.byref(res)))
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p),
+            *_pairs_arg(pairs, self.device), _dev(self.f_lr), _dev(self.f_sr), ctypes.byref(res)))
         return res, (self.f_lr, self.f_sr)
 
     def set_param_grads(self, on=True):
@@ -436,8 +453,8 @@ class ClassicalEngine:
         res = L.ClassicalResult()
         s = torch.cuda.current_stream(self.device)
         self._check(self.lib.dmffb_classical_compute(
-            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p), _dev(pairs),
-            0 if pairs is None else pairs.shape[0], _dev(self.forces), ctypes.byref(res)))
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p),
+            *_pairs_arg(pairs, self.device), _dev(self.forces), ctypes.byref(res)))
         return res, self.forces
 
     def param_grads(self):
