@@ -104,7 +104,8 @@ int dmffb_admp_set_params(dmffb_engine* h, const double* Q_local, const double* 
  * may be NULL when lpol == 0), forces_out [n*3] (= -dE/dpos, may be NULL).  pairs is a
  * device array of npairs rows (i, j, nbond) with the reference's padding semantics (rows with
  * i >= j are skipped, utils.py:67-85); pairs == NULL uses the engine's own neighbour list
- * (built on the first call and by dmffb_admp_build_neighbors).  box [9] is a host array.
+ * (built on the first call and by dmffb_admp_build_neighbors), while a non-NULL pairs with
+ * npairs == 0 is an empty list (no real-space pairs).  box [9] is a host array.
  * stream: a cudaStream_t (NULL = legacy default stream). */
 int dmffb_admp_compute(dmffb_engine* h, void* stream, const double* pos, const double* box,
                        const int32_t* pairs, int64_t npairs, double* U_inout, double* forces_out,
