@@ -2096,7 +2096,14 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
         b.mask = stride > 0 ? h->d_nbmask : nullptr;
         b.mask_stride = (int)stride;
     }
-    if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
+    // small neighbourhoods (staging room for 1.5x the mean candidate count within 44 KB): one CTA
+    // per cell with the candidates staged in shared memory; larger ones keep the warp-per-atom
+    // kernel, whose L2 gathers run at full occupancy (measured faster there than 100 KB stages)
+    const int chmax = (int)(1.5 * 125.0 * (double)n / (double)ncell + 64.0);
+    const size_t stage_bytes = (size_t)chmax * sizeof(float4);
+    const bool staged = stage_bytes <= kNbStageBytes;
+    if (fine && !staged) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
+    else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<0, 2, kNbWarps><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
     tb = h->cub_bytes;
@@ -2124,7 +2131,8 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.a.cap = h->pair_cap;
     b.ent = want_csr ? h->d_csr_ent : nullptr;
     b.cap_f = want_csr ? h->csr_cap : 0;
-    if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<1, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
+    if (fine && !staged) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<1, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
+    else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<1, 2, kNbWarps><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));

@@ -345,6 +345,8 @@ __global__ void __launch_bounds__(256) k_pairs_warp2(Nb2Args b) {
 // full 32-lane batches; each lane finds its candidate's cell by advancing a cursor (lanes move
 // forward monotonically).  Rows come out grouped by i like the coarse scan's.
 constexpr int kNbWarps = 8;  // warps per block of k_pairs_warp3
+constexpr size_t kNbStageBytes = 44u << 10;  // largest candidate stage of k_pairs_cell: with its static
+                                              // shared arrays it stays under the 48 KB default
 
 template <int PASS, int S>
 __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
@@ -465,6 +467,163 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
     if (PASS == 0 && lane == 0) {
         a.count[i] = cnt_h;
         if (b.count_f) b.count_f[i] = cnt_f;
+    }
+}
+
+// Block-per-cell form of k_pairs_warp3 (same stencil, candidate order, tests and outputs): one
+// CTA takes every atom of one cell.  The cell's (2S + 1)^3 neighbourhood is laid out once per CTA
+// and, when it fits in `chmax` entries, staged in shared memory as (x, y, z, j) float4s, so the
+// cell's atoms read their candidates from shared memory instead of each gathering them from L2;
+// neighbourhoods larger than the stage fall back to the global gathers.  The NW warps of the CTA
+// take the cell's atoms in turn.
+template <int PASS, int S, int NW>
+__global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
+    constexpr int W = 2 * S + 1, NQ = W * W * W;
+    __shared__ int s_beg[NQ];
+    __shared__ int s_off[NQ + 1];
+    extern __shared__ __align__(16) float4 s_cand[];
+    const NbArgs& a = b.a;
+    const int c = blockIdx.x;
+    const int cs0 = a.cell_start[c], m = a.cell_start[c + 1] - cs0;
+    if (m == 0) return;  // whole CTA
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c3[3] = {c / (a.nc[2] * a.nc[1]), (c / a.nc[2]) % a.nc[1], c % a.nc[2]};
+    if (wl == 0) {
+        int carry = 0;
+        if (lane == 0) s_off[0] = 0;
+        for (int q0 = 0; q0 < NQ; q0 += 32) {
+            const int q = q0 + lane;
+            int cnt = 0;
+            if (q < NQ) {
+                const int dx = q / (W * W) - S, dy = (q / W) % W - S, dz = q % W - S;
+                const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
+                const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
+                const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
+                const int cc = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+                const int cs = a.cell_start[cc];
+                cnt = a.cell_start[cc + 1] - cs;
+                s_beg[q] = cs;
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (q < NQ) s_off[q + 1] = carry + incl;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+    __syncthreads();
+    const int total = s_off[NQ];
+    const bool staged = total <= chmax;
+    if (staged) {
+        int qc = 0;
+        for (int t = threadIdx.x; t < total; t += blockDim.x) {
+            while (t >= s_off[qc + 1]) ++qc;
+            const int j = a.cell_atoms[s_beg[qc] + (t - s_off[qc])];
+            s_cand[t] = make_float4(b.posf[4 * j], b.posf[4 * j + 1], b.posf[4 * j + 2], __int_as_float(j));
+        }
+    }
+    __syncthreads();
+    float hf[9], hif[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { hf[k] = (float)a.box.h[k]; hif[k] = (float)a.box.hinv[k]; }
+    const float rlo = (float)(a.rc - 2e-3), rhi = (float)(a.rc + 2e-3);
+    const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int ai = wl; ai < m; ai += NW) {
+        const int i = a.cell_atoms[cs0 + ai];
+        const double* pi = a.pos + 3 * i;
+        const float pix = b.posf[4 * i], piy = b.posf[4 * i + 1], piz = b.posf[4 * i + 2];
+        int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1 && b.off_f) ? b.off_f[i] : 0;
+        int cnt_h = 0, cnt_f = 0;
+        int qc = 0;
+        const bool use_mask = b.mask && (total + 31) / 32 <= b.mask_stride;
+        uint32_t* mrow = use_mask ? b.mask + (size_t)i * b.mask_stride : nullptr;
+        for (int base = 0; base < total; base += 32) {
+            const int t = base + lane;
+            bool keep = false;
+            int j = -1;
+            if (PASS == 1 && use_mask) {
+                const uint32_t mk = mrow[base >> 5];
+                if (mk == 0u) continue;  // warp-uniform: no candidate of this batch is kept
+                if ((mk >> lane) & 1u) {
+                    if (staged) {
+                        j = __float_as_int(s_cand[t].w);
+                    } else {
+                        while (t >= s_off[qc + 1]) ++qc;
+                        j = a.cell_atoms[s_beg[qc] + (t - s_off[qc])];
+                    }
+                    keep = true;
+                }
+            } else if (t < total) {
+                float pjx, pjy, pjz;
+                if (staged) {
+                    const float4 cv = s_cand[t];
+                    pjx = cv.x;
+                    pjy = cv.y;
+                    pjz = cv.z;
+                    j = __float_as_int(cv.w);
+                } else {
+                    while (t >= s_off[qc + 1]) ++qc;
+                    j = a.cell_atoms[s_beg[qc] + (t - s_off[qc])];
+                    pjx = b.posf[4 * j];
+                    pjy = b.posf[4 * j + 1];
+                    pjz = b.posf[4 * j + 2];
+                }
+                if (j != i) {
+                    const float d0 = pjx - pix, d1 = pjy - piy, d2 = pjz - piz;
+                    bool amb = false;
+                    float sf[3];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        float tt = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
+                        float nn = floorf(tt + 0.5f);
+                        sf[q] = tt - nn;
+                        amb |= fabsf(sf[q]) > 0.4999f;
+                    }
+                    const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
+                    const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
+                    const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
+                    const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
+                    if (!amb && r2 < rlo2) keep = true;
+                    else if (!amb && r2 > rhi2) keep = false;
+                    else keep = j > i ? within_rc(a.box, pi, a.pos + 3 * j, a.rc)
+                                      : within_rc(a.box, a.pos + 3 * j, pi, a.rc);
+                }
+            }
+            const bool up = keep && j > i;
+            const unsigned mf = __ballot_sync(0xffffffffu, keep);
+            const unsigned mh = __ballot_sync(0xffffffffu, up);
+            if (PASS == 0 && use_mask && lane == 0) mrow[base >> 5] = mf;
+            if (PASS == 1) {
+                if (keep) {
+                    const int nbd = j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i);
+                    int sidx = nbd - 1;
+                    if (sidx < 0) sidx += 6;
+                    const int64_t sf_ = out_f + __popc(mf & lt);
+                    if (b.ent && sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
+                    if (up) {
+                        const int64_t sh = out_h + __popc(mh & lt);
+                        if (sh < a.cap) {
+                            a.pairs[3 * sh] = i;
+                            a.pairs[3 * sh + 1] = j;
+                            a.pairs[3 * sh + 2] = nbd;
+                        }
+                    }
+                }
+                out_f += __popc(mf);
+                out_h += __popc(mh);
+            } else {
+                cnt_f += __popc(mf);
+                cnt_h += __popc(mh);
+            }
+        }
+        if (PASS == 0 && lane == 0) {
+            a.count[i] = cnt_h;
+            if (b.count_f) b.count_f[i] = cnt_f;
+        }
     }
 }
 
