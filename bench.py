@@ -253,6 +253,16 @@ def bench_serving(args, systems, dev):
     plain.close()
     out["plain_fp64"] = dict(pst, sample="every 5th request of the stream, one at a time")
     out["speedup_vs_plain"] = out["offline_fp32"]["atom_evals_per_s"] / pst["atom_evals_per_s"]
+    # the same plain path with the reference's own dipole iteration (fixed-point steps, POL_CONV 1.0,
+    # MAX_N_POL 30, pme.py:342-423) in place of CG: the reference's algorithm run on this GPU
+    plain_r = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp64", use_graphs=False, solver="reference",
+                         cg_tol=1.0, max_iter=30, device=dev)
+    plain_r.prewarm([ServingRequest(s) for s in warm])
+    _, rst = plain_r.run_stream(sub, np.zeros(len(sub)))
+    plain_r.close()
+    out["plain_fp64_reference_solver"] = dict(rst, sample="every 5th request of the stream, one at a time",
+                                              solver="fixed-point dipole iteration, POL_CONV 1.0, MAX_N_POL 30")
+    out["speedup_vs_plain_reference_solver"] = out["offline_fp32"]["atom_evals_per_s"] / rst["atom_evals_per_s"]
     errs_e, errs_f = [], []
     for k, p in enumerate(preqs):
         q = fp32[5 * k]

@@ -118,6 +118,7 @@ struct dmffb_engine {
     // ---- CG iteration graph (two iterations per launch) and the side stream of the matvec
     cudaStream_t s1 = nullptr, s2 = nullptr;  // engine work stream (capturable) and matvec side stream
     cudaEvent_t e_fork = nullptr, e_join = nullptr, e_in = nullptr, e_out = nullptr;
+    cudaEvent_t e_build = nullptr;  // end of the last neighbour build on its stream (no host wait)
     cudaGraphExec_t cg_exec = nullptr;
     std::vector<double> cg_key;
     bool use_graphs = true;
@@ -963,6 +964,7 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     if (!pairs) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
     }
@@ -1238,6 +1240,7 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
     if (!pairs) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
     }
@@ -1341,6 +1344,7 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
     if (nonbonded && !pairs) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
     }
@@ -1714,6 +1718,7 @@ void dmffb_destroy(dmffb_engine* h) {
     if (h->e_in) cudaEventDestroy(h->e_in);
     if (h->e_out) cudaEventDestroy(h->e_out);
     if (h->e_fork) cudaEventDestroy(h->e_fork);
+    if (h->e_build) cudaEventDestroy(h->e_build);
     if (h->e_join) cudaEventDestroy(h->e_join);
     delete h;
 }
@@ -1812,6 +1817,7 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
             int st = dmffb_admp_build_neighbors(h, stream, pos, box);
             if (st) return st;
         }
+        if (h->e_build) CK(cudaStreamWaitEvent((cudaStream_t)stream, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
     }
@@ -2135,8 +2141,14 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<1, 2, kNbWarps><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(s));
-    prof_collect(h);
+    // no host wait for the fill pass: later work on this stream is ordered after it, and compute
+    // calls on other streams wait for e_build before they read the engine's list
+    if (h->prof) {
+        CK(cudaStreamSynchronize(s));
+        prof_collect(h);
+    }
+    if (!h->e_build) CK(cudaEventCreateWithFlags(&h->e_build, cudaEventDisableTiming));
+    CK(cudaEventRecord(h->e_build, s));
     h->npairs = tot[0];
     h->have_pairs = true;
     h->pairs_gen++;
