@@ -34,7 +34,7 @@ EXPORTED = [
     "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads", "dmffb_disp_set_param_grads",
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
-    "dmffb_set_graphs", "dmffb_admp_set_param_grads", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
+    "dmffb_set_graphs", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
     "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy",
 ]
 
@@ -229,6 +229,7 @@ def load():
     lib.dmffb_admp_field.argtypes = [vp, vp, vp, vp, vp, i64, vp, vp]
     lib.dmffb_admp_multipole_grads.argtypes = [vp, vp, vp, vp]
     lib.dmffb_admp_set_param_grads.argtypes = [vp, i32]
+    lib.dmffb_admp_set_zero_guess.argtypes = [vp, i32]
     lib.dmffb_admp_param_grads.argtypes = [vp, vp, vp, vp, vp, vp]
     lib.dmffb_build_neighbors.argtypes = [vp, vp, vp, vp, dbl, vp, i64, P(i64)]
     lib.dmffb_admp_build_neighbors.argtypes = [vp, vp, vp, vp]

@@ -143,6 +143,8 @@ struct dmffb_engine {
     double* d_tprm[3] = {nullptr, nullptr, nullptr};
     double* d_tdprm[3] = {nullptr, nullptr, nullptr};
     bool want_pgrad = false, charges_set = false;
+    bool zero_guess = false;  // dipole solves start from U = 0 (dmffb_admp_set_zero_guess)
+    bool u_zeroed = false;    // this call's U was zeroed by the host-buffer entry point
     // ---- ADMP parameter adjoints (dmffb_admp_set_param_grads)
     bool admp_pgrad = false, have_pgrad = false;
     double *d_dQloc = nullptr, *d_dpa = nullptr, *d_dth = nullptr, *d_dpol = nullptr;
@@ -857,8 +859,12 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         if ((st = stencil_prep<T>(h, s, pos, bx))) return st;
     }
     if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b))) return st;
-    if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
-    LAUNCH(h, s, KC_VEC, k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, h->d_Ap, h->d_pol, h->d_r, h->d_z, h->d_p));
+    // from U = 0 the residual is -b: no A U pass
+    const bool u0 = h->zero_guess || h->u_zeroed;
+    if (h->zero_guess) CK(cudaMemsetAsync(U, 0, (size_t)3 * n * sizeof(double), s));
+    if (!u0 && (st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
+    LAUNCH(h, s, KC_VEC, k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, u0 ? nullptr : h->d_Ap, h->d_pol, h->d_r, h->d_z,
+                                                     h->d_p));
     CK(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
     LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_r, h->d_z, h->d_r, h->d_r, sc + 0, sc + 3));
     LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_b, h->d_b, nullptr, nullptr, sc + 4, nullptr));
@@ -1788,14 +1794,18 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
         CK(cudaMemcpyAsync(dp, pairs, npairs * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     }
     if (h->lpol) {
-        if (U_inout) CK(cudaMemcpyAsync(h->d_U, U_inout, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+        // with a zero initial guess the input dipoles are not read: no copy in
+        if (U_inout && !h->zero_guess)
+            CK(cudaMemcpyAsync(h->d_U, U_inout, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
         else CK(cudaMemsetAsync(h->d_U, 0, 3 * n * sizeof(double), s));
     }
     if (!pairs) {  // host callers hold no device pair list: rebuild for these positions
         int sb = dmffb_admp_build_neighbors(h, (void*)s, h->d_pos, box);
         if (sb) return sb;
     }
+    h->u_zeroed = h->lpol && !U_inout;  // this call starts from U = 0
     int st = dmffb_admp_compute(h, s, h->d_pos, box, dp, npairs, h->lpol ? h->d_U : nullptr, h->d_forces, result);
+    h->u_zeroed = false;
     if (dp) h->have_pairs = false;  // the staged rows are not the engine's own neighbour list
     if (st != DMFFB_OK && st != DMFFB_NOT_CONVERGED) return st;
     if (forces_out) CK(cudaMemcpyAsync(forces_out, h->d_forces, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1845,6 +1855,12 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
     };
     if (h->prec == DMFFB_FP32) return run(float(0));
     return run(double(0));
+}
+
+int dmffb_admp_set_zero_guess(dmffb_engine* h, int32_t enabled) {
+    if (!h || h->kind != 0) return fail(h, DMFFB_BAD_ARG, "ADMP engine required");
+    h->zero_guess = enabled != 0;
+    return DMFFB_OK;
 }
 
 int dmffb_admp_set_param_grads(dmffb_engine* h, int32_t enabled) {

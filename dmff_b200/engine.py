@@ -206,6 +206,11 @@ class AdmpEngine:
         """Parameter adjoints (dE/dQ, dE/dpol, dE/dthole) on/off for the following computes."""
         self._check(self.lib.dmffb_admp_set_param_grads(self.h, int(bool(on))))
 
+    def set_zero_guess(self, on=True):
+        """Dipole solves of the following computes start from U = 0 (the U buffer's content is
+        ignored on input and receives the solution); the CG set-up then skips its A U pass."""
+        self._check(self.lib.dmffb_admp_set_zero_guess(self.h, int(bool(on))))
+
     def param_grads(self):
         """{'Q_global', 'Q_local': [n, 9], 'pol', 'thole': [n]} of the last compute."""
         dev = self.device

@@ -127,6 +127,11 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
  * Thole width: the quantities jax.grad gives for params["ADMPPmeForce"] in the reference
  * (dmff/admp/pme.py:186-232 under jax.value_and_grad), before the per-type scatter. */
 int dmffb_admp_set_param_grads(dmffb_engine* h, int32_t enabled);
+/* Zero initial guess on/off for the following computes of a polarizable engine.  When on, the
+ * dipole solve starts from U = 0 whatever U_inout holds (the solution is still written to it) and
+ * skips the A U evaluation of the CG set-up.  dmffb_admp_compute_host with U_inout == NULL starts
+ * from zero in the same way.  The reference's get_energy with U_init = None starts from zeros. */
+int dmffb_admp_set_zero_guess(dmffb_engine* h, int32_t enabled);
 /* Per-atom parameter adjoints of the last compute (device arrays, each may be NULL):
  * dE/dQ_global [n*9] and dE/dQ_local [n*9] (harmonic), dE/dpol [n] (A^-3 kJ/mol),
  * dE/dthole [n]. */

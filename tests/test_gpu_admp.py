@@ -60,6 +60,27 @@ def test_pol_energy_forces_dipoles(pol_small, prec):
     assert np.abs(bg - ref["box_grad"]).max() <= t["b"] * np.abs(ref["box_grad"]).max()
 
 
+def test_zero_guess_matches_explicit_zero(pol_small):
+    """dmffb_admp_set_zero_guess: the U buffer's content is ignored and the CG set-up skips its
+    A U pass; results equal a solve from an explicitly zeroed U and the oracle."""
+    s, pr, ref = pol_small
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
+    prt = torch.tensor(pr, dtype=torch.int32, device="cuda")
+    e1 = make_engine(s, precision="fp64", cg_tol=1e-8)
+    e1.U.zero_()
+    r1, F1, _ = e1.compute(pos, s["box"], pairs=prt)
+    F1 = F1.cpu().numpy().copy()
+    e2 = make_engine(s, precision="fp64", cg_tol=1e-8)
+    e2.set_zero_guess(True)
+    e2.U.fill_(123.0)  # ignored on input
+    r2, F2, U2 = e2.compute(pos, s["box"], pairs=prt)
+    assert r2.n_iter == r1.n_iter
+    assert abs(r2.energy - r1.energy) <= 1e-12 * abs(r1.energy)
+    assert rel_force_rms(F2.cpu().numpy(), F1) <= 1e-12
+    assert abs(r2.energy - ref["E"]) <= 1e-9 * abs(ref["E"])
+    assert bool(torch.isfinite(U2).all())
+
+
 def test_reference_solver_matches_fixed_step_oracle():
     s = water_box(27, 9.3, seed=12, lmax=2, pol=True, rc=4.5)
     pr = oracle_pairs(s)
