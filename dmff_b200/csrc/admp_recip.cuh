@@ -473,9 +473,10 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs<T> a) {
                 if (a.lmax < 2) { for (int k = 4; k < 9; ++k) qp[k] = T(0); }
                 if (a.lmax < 1) { qp[1] = qp[2] = qp[3] = T(0); }
                 torque9(qp, gT, t);
-                a.torque[3 * at] += t[0];
-                a.torque[3 * at + 1] += t[1];
-                a.torque[3 * at + 2] += t[2];
+                // atomics: the real-space FULL pass may add to the same torques concurrently
+                atomicAdd(a.torque + 3 * at, t[0]);
+                atomicAdd(a.torque + 3 * at + 1, t[1]);
+                atomicAdd(a.torque + 3 * at + 2, t[2]);
             }
             if (a.want_box) {
                 // X_NA = Y (x) R + (dE/dB)^T,  dE/dB = -Pu (x) mu + 2 P2 B Theta

@@ -765,36 +765,38 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
         for (int k = 0; k < 3; ++k)
             if (zero_scal[k]) CK(cudaMemsetAsync(zero_scal[k], 0, sizeof(double), s));
     if (include_perm) CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
+    // the real-space work (permanent pair field, matvec) runs on a side stream, overlapping the
+    // reciprocal pass; both write their own arrays and meet in the combine
+    const bool real_work = (include_perm && npairs > 0) || U;
+    const bool fork = real_work && h->s2 && !h->prof;
+    cudaStream_t sr = s;
+    if (fork) {
+        CK(cudaEventRecord(h->e_fork, s));
+        CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
+        sr = h->s2;
+    }
     if (include_perm && npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
         if (sizeof(T) == 4) {
-            LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_UNSCALED><<<nblk(npairs, 128), 128, 0, s>>>(a));
+            LAUNCH(h, sr, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_UNSCALED><<<nblk(npairs, 128), 128, 0, sr>>>(a));
             a.rowmap = h->d_srows;
             a.nrowmap = h->n_srows;
             if (h->n_srows > 0)
-                LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(h->n_srows, 128), 128, 0, s>>>(a));
+                LAUNCH(h, sr, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(h->n_srows, 128), 128, 0, sr>>>(a));
         } else {
-            LAUNCH(h, s, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, s>>>(a));
+            LAUNCH(h, sr, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, sr>>>(a));
         }
     }
-    // the real-space matvec runs on a side stream, overlapping the reciprocal pass
-    const bool fork = U && h->s2 && !h->prof;
     if (U) {
-        PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, U);
         CsrArgs c;
         c.n = h->n;
         c.off = h->d_csr_off;
         c.ent = h->d_csr_ent;
-        cudaStream_t sm = s;
-        if (fork) {
-            CK(cudaEventRecord(h->e_fork, s));
-            CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
-            sm = h->s2;
-        }
+        cudaStream_t sm = sr;
         LAUNCH(h, sm, KC_PAIR_MATVEC, k_matvec_apply<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, sm>>>(
                                           c, (const MvCoef<T>*)h->d_mvcoef, (const T*)h->d_posT, boxT<T>(bx), U, h->d_fmv));
-        if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
+    if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     const double* recip = nullptr;
     if (recip_on) {
         int st = recip_pass<T>(h, s, pos, bx, include_perm, U, GATHER_FIELD, h->d_fr, 0, zero_scal);
@@ -1003,32 +1005,43 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
         res->converged = 1;
     }
     if (h->timing) CK(cudaEventRecord(h->ev[2], s));
+    // the real-space FULL pass runs on the side stream beside the reciprocal FULL pass (both add
+    // torques with atomics; the gradients, energies and virials they write are separate)
+    const bool fork_full = npairs > 0 && h->lpme && h->have_plans && h->s2 && !h->prof && !h->timing;
+    cudaStream_t sp = s;
+    if (fork_full) {
+        CK(cudaEventRecord(h->e_fork, s));
+        CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
+        sp = h->s2;
+    }
     if (npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, h->lpol ? U : nullptr);
         const unsigned nbk = nblk(npairs, 128);
         if (sizeof(T) == 4) {
             const unsigned nbs = nblk(h->n_srows, 128);
             if (h->lpol) {
-                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(a));
+                LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, sp>>>(a));
                 a.rowmap = h->d_srows;
                 a.nrowmap = h->n_srows;
-                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, s>>>(a));
+                if (nbs) LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, sp>>>(a));
             } else {
-                LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(a));
+                LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, sp>>>(a));
                 a.rowmap = h->d_srows;
                 a.nrowmap = h->n_srows;
-                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, s>>>(a));
+                if (nbs) LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, sp>>>(a));
             }
         } else {
-            if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nbk, 128, 0, s>>>(a));
-            else LAUNCH(h, s, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL><<<nbk, 128, 0, s>>>(a));
+            if (h->lpol) LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nbk, 128, 0, sp>>>(a));
+            else LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL><<<nbk, 128, 0, sp>>>(a));
         }
         CK(cudaGetLastError());
     }
+    if (fork_full) CK(cudaEventRecord(h->e_join, h->s2));
     if (h->timing) CK(cudaEventRecord(h->ev[3], s));
     if (h->lpme && h->have_plans) {
         if ((st = recip_pass<T>(h, s, pos, bx, true, h->lpol ? U : nullptr, GATHER_FULL, nullptr, 0))) return st;
     }
+    if (fork_full) CK(cudaStreamWaitEvent(s, h->e_join, 0));
     if (h->timing) CK(cudaEventRecord(h->ev[4], s));
     SelfArgs<T> sa;
     sa.f = pa.f;
