@@ -700,13 +700,19 @@ int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, 
 
 // pair tensors of every CSR entry for the solve at these positions
 template <typename T>
-int matvec_setup(dmffb_engine* h, cudaStream_t s, const Box& bx, const int32_t* pairs, int64_t npairs) {
+int matvec_alloc(dmffb_engine* h) {
     int st;
     if (h->csr_cap > h->mv_cap) {
         if (h->d_mvcoef) cudaFree(h->d_mvcoef);
         h->mv_cap = h->csr_cap;
         if ((st = dalloc(h, &h->d_mvcoef, h->mv_cap * sizeof(MvCoef<T>)))) return st;
     }
+    return DMFFB_OK;
+}
+
+// pair tensors of every CSR entry (the buffer is sized by matvec_alloc)
+template <typename T>
+int matvec_coef_launch(dmffb_engine* h, cudaStream_t s, const Box& bx, const int32_t* pairs, int64_t npairs) {
     PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
     CsrArgs c;
     c.n = h->n;
@@ -759,7 +765,7 @@ int build_csr(dmffb_engine* h, cudaStream_t s, const int32_t* pairs, int64_t npa
 template <typename T>
 int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
                int64_t npairs, const double* U, bool include_perm, double* out, const double* dotv = nullptr,
-               double* dot_out = nullptr, double* const* zero_scal = nullptr) {
+               double* dot_out = nullptr, double* const* zero_scal = nullptr, bool with_mvcoef = false) {
     const bool recip_on = h->lpme && h->have_plans;
     if (zero_scal && !recip_on)
         for (int k = 0; k < 3; ++k)
@@ -767,13 +773,18 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     if (include_perm) CK(cudaMemsetAsync(h->d_fieldT, 0, (size_t)3 * h->n * sizeof(T), s));
     // the real-space work (permanent pair field, matvec) runs on a side stream, overlapping the
     // reciprocal pass; both write their own arrays and meet in the combine
-    const bool real_work = (include_perm && npairs > 0) || U;
+    const bool real_work = (include_perm && npairs > 0) || U || with_mvcoef;
     const bool fork = real_work && h->s2 && !h->prof;
     cudaStream_t sr = s;
     if (fork) {
         CK(cudaEventRecord(h->e_fork, s));
         CK(cudaStreamWaitEvent(h->s2, h->e_fork, 0));
         sr = h->s2;
+    }
+    // the CG matvec's pair tensors, needed only after this pass: also beside the reciprocal pass
+    if (with_mvcoef) {
+        int stc = matvec_coef_launch<T>(h, sr, bx, pairs, npairs);
+        if (stc) return stc;
     }
     if (include_perm && npairs > 0) {
         PairArgs<T> a = pair_args<T>(h, bx, pairs, npairs, nullptr);
@@ -821,8 +832,9 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     double* sc = h->d_scal + S_CG;
     int st;
     if ((st = build_csr(h, s, pairs, npairs))) return st;
-    if ((st = matvec_setup<T>(h, s, bx, pairs, npairs))) return st;
+    if ((st = matvec_alloc<T>(h))) return st;
     if (h->solver == DMFFB_SOLVER_REFERENCE) {
+        if ((st = matvec_coef_launch<T>(h, s, bx, pairs, npairs))) return st;
         int it = 0;
         bool conv = false;
         const int maxit = h->steps_pol > 0 ? h->steps_pol : h->max_iter;
@@ -860,7 +872,8 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         CK(cudaMemsetAsync(h->d_grid2, 0, (size_t)h->K[0] * h->K[1] * h->K[2] * sizeof(T), s));
         if ((st = stencil_prep<T>(h, s, pos, bx))) return st;
     }
-    if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b))) return st;
+    if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b, nullptr, nullptr, nullptr, true)))
+        return st;
     // from U = 0 the residual is -b: no A U pass
     const bool u0 = h->zero_guess || h->u_zeroed;
     if (h->zero_guess) CK(cudaMemsetAsync(U, 0, (size_t)3 * n * sizeof(double), s));
@@ -1861,7 +1874,10 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
         LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
         int st;
         if (sizeof(T) == 4 && npairs > 0 && (st = scaled_rows(h, s, pairs, npairs))) return st;
-        st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out);
+        // the matvec of U needs this call's CSR and pair tensors (not a previous compute's)
+        if ((st = build_csr(h, s, pairs, npairs))) return st;
+        if ((st = matvec_alloc<T>(h))) return st;
+        st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out, nullptr, nullptr, nullptr, true);
         if (st) return st;
         CK(cudaStreamSynchronize(s));
         return DMFFB_OK;

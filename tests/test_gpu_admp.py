@@ -60,6 +60,30 @@ def test_pol_energy_forces_dipoles(pol_small, prec):
     assert np.abs(bg - ref["box_grad"]).max() <= t["b"] * np.abs(ref["box_grad"]).max()
 
 
+def test_field_entry_point_matches_oracle_grad_U(pol_small):
+    """dmffb_admp_field (dE/dU at a given U, the reference's grad_U_fn, pme.py:181) at positions
+    other than the engine's last compute: it builds its own CSR and pair tensors."""
+    import oracle.admp_ref as R
+    s, pr, _ = pol_small
+    eng = make_engine(s, precision="fp64", cg_tol=1e-8)
+    pos_a = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
+    eng.U.zero_()
+    eng.compute(pos_a, s["box"], pairs=torch.tensor(pr, dtype=torch.int32, device="cuda"))
+    rng = np.random.default_rng(9)
+    sb = dict(s, pos=s["pos"] + rng.normal(0.0, 0.05, size=s["pos"].shape))
+    prb = oracle_pairs(sb)
+    U = rng.normal(0.0, 0.02, size=(s["n_atoms"], 3))
+    got = eng.field(torch.tensor(sb["pos"], dtype=torch.float64, device="cuda"), sb["box"],
+                    torch.tensor(prb, dtype=torch.int32, device="cuda"),
+                    torch.tensor(U, dtype=torch.float64, device="cuda")).cpu().numpy()
+    f = R.ADMPPmeForce(sb["box"], sb["axis_types"], sb["axis_indices"], sb["rc"], sb["ethresh"], sb["lmax"],
+                       sb["lpol"], kappa=sb["kappa"], K=sb["K"])
+    want = f.grad_U(torch.tensor(sb["pos"]), torch.tensor(sb["box"]), prb, torch.tensor(sb["Q_local"]),
+                    torch.tensor(U), torch.tensor(sb["pol"]), torch.tensor(sb["thole"]), torch.tensor(sb["mscales"]),
+                    torch.tensor(sb["pscales"]), torch.tensor(sb["dscales"])).numpy()
+    assert rel_force_rms(got, want) <= 1e-9
+
+
 def test_zero_guess_matches_explicit_zero(pol_small):
     """dmffb_admp_set_zero_guess: the U buffer's content is ignored and the CG set-up skips its
     A U pass; results equal a solve from an explicitly zeroed U and the oracle."""
