@@ -552,43 +552,6 @@ __device__ __forceinline__ T sel6(const T v[6], int k) {
     return r;
 }
 
-// Lane layout of the lean dipole spread / field gather: a warp per atom, lanes 0..29 form five
-// groups of six consecutive z points of one (x, y) stencil column; the 36 columns take eight
-// passes.  A warp's atomics / loads of one pass then touch five runs of six consecutive floats
-// (coalesced in L2) instead of 32 scattered addresses.
-template <typename T>
-__global__ void __launch_bounds__(256) k_spread_dip(SpreadArgs<T> a) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
-    if (warp >= a.n) return;
-    const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
-    int m0[3];
-    T Mx[2][6], My[2][6], Mz[2][6];
-    stencil01<T>(a.g, a.pos, at, m0, Mx, My, Mz);
-    const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
-    const double* B = a.g.B;
-    const T c1 = -(T(B[0]) * mu0 + T(B[1]) * mu1 + T(B[2]) * mu2);
-    const T c2 = -(T(B[3]) * mu0 + T(B[4]) * mu1 + T(B[5]) * mu2);
-    const T c3 = -(T(B[6]) * mu0 + T(B[7]) * mu1 + T(B[8]) * mu2);
-    const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
-    const int grp = lane / 6, iz = lane - 6 * grp;
-    if (grp >= 5) return;
-    const T mz0 = sel6(Mz[0], iz), mz1 = sel6(Mz[1], iz);
-    const int gz = wrapi(m0[2] - 3 + iz, K2);
-#pragma unroll
-    for (int pass = 0; pass < 8; ++pass) {
-        const int col = grp + 5 * pass;
-        if (col < 36) {
-            const int ix = col / 6, iy = col - 6 * ix;
-            const T mx0 = sel6(Mx[0], ix), mx1 = sel6(Mx[1], ix), my0 = sel6(My[0], iy), my1 = sel6(My[1], iy);
-            const T v = (c1 * mx1 * my0 + c2 * mx0 * my1) * mz0 + c3 * mx0 * my0 * mz1;
-            const int gx = wrapi(m0[0] - 3 + ix, K0), gy = wrapi(m0[1] - 3 + iy, K1);
-            atomicAdd(a.grid + ((size_t)gx * K1 + gy) * K2 + gz, v);
-        }
-    }
-}
-
 // dE/dmu (Cartesian) of every site from the convolved mesh: out = scale * (-B^T grad_u phi).
 // Lanes take whole (x, y) stencil columns and read their six z points in sequence (one cache
 // line, L1 hits after the first); sel6 keeps the column weights in registers.
@@ -676,7 +639,10 @@ __global__ void __launch_bounds__(256) k_stencil_prep(int n, const double* pos, 
     }
 }
 
-// k_spread_dip with the cached stencil (same lane layout and per-point arithmetic)
+// Dipole-only spread of the CG loop from the cached stencil: a warp per atom, lanes 0..29 form
+// five groups of six consecutive z points of one (x, y) stencil column; the 36 columns take eight
+// passes, so a warp's atomics of one pass touch five runs of six consecutive floats (coalesced in
+// L2) instead of 32 scattered addresses.
 template <typename T>
 __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, StencilCache<T> st) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;

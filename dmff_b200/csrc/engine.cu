@@ -548,12 +548,15 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     sa.perm_mul = h->perm_mul;
     if (zero_scal)
         for (int k = 0; k < 3; ++k) sa.zero_scal[k] = zero_scal[k];
-    if (dip && h->stencils_ready)
+    if (dip && h->stencils_ready) {
         LAUNCH(h, s, KC_SPREAD, k_spread_dip_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa, stencil_cache<T>(h)));
-    else if (dip)
-        LAUNCH(h, s, KC_SPREAD, k_spread_dip<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
-    else
+    } else {
+        // the general spread (dipoles alone when Qg is null) clears no scalars itself
+        if (zero_scal)
+            for (int k = 0; k < 3; ++k)
+                if (zero_scal[k]) CK(cudaMemsetAsync(zero_scal[k], 0, sizeof(double), s));
         LAUNCH(h, s, KC_SPREAD, k_spread<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa));
+    }
     CKFFT(cufftSetStream(h->plan_f, s));
     CKFFT(cufftSetStream(h->plan_b, s));
     if (sizeof(T) == 4) {
