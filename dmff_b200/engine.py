@@ -177,13 +177,28 @@ class AdmpEngine:
         self._check(st, allow=(L.DMFFB_NOT_CONVERGED,))
         return res, forces, U
 
-    def compute_host(self, pos, box, pairs=None, U=None):
-        """Host-buffer entry point: numpy in, numpy out (copies inside the engine)."""
+    def compute_host(self, pos, box, pairs=None, U=None, forces_out=None, U_out=None):
+        """Host-buffer entry point: numpy in, numpy out (copies inside the engine).  forces_out /
+        U_out: optional caller-owned float64 [n, 3] C-contiguous arrays (pinned memory copies
+        fastest) that receive the forces and the dipoles; U, when given, is the initial guess."""
         pos = np.ascontiguousarray(np.asarray(pos, np.float64))
         b = self._box(box)
         pr = None if pairs is None else np.ascontiguousarray(np.asarray(pairs, np.int32))
-        Uh = np.zeros((self.n, 3)) if U is None else np.ascontiguousarray(np.asarray(U, np.float64)).copy()
-        F = np.zeros((self.n, 3))
+
+        def out_array(a):
+            if a is None:
+                return np.zeros((self.n, 3))
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.shape == (self.n, 3)
+                    and a.flags["C_CONTIGUOUS"] and a.flags["WRITEABLE"]):
+                raise ValueError("output arrays must be writeable C-contiguous float64 [n, 3]")
+            return a
+
+        Uh = out_array(U_out)
+        if U is not None:
+            Uh[...] = np.asarray(U, np.float64)
+        elif U_out is not None and not getattr(self, "_zero_guess", False):
+            Uh[...] = 0.0  # the default initial guess (ignored by the engine under set_zero_guess)
+        F = out_array(forces_out)
         res = L.AdmpResult()
         with torch.cuda.device(self.device):
             st = self.lib.dmffb_admp_compute_host(
@@ -210,6 +225,7 @@ class AdmpEngine:
         """Dipole solves of the following computes start from U = 0 (the U buffer's content is
         ignored on input and receives the solution); the CG set-up then skips its A U pass."""
         self._check(self.lib.dmffb_admp_set_zero_guess(self.h, int(bool(on))))
+        self._zero_guess = bool(on)
 
     def param_grads(self):
         """{'Q_global', 'Q_local': [n, 9], 'pol', 'thole': [n]} of the last compute."""

@@ -125,6 +125,22 @@ def test_host_buffer_path_matches_device_path(pol_small):
     assert rel_force_rms(F_h, F_d) <= 1e-5
 
 
+def test_host_buffer_path_into_caller_arrays(pol_small):
+    """compute_host writes forces and dipoles into caller-owned (here pinned) arrays."""
+    s, pr, _ = pol_small
+    eng = make_engine(s, precision="fp32", cg_tol=1e-6)
+    res_a, F_a, U_a = eng.compute_host(s["pos"], s["box"], pairs=pr)
+    F_out = torch.zeros((s["n_atoms"], 3), dtype=torch.float64).pin_memory().numpy()
+    U_out = torch.full((s["n_atoms"], 3), 7.0, dtype=torch.float64).pin_memory().numpy()
+    res_b, F_b, U_b = eng.compute_host(s["pos"], s["box"], pairs=pr, forces_out=F_out, U_out=U_out)
+    assert F_b is F_out and U_b is U_out
+    assert abs(res_b.energy - res_a.energy) <= 1e-6 * abs(res_a.energy)
+    assert rel_force_rms(F_b, F_a) <= 1e-5
+    assert rel_force_rms(U_b, U_a) <= 1e-5
+    with pytest.raises(ValueError):
+        eng.compute_host(s["pos"], s["box"], pairs=pr, forces_out=np.zeros((s["n_atoms"], 3), np.float32))
+
+
 @pytest.mark.parametrize("name,L,n,rc", [("tiny", 9.3, 27, 4.5), ("c0", 18.6, 216, 6.0), ("mid", 31.0, 1000, 8.0)])
 def test_neighbor_set_bit_exact(name, L, n, rc):
     import oracle.admp_ref as R
