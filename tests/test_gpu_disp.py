@@ -56,6 +56,26 @@ def test_dispersion_pme_and_tt_match_oracle(disp_case, prec, te, tf):
     assert np.abs(np.array(res.box_grad_sr[:]).reshape(3, 3) - ref["Bsr"]).max() <= tf * np.abs(ref["Bsr"]).max()
 
 
+@pytest.mark.parametrize("prec,te,tf", [("fp64", 1e-10, 1e-8), ("fp32", 1e-5, 1e-4)])
+def test_dispersion_triclinic_box(prec, te, tf):
+    """Dispersion PME + TT on a sheared box (K from the box diagonal, as the reference)."""
+    from tests.test_gpu_edges import _sheared
+    s = _sheared(water_box(64, 12.4, seed=22, lmax=2, pol=False, rc=5.0), (0.2, -0.12, 0.15))
+    d = disp_params(64, seed=3)
+    pr = oracle_pairs(s)
+    ref = disp_oracle(s, d, pr)
+    eng = DispEngine(s["n_atoms"], 10, True, s["rc"], s["kappa"], s["K"], s["cov_rows"], d["mscales"], tt=True,
+                     precision=prec)
+    eng.set_params(d["c_list"], d["a"], d["b"], d["q"])
+    pos = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
+    res, (Flr, Fsr) = eng.compute(pos, s["box"], pairs=torch.tensor(pr, dtype=torch.int32, device="cuda"))
+    assert abs(res.energy - ref["Elr"]) <= te * abs(ref["Elr"])
+    assert abs(res.e_sr - ref["Esr"]) <= te * abs(ref["Esr"])
+    assert rel_force_rms(Flr.cpu().numpy(), ref["Flr"]) <= tf
+    assert rel_force_rms(Fsr.cpu().numpy(), ref["Fsr"]) <= tf
+    assert np.abs(np.array(res.box_grad[:]).reshape(3, 3) - ref["Blr"]).max() <= tf * np.abs(ref["Blr"]).max()
+
+
 def _waterbox():
     from tests.test_oracle_golden import _waterbox_topology
     return _waterbox_topology()
