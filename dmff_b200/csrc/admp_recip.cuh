@@ -648,11 +648,10 @@ __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, Sten
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
-    if (warp >= a.n) return;
+    if (warp >= a.n) return;  // whole warps: every lane below takes part in the shuffles
     const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
     const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
     const int grp = lane / 6, iz = lane - 6 * grp;
-    if (grp >= 5) return;
     const int4 o = st.org[at];
     const T* w = st.w + 36 * (size_t)at;
     const double* B = a.g.B;
@@ -660,17 +659,30 @@ __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, Sten
     const T c2 = -(T(B[3]) * mu0 + T(B[4]) * mu1 + T(B[5]) * mu2);
     const T c3 = -(T(B[6]) * mu0 + T(B[7]) * mu1 + T(B[8]) * mu2);
     const int K0 = a.g.K[0], K1 = a.g.K[1], K2 = a.g.K[2];
-    const T mz0 = __ldg(w + 24 + iz), mz1 = __ldg(w + 30 + iz);
-    const int gz = wrap_up(o.z + iz, K2);
+    // the atom's 36 weights sit in lanes (w[0..31] in wl, w[32..35] in wh of lanes 0..3) and the
+    // wrapped mesh bases in lanes 0..5 (x rows times K1) and 6..11 (y columns); the passes read
+    // them by shuffles instead of loads and integer wraps
+    const T wl = __ldg(w + lane);
+    const T wh = lane < 4 ? __ldg(w + 32 + lane) : T(0);
+    int base = 0;
+    if (lane < 6) base = wrap_up(o.x + lane, K0) * K1;
+    else if (lane < 12) base = wrap_up(o.y + lane - 6, K1);
+    const int izc = iz < 6 ? iz : 0;
+    const T mz0 = __shfl_sync(0xffffffffu, wl, 24 + izc);
+    const T mz1a = __shfl_sync(0xffffffffu, wl, (30 + izc) & 31), mz1b = __shfl_sync(0xffffffffu, wh, (izc + 30) & 3);
+    const T mz1 = 30 + izc < 32 ? mz1a : mz1b;
+    const int gz = wrap_up(o.z + izc, K2);
 #pragma unroll
     for (int pass = 0; pass < 8; ++pass) {
         const int col = grp + 5 * pass;
-        if (col < 36) {
-            const int ix = col / 6, iy = col - 6 * ix;
-            const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy), my1 = __ldg(w + 18 + iy);
+        const int cc = col < 36 ? col : 35;
+        const int ix = cc / 6, iy = cc - 6 * ix;
+        const T mx0 = __shfl_sync(0xffffffffu, wl, ix), mx1 = __shfl_sync(0xffffffffu, wl, 6 + ix);
+        const T my0 = __shfl_sync(0xffffffffu, wl, 12 + iy), my1 = __shfl_sync(0xffffffffu, wl, 18 + iy);
+        const int xb = __shfl_sync(0xffffffffu, base, ix), yb = __shfl_sync(0xffffffffu, base, 6 + iy);
+        if (grp < 5 && col < 36) {
             const T v = (c1 * mx1 * my0 + c2 * mx0 * my1) * mz0 + c3 * mx0 * my0 * mz1;
-            const int gx = wrap_up(o.x + ix, K0), gy = wrap_up(o.y + iy, K1);
-            atomicAdd(a.grid + ((size_t)gx * K1 + gy) * K2 + gz, v);
+            atomicAdd(a.grid + (size_t)(xb + yb) * K2 + gz, v);
         }
     }
 }

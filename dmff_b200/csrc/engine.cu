@@ -2156,8 +2156,10 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     const int chmax = (int)(1.5 * 125.0 * (double)n / (double)ncell + 64.0);
     const size_t stage_bytes = (size_t)chmax * sizeof(float4);
     const bool staged = stage_bytes <= kNbStageBytes;
+    const bool ortho = m[1] == 0.0 && m[2] == 0.0 && m[3] == 0.0 && m[5] == 0.0 && m[6] == 0.0 && m[7] == 0.0;
     if (fine && !staged) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
-    else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<0, 2, kNbWarps><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
+    else if (fine && ortho) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<0, 2, kNbWarps, true><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
+    else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<0, 2, kNbWarps, false><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<0><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
     tb = h->cub_bytes;
@@ -2186,7 +2188,8 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.ent = want_csr ? h->d_csr_ent : nullptr;
     b.cap_f = want_csr ? h->csr_cap : 0;
     if (fine && !staged) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<1, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
-    else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<1, 2, kNbWarps><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
+    else if (fine && ortho) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<1, 2, kNbWarps, true><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
+    else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<1, 2, kNbWarps, false><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
     else LAUNCH(h, s, KC_NBLIST, k_pairs_warp2<1><<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(b));
     CK(cudaGetLastError());
     // no host wait for the fill pass: later work on this stream is ordered after it, and compute

@@ -475,8 +475,9 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_pairs_warp3(Nb2Args b) {
 // and, when it fits in `chmax` entries, staged in shared memory as (x, y, z, j) float4s, so the
 // cell's atoms read their candidates from shared memory instead of each gathering them from L2;
 // neighbourhoods larger than the stage fall back to the global gathers.  The NW warps of the CTA
-// take the cell's atoms in turn.
-template <int PASS, int S, int NW>
+// take the cell's atoms in turn.  ORTHO: the box is orthorhombic and the FP32 prefilter's minimum
+// image is three multiplies per axis (candidates near rc still take the exact FP64 test).
+template <int PASS, int S, int NW, bool ORTHO>
 __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
     constexpr int W = 2 * S + 1, NQ = W * W * W;
     __shared__ int s_beg[NQ];
@@ -575,18 +576,32 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
                 if (j != i) {
                     const float d0 = pjx - pix, d1 = pjy - piy, d2 = pjz - piz;
                     bool amb = false;
-                    float sf[3];
+                    float r2;
+                    if (ORTHO) {
+                        const float dd[3] = {d0, d1, d2};
+                        r2 = 0.f;
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        float tt = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
-                        float nn = floorf(tt + 0.5f);
-                        sf[q] = tt - nn;
-                        amb |= fabsf(sf[q]) > 0.4999f;
+                        for (int q = 0; q < 3; ++q) {
+                            const float tt = dd[q] * hif[4 * q];
+                            const float sq = tt - floorf(tt + 0.5f);
+                            amb |= fabsf(sq) > 0.4999f;
+                            const float e = sq * hf[4 * q];
+                            r2 = fmaf(e, e, r2);
+                        }
+                    } else {
+                        float sf[3];
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            float tt = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
+                            float nn = floorf(tt + 0.5f);
+                            sf[q] = tt - nn;
+                            amb |= fabsf(sf[q]) > 0.4999f;
+                        }
+                        const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
+                        const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
+                        const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
+                        r2 = e0 * e0 + e1 * e1 + e2 * e2;
                     }
-                    const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
-                    const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
-                    const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
-                    const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
                     if (!amb && r2 < rlo2) keep = true;
                     else if (!amb && r2 > rhi2) keep = false;
                     else keep = j > i ? within_rc(a.box, pi, a.pos + 3 * j, a.rc)
