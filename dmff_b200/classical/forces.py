@@ -26,11 +26,12 @@ class ClassicalForce:
 
     def __init__(self, n_atoms, n_types=0, coulomb="none", pbc=True, rc=10.0, kappa=0.0, K=(0, 0, 0),
                  cov_rows=None, mscales_coul=(0, 0, 0, 1, 1, 1), mscales_lj=(0, 0, 0, 1, 1, 1),
-                 precision="fp32", device=None):
+                 eps_solvent=78.5, precision="fp32", device=None):
         self.cfg = dict(n_atoms=int(n_atoms), n_types=int(n_types), coulomb=coulomb, pbc=bool(pbc), rc=float(rc),
                         kappa=float(kappa), K=tuple(int(k) for k in K), cov_rows=cov_rows,
                         mscales_coul=tuple(float(x) for x in mscales_coul),
-                        mscales_lj=tuple(float(x) for x in mscales_lj), precision=precision, device=device)
+                        mscales_lj=tuple(float(x) for x in mscales_lj), eps_solvent=float(eps_solvent),
+                        precision=precision, device=device)
         self.n_atoms = int(n_atoms)
         self.n_types = int(n_types)
         self.coulomb = coulomb
