@@ -10,9 +10,9 @@ from .api.topology import DMFFTopology, PDBFile  # noqa: F401
 
 
 def __getattr__(name):
-    if name == "NeighborList":
-        from .common.nblist import NeighborList
-        return NeighborList
+    if name in ("NeighborList", "NeighborListFreud"):
+        from .common import nblist
+        return getattr(nblist, name)
     if name == "ADMPPmeForce":
         from .admp.pme import ADMPPmeForce
         return ADMPPmeForce
