@@ -75,7 +75,7 @@ class _AdmpEnergy(torch.autograd.Function):
         res, forces, U = eng.compute(pos, box, pairs=pairs, U=U)
         force.last_result = res
         if aux is not None:
-            aux["U_ind_A"] = U
+            aux["U_ind"] = U * 0.1  # Angstrom -> nm, as pme.py:225
             aux["lconverg"] = bool(res.converged)
             aux["n_cycle"] = int(res.n_iter)
         ctx.save_for_backward(forces.clone())
@@ -134,6 +134,7 @@ class ADMPPmeForce:
         self._engine = None
         self._param_key = None
         self.last_result = None
+        self.refresh_calculators()
 
     @property
     def engine(self):
@@ -157,8 +158,7 @@ class ADMPPmeForce:
                 for a, b in zip(old[0], vals)):
             return
         key = (vals, scales)
-        eng = self.engine
-        d = eng.lib  # scales are part of the description: rebuild when they change
+        # scales are part of the engine description: rebuild when they change
         ms = np.asarray(torch.as_tensor(mScales).detach().cpu(), np.float64)
         ps = np.asarray(torch.as_tensor(pScales).detach().cpu(), np.float64) if pScales is not None else None
         ds = np.asarray(torch.as_tensor(dScales).detach().cpu(), np.float64) if dScales is not None else None
@@ -170,27 +170,29 @@ class ADMPPmeForce:
                 self.cov_rows, ms, ps, ds, precision=self.precision, solver=self.pol_solver, cg_tol=self.cg_tol,
                 max_iter=self.max_iter, steps_pol=self.steps_pol, device=self.device)
             self._scales = scales
-        del d
         self.engine.set_params(Q_local, pol if self.lpol else None, tholes if self.lpol else None)
         self._param_key = key
 
     def get_energy(self, positions, box, pairs, Q_local, pol=None, tholes=None, mScales=None, pScales=None,
                    dScales=None, U_init=None, aux=None):
         """Energy (kJ/mol) for positions / box in Angstrom; pairs (i, j, nbond) rows or None for the
-        engine's own cell-list pairs.  U_init in Angstrom (the reference scales aux U by 10 before)."""
+        engine's own cell-list pairs.  As in the reference (pme.py:186-232), U_init is in nm and is
+        scaled to Angstrom here, and ``aux`` receives U_ind (nm), lconverg and n_cycle."""
         if not self.lpol:
             # non-polarizable signature: get_energy(positions, box, pairs, Q_local, mScales)
             if mScales is None and pol is not None:
                 mScales, pol = pol, None
         self._sync_params(Q_local, pol, tholes, mScales, pScales, dScales)
         eng = self.engine
+        if not torch.is_tensor(positions):
+            positions = torch.as_tensor(np.asarray(positions), dtype=torch.float64)
         if not torch.is_tensor(box):
             box = torch.as_tensor(np.asarray(box), dtype=torch.float64)
         pairs_d = _as_cuda_pairs(pairs, eng.device)
         U0 = None
         if self.lpol:
             U0 = U_init if U_init is not None else self.U_ind
-            U0 = torch.as_tensor(U0, dtype=torch.float64)
+            U0 = torch.as_tensor(np.asarray(U0) if not torch.is_tensor(U0) else U0, dtype=torch.float64) * 10.0
         Q_local = torch.as_tensor(Q_local, dtype=torch.float64)
         if self.lpol:
             pol = torch.as_tensor(pol, dtype=torch.float64)
@@ -198,4 +200,36 @@ class ADMPPmeForce:
         else:
             pol = tholes = None
         E = _AdmpEnergy.apply(positions, box, Q_local, pol, tholes, self, pairs_d, U0, aux)
-        return E
+        return E if aux is None else (E, aux)
+
+    def generate_get_energy(self):
+        """The energy closure of pme.py:116-245.  Its signature covers both of the reference's
+        forms: (positions, box, pairs, Q_local, mScales) and, polarizable, (..., Q_local, pol,
+        tholes, mScales, pScales, dScales, U_init, aux)."""
+        return ADMPPmeForce.get_energy.__get__(self)
+
+    def update_env(self, attr, val):
+        """Set one attribute (kappa, K1, lmax, axis_type, ...) and rebuild the calculators
+        (pme.py:198-203)."""
+        setattr(self, attr, val)
+        self.refresh_calculators()
+
+    def refresh_calculators(self):
+        """Drop the engine so that the next call builds one from the current attributes, and
+        regenerate ``get_forces`` = value_and_grad(get_energy) w.r.t. positions (pme.py:205-224)."""
+        self._engine = None
+        self._param_key = None
+        self._scales = None
+        self.n_atoms = len(self.axis_type)
+        self.U_ind = torch.zeros((self.n_atoms, 3), dtype=torch.float64)
+        energy = self.generate_get_energy()
+
+        def get_forces(positions, *args, **kwargs):
+            with torch.enable_grad():
+                p = torch.as_tensor(positions, dtype=torch.float64).detach().requires_grad_(True)
+                out = energy(p, *args, **kwargs)
+                E = out[0] if isinstance(out, tuple) else out
+                (g,) = torch.autograd.grad(E, p)
+            return (E.detach(), g) if not isinstance(out, tuple) else ((E.detach(), out[1]), g)
+
+        self.get_forces = get_forces

@@ -218,12 +218,10 @@ class ADMPPmeGenerator:
                 pol = torch.as_tensor(p["pol"])[torch.as_tensor(map_poltype)]
                 tholes = torch.as_tensor(p["thole"])[torch.as_tensor(map_poltype)]
                 if has_aux:
-                    U0 = aux["U_ind"] * 10.0 if (aux is not None and "U_ind" in aux) else torch.zeros((n_atoms, 3))
+                    U0 = aux["U_ind"] if (aux is not None and "U_ind" in aux) else torch.zeros((n_atoms, 3))
                     aux = {} if aux is None else aux
-                    energy = pme_force.get_energy(positions, box, pairs, Q_local, pol, tholes, mS, pS, dS,
-                                                  U_init=U0, aux=aux)
-                    aux["U_ind"] = aux.pop("U_ind_A") * 0.1
-                    return energy, aux
+                    return pme_force.get_energy(positions, box, pairs, Q_local, pol, tholes, mS, pS, dS,
+                                                U_init=U0, aux=aux)
                 return pme_force.get_energy(positions, box, pairs, Q_local, pol, tholes, mS, pS, dS,
                                             U_init=pme_force.U_ind)
             energy = pme_force.get_energy(positions, box, pairs, Q_local, mS)
