@@ -28,6 +28,34 @@ class ADMPDispPmeForce:
         self._engine = None
         self._key = None
         self.last_result = None
+        self.refresh_calculators()
+
+    def generate_get_energy(self):
+        """The energy closure of disp_pme.py:45-51, get_energy(positions, box, pairs, c_list,
+        mScales) (with the optional ``tt`` triple of this engine's fused short-range term)."""
+        return ADMPDispPmeForce.get_energy.__get__(self)
+
+    def update_env(self, attr, val):
+        """Set one attribute (kappa, K1, pmax, ...) and rebuild the calculators
+        (disp_pme.py:54-59)."""
+        setattr(self, attr, val)
+        self.refresh_calculators()
+
+    def refresh_calculators(self):
+        """Drop the engine so that the next call builds one from the current attributes, and
+        regenerate ``get_forces`` = value_and_grad(get_energy) w.r.t. positions
+        (disp_pme.py:62-77)."""
+        self._engine = None
+        energy = self.generate_get_energy()
+
+        def get_forces(positions, *args, **kwargs):
+            with torch.enable_grad():
+                p = torch.as_tensor(positions, dtype=torch.float64).detach().requires_grad_(True)
+                E = energy(p, *args, **kwargs)
+                (g,) = torch.autograd.grad(E, p)
+            return E.detach(), g
+
+        self.get_forces = get_forces
 
     def _eng(self, n, mScales):
         from ..engine import DispEngine

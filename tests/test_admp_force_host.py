@@ -65,3 +65,33 @@ def test_get_forces_and_update_env():
     assert f.generate_get_energy()(pos, torch.eye(3) * 20, None, Q, ms).item() == -12.5
     f.update_env("kappa", 0.41)
     assert f.kappa == 0.41 and f._engine is None and f._scales is None
+
+
+class _DispRecorder:
+    device = torch.device("cpu")
+
+    def __init__(self, n, mscales):
+        self.n, self.mscales = n, mscales
+
+    def set_params(self, *args):
+        pass
+
+    def set_param_grads(self, on):
+        pass
+
+    def compute(self, pos, box, pairs=None):
+        res = SimpleNamespace(energy=3.0, e_sr=5.0, box_grad=[0.0] * 9, box_grad_sr=[0.0] * 9)
+        return res, (torch.ones_like(pos) * 0.5, torch.ones_like(pos) * 2.0)
+
+
+def test_disp_force_calculators():
+    from dmff_b200.admp.disp_pme import ADMPDispPmeForce
+    n, ms = 4, [0.0, 0.0, 0.0, 1.0, 1.0, 1.0]
+    f = ADMPDispPmeForce(np.eye(3) * 20.0, 8.0, 5e-4, 10)
+    f._engine = _DispRecorder(n, tuple(ms))
+    c = torch.ones((n, 3), dtype=torch.float64)
+    E, g = f.get_forces(np.zeros((n, 3)), torch.eye(3) * 20, None, c, ms)
+    assert E.item() == 3.0 and torch.allclose(g, torch.full((n, 3), -0.5, dtype=torch.float64))
+    assert f.generate_get_energy()(torch.zeros((n, 3)), torch.eye(3) * 20, None, c, ms).item() == 3.0
+    f.update_env("kappa", 0.3)
+    assert f.kappa == 0.3 and f._engine is None
