@@ -7,11 +7,27 @@ topology from the XML residue templates and returns a ``Potential`` whose
 Nonbonded methods are accepted as OpenMM constants or their names ("PME", "CutoffPeriodic",
 "NoCutoff", "CutoffNonPeriodic").
 """
+import numpy as np
+
 from .paramset import ParamSet
-from .topology import DMFFTopology, PDBFile
+from .topology import DMFFTopology, PDBFile, covalent_rows
 from .xmlio import XMLIO
 
 _DMFFGenerators = {}
+
+
+def build_covalent_map(data, max_neighbor):
+    """Dense [n, n] matrix of shortest bond-path lengths 1 .. max_neighbor (0 otherwise) for a
+    topology record with ``atoms`` and ``bonds`` (bond.atom1 / bond.atom2 as indices or atoms),
+    the breadth-first map of hamiltonian.py:17-35."""
+    n = len(data.atoms)
+    idx = lambda a: int(getattr(a, "index", a))
+    rows = covalent_rows(n, [(idx(b.atom1), idx(b.atom2)) for b in data.bonds], max_neighbor)
+    cm = np.zeros((n, n), dtype=int)
+    if len(rows):
+        cm[rows[:, 0], rows[:, 1]] = rows[:, 2]
+        cm[rows[:, 1], rows[:, 0]] = rows[:, 2]
+    return cm
 
 
 def method_name(m):

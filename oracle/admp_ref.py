@@ -1052,6 +1052,26 @@ def torsion_energy(positions, p1, p2, p3, p4, k, psi, order):
 
 
 # --------------------------------------------------------------------------------------
+# covalent map — dmff/api/hamiltonian.py:17-35
+# --------------------------------------------------------------------------------------
+def build_covalent_map(n_atoms, bonds, max_neighbor):
+    """hamiltonian.py:17-35, step for step: bonded pairs get 1; then for n_curr = 1 ..
+    max_neighbor - 1, every atom k bonded to a current neighbour j (0 < d(i, j) <= n_curr) of i,
+    k != i and k not among those neighbours, gets n_curr + 1 (both orientations)."""
+    cm = np.zeros((n_atoms, n_atoms), dtype=int)
+    for a, b in bonds:
+        cm[a, b] = cm[b, a] = 1
+    for n_curr in range(1, max_neighbor):
+        for i in range(n_atoms):
+            j_list = np.where((cm[i] <= n_curr) & (cm[i] > 0))[0]
+            for j in j_list:
+                for k in np.where(cm[j] == 1)[0]:
+                    if k != i and k not in j_list:
+                        cm[i, k] = cm[k, i] = n_curr + 1
+    return cm
+
+
+# --------------------------------------------------------------------------------------
 # neighbour pairs — dmff/common/nblist.py:22-55 semantics (brute force, strict r < rc)
 # --------------------------------------------------------------------------------------
 def brute_force_pairs(positions, box, rc, nbond_of=None):

@@ -102,3 +102,27 @@ def test_pairs_nbond_lookup():
     s = water_box(8, 6.2, seed=3)
     pr = np.array([[0, 1, 0], [1, 2, 0], [0, 3, 0], [3, 5, 0]])
     np.testing.assert_array_equal(pairs_nbond(pr, s["cov_rows"], s["n_atoms"]), [1, 2, 0, 1])
+
+
+def test_build_covalent_map_matches_reference_loop():
+    """build_covalent_map (hamiltonian.py:17-35) on chains, rings and branches, against the
+    oracle's step-for-step restatement of the reference's loop."""
+    from types import SimpleNamespace
+
+    import oracle.admp_ref as R
+    from dmff_b200.api.hamiltonian import build_covalent_map
+    rng = np.random.default_rng(3)
+    graphs = [
+        [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (5, 0)],            # six-ring
+        [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (5, 6), (6, 7)],    # chain longer than the map
+        [(0, 1), (0, 2), (0, 3), (3, 4), (4, 5), (4, 6), (6, 7), (7, 3)],  # branch + four-ring
+    ]
+    tree = [(k, int(rng.integers(0, k))) for k in range(1, 14)]
+    graphs.append(tree + [(2, 9), (5, 12)])  # random tree with two extra ring bonds
+    for bonds in graphs:
+        n = max(max(b) for b in bonds) + 2  # one isolated atom
+        data = SimpleNamespace(atoms=list(range(n)), bonds=[SimpleNamespace(atom1=a, atom2=b) for a, b in bonds])
+        for mx in (1, 3, 6):
+            got = build_covalent_map(data, mx)
+            want = R.build_covalent_map(n, bonds, mx)
+            assert np.array_equal(got, want), (bonds, mx)
