@@ -5,6 +5,7 @@ import re
 import subprocess
 
 import numpy as np
+import torch
 import pytest
 
 from dmff_b200 import Hamiltonian, PDBFile
@@ -126,3 +127,18 @@ def test_build_covalent_map_matches_reference_loop():
             got = build_covalent_map(data, mx)
             want = R.build_covalent_map(n, bonds, mx)
             assert np.array_equal(got, want), (bonds, mx)
+
+
+def test_utils_pair_helpers_match_oracle():
+    import oracle.admp_ref as R
+    from dmff_b200 import utils as U
+    rng = np.random.default_rng(8)
+    p = rng.integers(0, 50, (200, 2))
+    p[:20] = 50  # (N, N) padding rows
+    assert np.array_equal(U.regularize_pairs(p).numpy(), R.regularize_pairs(p).numpy())
+    assert np.array_equal(U.pair_buffer_scales(p).numpy(), R.pair_buffer_scales(p).numpy().astype(int))
+    assert U.convertStr2Float("1.5") == 1.5 and U.convertStr2Float("OW") == "OW"
+    assert U.findItemInList("b", ["a", "b"]) == 1 and U.findItemInList("c", ["a"]) == -1
+    d = U.dict_to_jnp({"A": {"k": [1, 2]}, "x": 3.0})
+    assert d["A"]["k"].dtype == torch.float64 and float(d["x"]) == 3.0
+    assert U.jit_condition(static_argnums=(1,))(len) is len
