@@ -142,3 +142,31 @@ def test_utils_pair_helpers_match_oracle():
     d = U.dict_to_jnp({"A": {"k": [1, 2]}, "x": 3.0})
     assert d["A"]["k"].dtype == torch.float64 and float(d["x"]) == 3.0
     assert U.jit_condition(static_argnums=(1,))(len) is len
+
+
+# every import a caller of the reference's energy/force path makes, as (module, names)
+DROP_IN_IMPORTS = [
+    ("", ["Hamiltonian", "NeighborList", "NeighborListFreud"]),
+    ("api", ["Hamiltonian", "DMFFTopology"]),
+    ("api.hamiltonian", ["Hamiltonian", "Potential", "build_covalent_map"]),
+    ("admp.pme", ["ADMPPmeForce", "setup_ewald_parameters", "DIELECTRIC"]),
+    ("admp.disp_pme", ["ADMPDispPmeForce"]),
+    ("admp.multipole", ["convert_cart2harm", "convert_harm2cart", "rot_global2local", "rot_local2global",
+                        "rot_ind_global2local", "C1_h2c", "C2_h2c"]),
+    ("classical.inter", ["LennardJonesForce", "LennardJonesLongRangeForce", "CoulNoCutoffForce",
+                         "CoulReactionFieldForce", "CoulombPMEForce"]),
+    ("classical.intra", ["HarmonicBondJaxForce", "HarmonicAngleJaxForce", "PeriodicTorsionJaxForce"]),
+    ("common.nblist", ["NeighborList", "NeighborListFreud", "NoCutoffNeighborList", "NoPeriodicNeighborList"]),
+    ("generators", ["ADMPPmeGenerator", "ADMPDispPmeGenerator", "ADMPDispGenerator", "NonbondedGenerator",
+                    "CoulombGenerator", "LennardJonesGenerator", "HarmonicBondGenerator", "HarmonicAngleGenerator",
+                    "PeriodicTorsionGenerator"]),
+    ("utils", ["regularize_pairs", "pair_buffer_scales", "DMFFException"]),
+]
+
+
+@pytest.mark.parametrize("mod,names", DROP_IN_IMPORTS, ids=[m or "dmff" for m, _ in DROP_IN_IMPORTS])
+def test_drop_in_import_surface(mod, names):
+    import importlib
+    m = importlib.import_module("dmff_b200" + ("." + mod if mod else ""))
+    for n in names:
+        assert getattr(m, n, None) is not None, f"dmff.{mod}.{n}"
