@@ -208,6 +208,25 @@ class ADMPPmeForce:
         tholes, mScales, pScales, dScales, U_init, aux)."""
         return ADMPPmeForce.get_energy.__get__(self)
 
+    def generate_Q_global_function(self):
+        """``get_Q_global(positions, box, Q_local)`` -> global Cartesian multipoles [n, 1 | 4 | 10]
+        (charge; dipole; quadrupole xx yy zz xy xz yz), i.e. Q_local per type mapped to atoms,
+        rotated by the local frames and converted to Cartesian (pme.py:183-196).  A host
+        utility in torch; the engine keeps its own global multipoles on the GPU."""
+        from .multipole import convert_harm2cart, rot_local2global
+        from .spatial import generate_construct_local_frames
+        lmax, mt = self.lmax, torch.as_tensor(self.map_atomtype, dtype=torch.long)
+        frames = generate_construct_local_frames(self.axis_type, self.axis_indices) if lmax > 0 else None
+
+        def get_Q_global(positions, box, Q_local):
+            Q = torch.as_tensor(Q_local, dtype=torch.float64)[mt.to(Q_local.device if torch.is_tensor(Q_local)
+                                                                      else "cpu")]
+            if frames is not None:
+                Q = rot_local2global(Q[:, : (lmax + 1) ** 2], frames(positions, box), lmax)
+            return convert_harm2cart(Q, lmax)
+
+        return get_Q_global
+
     def update_env(self, attr, val):
         """Set one attribute (kappa, K1, lmax, axis_type, ...) and rebuild the calculators
         (pme.py:198-203)."""
@@ -222,6 +241,12 @@ class ADMPPmeForce:
         self._scales = None
         self.n_atoms = len(self.axis_type)
         self.U_ind = torch.zeros((self.n_atoms, 3), dtype=torch.float64)
+        self.Q_local_to_global = self.generate_Q_global_function()
+        if self.lmax > 0:
+            from .spatial import generate_construct_local_frames
+            self.construct_local_frames = generate_construct_local_frames(self.axis_type, self.axis_indices)
+        else:
+            self.construct_local_frames = None
         energy = self.generate_get_energy()
 
         def get_forces(positions, *args, **kwargs):

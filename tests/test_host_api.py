@@ -151,6 +151,8 @@ DROP_IN_IMPORTS = [
     ("api.hamiltonian", ["Hamiltonian", "Potential", "build_covalent_map"]),
     ("admp.pme", ["ADMPPmeForce", "setup_ewald_parameters", "DIELECTRIC"]),
     ("admp.disp_pme", ["ADMPDispPmeForce"]),
+    ("admp.spatial", ["pbc_shift", "v_pbc_shift", "normalize", "generate_construct_local_frames",
+                      "build_quasi_internal"]),
     ("admp.multipole", ["convert_cart2harm", "convert_harm2cart", "rot_global2local", "rot_local2global",
                         "rot_ind_global2local", "C1_h2c", "C2_h2c"]),
     ("classical.inter", ["LennardJonesForce", "LennardJonesLongRangeForce", "CoulNoCutoffForce",
