@@ -216,7 +216,8 @@ class ADMPPmeForce:
         from .multipole import convert_harm2cart, rot_local2global
         from .spatial import generate_construct_local_frames
         lmax, mt = self.lmax, torch.as_tensor(self.map_atomtype, dtype=torch.long)
-        frames = generate_construct_local_frames(self.axis_type, self.axis_indices) if lmax > 0 else None
+        has_frames = lmax > 0 and self.axis_indices is not None
+        frames = generate_construct_local_frames(self.axis_type, self.axis_indices) if has_frames else None
 
         def get_Q_global(positions, box, Q_local):
             Q = torch.as_tensor(Q_local, dtype=torch.float64)[mt.to(Q_local.device if torch.is_tensor(Q_local)
@@ -242,7 +243,7 @@ class ADMPPmeForce:
         self.n_atoms = len(self.axis_type)
         self.U_ind = torch.zeros((self.n_atoms, 3), dtype=torch.float64)
         self.Q_local_to_global = self.generate_Q_global_function()
-        if self.lmax > 0:
+        if self.lmax > 0 and self.axis_indices is not None:
             from .spatial import generate_construct_local_frames
             self.construct_local_frames = generate_construct_local_frames(self.axis_type, self.axis_indices)
         else:
