@@ -208,6 +208,47 @@ class ADMPPmeForce:
         tholes, mScales, pScales, dScales, U_init, aux)."""
         return ADMPPmeForce.get_energy.__get__(self)
 
+    def generate_esp(self):
+        """``get_esp(positions, grids, Q_local[, U_ind])`` -> potential [n_grid] (kJ/mol/e) of the
+        global multipoles (and induced dipoles when polarizable) at grid points, no periodic
+        images (pme.py:236-293).  Charge q / r, dipoles -(d / 10 + U) . dR / r^3 and
+        quadrupoles 3 dR^T (Q / 300) dR / r^5 with dR = r_site - r_grid, times DIELECTRIC / 10.
+        Host torch on the input's device, 4096 grid points at a time."""
+
+        def esp(positions, grids, Q_local, U_ind=None):
+            pos = torch.as_tensor(positions, dtype=torch.float64)
+            g = torch.as_tensor(grids, dtype=torch.float64).to(pos.device)
+            Qg = self.Q_local_to_global(pos, torch.eye(3, dtype=torch.float64, device=pos.device) * 1000.0,
+                                        torch.as_tensor(Q_local, dtype=torch.float64).to(pos.device))
+            n = pos.shape[0]
+            q = Qg[:, 0]
+            d = Qg[:, 1:4] / 10.0 if Qg.shape[1] >= 4 else torch.zeros((n, 3), dtype=torch.float64, device=pos.device)
+            if U_ind is not None:
+                d = d + torch.as_tensor(U_ind, dtype=torch.float64).to(pos.device)
+            quad = Qg[:, 4:10] / 300.0 if Qg.shape[1] >= 10 else None
+            out = []
+            for g0 in range(0, g.shape[0], 4096):
+                dR = pos[None, :, :] - g[g0:g0 + 4096, None, :]  # [G, n, 3]
+                r2 = (dR * dR).sum(-1) + 1e-16
+                rr1 = torch.rsqrt(r2)
+                rr3 = rr1 * rr1 * rr1
+                v = q * rr1 - (d * dR).sum(-1) * rr3
+                if quad is not None:
+                    xx, yy, zz, xy, xz, yz = quad.unbind(-1)
+                    x, y, z = dR.unbind(-1)
+                    scq = (xx * x * x + yy * y * y + zz * z * z) + 2.0 * (xy * x * y + xz * x * z + yz * y * z)
+                    v = v + scq * 3.0 * rr3 * rr1 * rr1
+                out.append(v.sum(-1))
+            return torch.cat(out) * DIELECTRIC * 0.1
+
+        if self.lpol:
+            def get_esp(positions, grids, Q_local, U_ind):
+                return esp(positions, grids, Q_local, U_ind)
+        else:
+            def get_esp(positions, grids, Q_local):
+                return esp(positions, grids, Q_local)
+        return get_esp
+
     def generate_Q_global_function(self):
         """``get_Q_global(positions, box, Q_local)`` -> global Cartesian multipoles [n, 1 | 4 | 10]
         (charge; dipole; quadrupole xx yy zz xy xz yz), i.e. Q_local per type mapped to atoms,

@@ -177,13 +177,35 @@ class _CoulombBase:
 
 
 class CoulNoCutoffForce(_CoulombBase):
-    """q_i q_j / (4 pi eps0 eps_1 r) over the pair rows, no periodic image (inter.py:133-174).
-    The grid ESP helper of inter.py:176-201 is not on the energy path and is not provided."""
+    """q_i q_j / (4 pi eps0 eps_1 r) over the pair rows, no periodic image (inter.py:133-174)."""
 
     coulomb = "nocutoff"
 
     def __init__(self, init_charges, epsilon_1=1.0, topology_matrix=None, precision="fp32", device=None) -> None:
         self._setup(init_charges, topology_matrix, epsilon_1, False, 1.0, precision=precision, device=device)
+
+    def generate_esp(self):
+        """``get_esp(positions, grids[, bcc])`` -> sum_i ONE_4PI_EPS0 q_i / |r_i - g + 1e-16| per
+        grid point (inter.py:176-201; the 1e-16 is added to each component, as there).  Host
+        torch on the input's device, 4096 grid points at a time."""
+
+        def esp(positions, grids, bcc):
+            pos = _t(positions)
+            g = _t(grids).to(pos.device)
+            q = self._charges(bcc).to(pos.device)
+            out = []
+            for g0 in range(0, g.shape[0], 4096):
+                r = torch.linalg.norm(pos[None, :, :] - g[g0:g0 + 4096, None, :] + 1e-16, dim=-1)
+                out.append((ONE_4PI_EPS0 * q / r).sum(-1))
+            return torch.cat(out)
+
+        if self.top_mat is None:
+            def get_esp(positions, grids):
+                return esp(positions, grids, None)
+        else:
+            def get_esp(positions, grids, bcc):
+                return esp(positions, grids, bcc)
+        return get_esp
 
 
 class CoulReactionFieldForce(_CoulombBase):

@@ -1052,6 +1052,36 @@ def torsion_energy(positions, p1, p2, p3, p4, k, psi, order):
 
 
 # --------------------------------------------------------------------------------------
+# electrostatic potential on grid points — dmff/admp/pme.py:236-293, classical/inter.py:176-201
+# --------------------------------------------------------------------------------------
+def admp_esp(positions, grids, Q_global_cart, U_ind):
+    """pme.py:236-293, one grid point at a time: per site dR = r_site - g, r = sqrt(dR.dR + 1e-16),
+    q / r - (d / 10 + U) . dR / r^3 + 3 dR^T (Q / 300) dR / r^5, summed, times DIELECTRIC / 10."""
+    pos = _t(positions)
+    Qc = _t(Q_global_cart)
+    U = _t(U_ind)
+    out = []
+    for g in _t(grids):
+        dR = pos - g
+        r = torch.sqrt((dR * dR).sum(1) + 1e-16)
+        v = Qc[:, 0] / r - ((Qc[:, 1:4] / 10.0 + U) * dR).sum(1) / r ** 3
+        quad = Qc[:, 4:10] / 300.0
+        M = torch.stack([torch.stack([quad[:, 0], quad[:, 3], quad[:, 4]], 1),
+                         torch.stack([quad[:, 3], quad[:, 1], quad[:, 5]], 1),
+                         torch.stack([quad[:, 4], quad[:, 5], quad[:, 2]], 1)], 1)
+        v = v + torch.einsum("ni,nij,nj->n", dR, M, dR) * 3.0 / r ** 5
+        out.append(v.sum() * DIELECTRIC * 0.1)
+    return torch.stack(out)
+
+
+def coul_nocutoff_esp(positions, grids, charges):
+    """inter.py:176-201: sum_i ONE_4PI_EPS0 q_i / |r_i - g + 1e-16| per grid point."""
+    pos = _t(positions)
+    q = _t(charges)
+    return torch.stack([(DIELECTRIC * 0.1 * q / torch.linalg.norm(pos - g + 1e-16, dim=1)).sum() for g in _t(grids)])
+
+
+# --------------------------------------------------------------------------------------
 # covalent map — dmff/api/hamiltonian.py:17-35
 # --------------------------------------------------------------------------------------
 def build_covalent_map(n_atoms, bonds, max_neighbor):

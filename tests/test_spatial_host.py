@@ -67,3 +67,35 @@ def test_global_multipoles_match_oracle():
         assert got.shape == (len(pos), [1, 4, 10][lmax])
         assert (got - want).abs().max() < 1e-10
     assert f.construct_local_frames is not None
+
+
+def test_esp_helpers_match_oracle():
+    """ADMPPmeForce.generate_esp (pme.py:236-293) and CoulNoCutoffForce.generate_esp
+    (inter.py:176-201) on grid points around a small water cluster."""
+    from dmff_b200.classical.inter import CoulNoCutoffForce
+    from dmff_b200.synthetic import water_box
+    s = water_box(8, 6.4, seed=2, lmax=2, pol=True, rc=3.0)
+    pos = np.asarray(s["pos"]) / 10.0  # nm, as the reference's ESP fits use
+    n = len(pos)
+    grids = np.random.default_rng(4).uniform(-0.3, 0.95, (5000, 3))  # > one 4096-point chunk
+    mt = np.arange(n)
+    Q = torch.tensor(np.asarray(s["Q_local"], dtype=np.float64))
+    U = torch.tensor(np.random.default_rng(5).normal(0, 0.01, (n, 3)))
+    f = ADMPPmeForce(np.eye(3) * 30, mt, s["axis_types"], s["axis_indices"], 6.0, 5e-4, 2, lpol=True)
+    got = f.generate_esp()(torch.tensor(pos), torch.tensor(grids), Q, U)
+    big = np.eye(3) * 1000.0
+    Qg = R.convert_harm2cart(R.rot_local2global(Q, R.construct_local_frames(pos, big, s["axis_types"],
+                                                                            s["axis_indices"]), 2), 2)
+    want = R.admp_esp(pos, grids, Qg, U)
+    assert got.shape == (5000,)
+    assert (got - want).abs().max() <= 1e-10 * want.abs().max()
+    f0 = ADMPPmeForce(np.eye(3) * 30, mt, s["axis_types"], s["axis_indices"], 6.0, 5e-4, 2)
+    got0 = f0.generate_esp()(torch.tensor(pos), torch.tensor(grids), Q)
+    assert (got0 - R.admp_esp(pos, grids, Qg, torch.zeros((n, 3)))).abs().max() <= 1e-10 * want.abs().max()
+    q = np.asarray(s["Q_local"])[:, 0]
+    top = np.random.default_rng(6).integers(-1, 2, (n, 2)).astype(float)
+    nc = CoulNoCutoffForce(q, topology_matrix=top)
+    bcc = torch.tensor([0.02, -0.01], dtype=torch.float64)
+    got = nc.generate_esp()(torch.tensor(pos), torch.tensor(grids), bcc)
+    want = R.coul_nocutoff_esp(pos, grids, torch.tensor(q) + torch.tensor(top) @ bcc)
+    assert (got - want).abs().max() <= 1e-12 * want.abs().max()
