@@ -10,7 +10,7 @@ Nonbonded methods are accepted as OpenMM constants or their names ("PME", "Cutof
 import numpy as np
 
 from .paramset import ParamSet
-from .topology import DMFFTopology, PDBFile, covalent_rows
+from .topology import DMFFTopology, covalent_rows
 from .xmlio import XMLIO
 
 _DMFFGenerators = {}
