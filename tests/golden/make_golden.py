@@ -93,6 +93,10 @@ def main():
         f"{REF}/tests/data/admp.xml": "admp.xml",
         f"{REF}/tests/data/admp_mono.xml": "admp_mono.xml",
         f"{REF}/tests/data/admp_nonpol.xml": "admp_nonpol.xml",
+        # ESP consistency inputs (tests/test_admp/test_esp.py)
+        f"{REF}/tests/data/admp_charge.xml": "admp_charge.xml",
+        f"{REF}/tests/data/water.pdb": "water.pdb",
+        f"{REF}/tests/data/water_ion.pdb": "water_ion.pdb",
         f"{wf}/forcefield.xml": "waterbox_forcefield.xml",
         f"{wf}/residues.xml": "waterbox_residues.xml",
         f"{wf}/quadrupole_nonpol/forcefield.xml": "waterbox_quadrupole_nonpol.xml",
