@@ -97,6 +97,9 @@ def main():
         f"{REF}/tests/data/admp_charge.xml": "admp_charge.xml",
         f"{REF}/tests/data/water.pdb": "water.pdb",
         f"{REF}/tests/data/water_ion.pdb": "water_ion.pdb",
+        # XML reader inputs (tests/test_frontend/test_xmlio.py)
+        f"{REF}/tests/data/test1.xml": "xmlio_test1.xml",
+        f"{REF}/tests/data/test2.xml": "xmlio_test2.xml",
         f"{wf}/forcefield.xml": "waterbox_forcefield.xml",
         f"{wf}/residues.xml": "waterbox_residues.xml",
         f"{wf}/quadrupole_nonpol/forcefield.xml": "waterbox_quadrupole_nonpol.xml",

@@ -172,3 +172,24 @@ def test_drop_in_import_surface(mod, names):
     m = importlib.import_module("dmff_b200" + ("." + mod if mod else ""))
     for n in names:
         assert getattr(m, n, None) is not None, f"dmff.{mod}.{n}"
+
+
+@pytest.mark.parametrize("files,n_types,residues,n_bond,n_nb", [
+    (["xmlio_test1.xml"], 4, [(4, 3, 2)], 3, 4),
+    (["xmlio_test1.xml", "xmlio_test2.xml"], 8, [(4, 3, 2), (5, 4, 2)], 6, 8),
+])
+def test_xml_reader_counts_like_reference(files, n_types, residues, n_bond, n_nb):
+    """tests/test_frontend/test_xmlio.py:7-57: one file, and two files merged, read into atom
+    types, residue templates (particles, bonds, externals) and force nodes with their attributes."""
+    from dmff_b200.api.xmlio import XMLIO
+    io = XMLIO()
+    for f in files:
+        io.loadXML(os.path.join(DATA, f))
+    ret = io.parseXML()
+    assert len(ret["AtomTypes"]) == n_types
+    assert [(len(r["particles"]), len(r["bonds"]), len(r["externals"])) for r in ret["Residues"]] == residues
+    assert len(ret["Forces"]) == 2
+    assert len(ret["Forces"]["HarmonicBondForce"]["node"]) == n_bond
+    assert {"k", "length", "type1", "type2"} <= set(ret["Forces"]["HarmonicBondForce"]["node"][0]["attrib"])
+    assert len(ret["Forces"]["NonbondedForce"]["node"]) == n_nb
+    assert {"charge", "epsilon", "sigma", "type"} <= set(ret["Forces"]["NonbondedForce"]["node"][0]["attrib"])
