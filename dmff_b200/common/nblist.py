@@ -91,11 +91,18 @@ def _nbond_lookup(cov_map, n, i, j):
     ``CovalentMap``; 0 for pairs that are not bonded."""
     dev = i.device
     if hasattr(cov_map, "pairs"):
-        r = torch.as_tensor(np.asarray(cov_map.pairs(), dtype=np.int64).reshape(-1, 3), device=dev)
-        dense = torch.zeros((n, n), dtype=torch.int32, device=dev)
-        if r.shape[0]:
-            dense[r[:, 0], r[:, 1]] = r[:, 2].to(torch.int32)
-            dense[r[:, 1], r[:, 0]] = r[:, 2].to(torch.int32)
+        # sparse rows: sorted keys i * n + j of both orientations, looked up by binary search
+        r = np.asarray(cov_map.pairs(), dtype=np.int64).reshape(-1, 3)
+        if r.shape[0] == 0:
+            return torch.zeros(i.shape, dtype=torch.int32, device=dev)
+        keys = np.concatenate([r[:, 0] * n + r[:, 1], r[:, 1] * n + r[:, 0]])
+        vals = np.concatenate([r[:, 2], r[:, 2]])
+        order = np.argsort(keys)
+        keys = torch.as_tensor(keys[order], device=dev)
+        vals = torch.as_tensor(vals[order], device=dev).to(torch.int32)
+        q = i.to(torch.int64) * n + j.to(torch.int64)
+        at = torch.searchsorted(keys, q).clamp(max=keys.shape[0] - 1)
+        return torch.where(keys[at] == q, vals[at], torch.zeros((), dtype=torch.int32, device=dev))
     else:
         m = cov_map.detach().cpu() if torch.is_tensor(cov_map) else cov_map
         dense = torch.as_tensor(np.asarray(m), device=dev).to(torch.int32)

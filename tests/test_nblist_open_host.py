@@ -4,7 +4,7 @@ distance), the nbond lookup, padding, and the every-pair list made on the CPU de
 import numpy as np
 import torch
 
-from dmff_b200.api.topology import CovalentMap
+from dmff_b200.api.topology import CovalentMap, covalent_rows
 from dmff_b200.common.nblist import NoCutoffNeighborList, NoPeriodicNeighborList, _nbond_lookup, _padded
 
 
@@ -85,3 +85,15 @@ def test_padding_capacity_grows_and_stays():
     assert _padded(nl, r, 4).shape[0] == 13
     assert _padded(nl, torch.zeros((20, 3), dtype=torch.int32), 4).shape[0] == 20
     assert _padded(nl, r, 4).shape[0] == 20
+
+
+def test_sparse_nbond_lookup_matches_dense_on_a_random_graph():
+    rng = np.random.default_rng(17)
+    n = 300
+    bonds = [(k, int(rng.integers(0, k))) for k in range(1, n)]  # a random tree
+    cov = CovalentMap(n, covalent_rows(n, bonds, 3))  # each pair once, distances 1..3
+    dense = np.zeros((n, n), dtype=np.int64)
+    for a, b, d in cov.pairs():
+        dense[a, b] = dense[b, a] = d
+    i, j = torch.triu_indices(n, n, 1)
+    assert np.array_equal(_nbond_lookup(cov, n, i, j).numpy(), dense[i.numpy(), j.numpy()])
