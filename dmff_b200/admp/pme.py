@@ -13,10 +13,9 @@ import numpy as np
 import torch
 
 from ..engine import AdmpEngine
+from .settings import MAX_N_POL, POL_CONV
 
 DIELECTRIC = 1389.35455846
-POL_CONV = 1.0  # dmff/admp/settings.py:2
-MAX_N_POL = 30  # dmff/admp/settings.py:3
 
 
 def setup_ewald_parameters(rc, ethresh, box=None, spacing=None, method="openmm"):

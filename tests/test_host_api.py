@@ -151,6 +151,7 @@ DROP_IN_IMPORTS = [
     ("api.hamiltonian", ["Hamiltonian", "Potential", "build_covalent_map"]),
     ("admp.pme", ["ADMPPmeForce", "setup_ewald_parameters", "DIELECTRIC"]),
     ("admp.disp_pme", ["ADMPDispPmeForce"]),
+    ("admp.settings", ["POL_CONV", "MAX_N_POL"]),
     ("admp.pairwise", ["generate_pairwise_interaction", "TT_damping_qq_c6_kernel", "TT_damping_qq_kernel",
                        "distribute_scalar", "distribute_v3", "distribute_matrix"]),
     ("admp.spatial", ["pbc_shift", "v_pbc_shift", "normalize", "generate_construct_local_frames",
