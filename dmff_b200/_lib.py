@@ -29,7 +29,7 @@ DMFFB_SOLVER_REFERENCE = 1
 EXPORTED = [
     "dmffb_admp_create", "dmffb_admp_reconfigure", "dmffb_destroy", "dmffb_last_error", "dmffb_admp_set_params",
     "dmffb_admp_compute", "dmffb_admp_compute_host", "dmffb_admp_field", "dmffb_admp_multipole_grads",
-    "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_get_timings", "dmffb_set_timing",
+    "dmffb_build_neighbors", "dmffb_admp_build_neighbors", "dmffb_engine_pairs", "dmffb_get_timings", "dmffb_set_timing",
     "dmffb_set_profiling", "dmffb_get_kernel_stats", "dmffb_get_counters", "dmffb_build_neighbors_noalloc",
     "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads", "dmffb_disp_set_param_grads",
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
@@ -233,6 +233,7 @@ def load():
     lib.dmffb_admp_param_grads.argtypes = [vp, vp, vp, vp, vp, vp]
     lib.dmffb_build_neighbors.argtypes = [vp, vp, vp, vp, dbl, vp, i64, P(i64)]
     lib.dmffb_admp_build_neighbors.argtypes = [vp, vp, vp, vp]
+    lib.dmffb_engine_pairs.argtypes = [vp, vp, vp, i64, P(i64)]
     lib.dmffb_get_timings.argtypes = [vp, P(dbl), i32]
     lib.dmffb_set_timing.argtypes = [vp, i32]
     lib.dmffb_set_profiling.argtypes = [vp, i32]

@@ -2207,6 +2207,21 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     return DMFFB_OK;
 }
 
+int dmffb_engine_pairs(dmffb_engine* h, void* stream, int32_t* pairs_out, int64_t capacity, int64_t* npairs_out) {
+    if (!h || !npairs_out) return fail(h, DMFFB_BAD_ARG, "null argument");
+    if (!h->have_pairs) return fail(h, DMFFB_BAD_ARG, "the engine has no neighbour list yet");
+    cudaStream_t s = (cudaStream_t)stream;
+    *npairs_out = h->npairs;
+    if (h->npairs > capacity || (!pairs_out && h->npairs > 0)) {
+        h->err = "pair capacity too small";
+        return DMFFB_NEIGHBOR_OVERFLOW;
+    }
+    if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
+    if (h->npairs > 0)
+        CK(cudaMemcpyAsync(pairs_out, h->d_pairs, (size_t)h->npairs * 3 * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    return DMFFB_OK;
+}
+
 int dmffb_disp_create(const dmffb_disp_desc* d, dmffb_engine** out) {
     if (!d || !out) return DMFFB_BAD_ARG;
     *out = nullptr;

@@ -158,16 +158,21 @@ extern "C" int dmffb_build_neighbors_noalloc(void* stream, const double* pos, in
         if (cudaMemsetAsync(cell_count, 0, (size_t)(ncell + 1) * 4, s) != cudaSuccess) return DMFFB_CUDA_ERROR;
         if (cudaMemsetAsync(cell_cursor, 0, (size_t)(ncell + 1) * 4, s) != cudaSuccess) return DMFFB_CUDA_ERROR;
         k_cell_count<<<nb(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], atom_cell, cell_count);
+        if (cudaGetLastError() != cudaSuccess) return DMFFB_CUDA_ERROR;
         size_t tb = kScanTempBytes;
         if (cub::DeviceScan::ExclusiveSum(temp, tb, cell_count, cell_start, ncell + 1, s) != cudaSuccess)
             return DMFFB_CUDA_ERROR;
         k_cell_fill<<<nb(n, 256), 256, 0, s>>>(n, atom_cell, cell_start, cell_cursor, cell_atoms);
+        if (cudaGetLastError() != cudaSuccess) return DMFFB_CUDA_ERROR;
         a.cell_start = cell_start;
         a.cell_atoms = cell_atoms;
         k_pairs_warp<0><<<nb((int64_t)n * 32, 256), 256, 0, s>>>(a);
     } else {
         k_pairs_all<0><<<nb(n, 128), 128, 0, s>>>(a);
     }
+    // a failed launch here would leave the count pass undone and the total below stale (the
+    // array keeps the previous call's offsets), so check before reading it
+    if (cudaGetLastError() != cudaSuccess) return DMFFB_CUDA_ERROR;
     size_t tb = kScanTempBytes;
     if (cub::DeviceScan::InclusiveSum(temp, tb, count, offsets + 1, n, s) != cudaSuccess) return DMFFB_CUDA_ERROR;
     int64_t total = 0;

@@ -267,6 +267,18 @@ class AdmpEngine:
         self._check(self.lib.dmffb_admp_build_neighbors(self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos),
                                                         b.ctypes.data_as(ctypes.c_void_p)))
 
+    def internal_pairs(self):
+        """The engine's own neighbour list (built by ``rebuild_internal_pairs`` or the first
+        compute without pairs) as a cuda int32 [np, 3] tensor, rows sorted by i."""
+        s = torch.cuda.current_stream(self.device)
+        need = ctypes.c_int64(0)
+        self._check(self.lib.dmffb_engine_pairs(self.h, ctypes.c_void_p(s.cuda_stream), None, 0, ctypes.byref(need)),
+                    allow=(L.DMFFB_NEIGHBOR_OVERFLOW,))
+        buf = torch.empty((max(need.value, 1), 3), dtype=torch.int32, device=self.device)
+        self._check(self.lib.dmffb_engine_pairs(self.h, ctypes.c_void_p(s.cuda_stream), _dev(buf), buf.shape[0],
+                                                ctypes.byref(need)))
+        return buf[: need.value]
+
     def set_timing(self, on=True):
         self.lib.dmffb_set_timing(self.h, int(on))
 
@@ -337,6 +349,7 @@ class DispEngine:
     _box = staticmethod(AdmpEngine._box)
     rebuild_internal_pairs = AdmpEngine.rebuild_internal_pairs
     build_neighbors = AdmpEngine.build_neighbors
+    internal_pairs = AdmpEngine.internal_pairs
     set_profiling = AdmpEngine.set_profiling
     kernel_stats = AdmpEngine.kernel_stats
 
@@ -431,6 +444,7 @@ class ClassicalEngine:
     _box = staticmethod(AdmpEngine._box)
     rebuild_internal_pairs = AdmpEngine.rebuild_internal_pairs
     build_neighbors = AdmpEngine.build_neighbors
+    internal_pairs = AdmpEngine.internal_pairs
     set_profiling = AdmpEngine.set_profiling
     kernel_stats = AdmpEngine.kernel_stats
     counters = AdmpEngine.counters

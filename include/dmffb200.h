@@ -150,6 +150,13 @@ int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, cons
 /* Rebuild the engine-owned pair list used when compute() gets pairs == NULL. */
 int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box);
 
+/* Copy of the engine's own neighbour list (the rows compute() uses when pairs == NULL), the
+ * counterpart of the reference's NeighborList.pairs property (dmff/common/nblist.py:62-64) without
+ * its padding rows: npairs rows (i, j, nbond), i < j, sorted by i, written to pairs_out (device,
+ * capacity rows) on the given stream after the last build.  *npairs_out = the row count;
+ * DMFFB_NEIGHBOR_OVERFLOW when capacity is short (nothing written). */
+int dmffb_engine_pairs(dmffb_engine* h, void* stream, int32_t* pairs_out, int64_t capacity, int64_t* npairs_out);
+
 /* Per-stage device times of the last compute() in milliseconds (CUDA events):
  * [0] frames, [1] pol solve, [2] real FULL, [3] recip FULL, [4] self+frames, [5] total. */
 int dmffb_get_timings(const dmffb_engine* h, double* ms_out, int32_t n);
@@ -345,11 +352,13 @@ void dmffb_server_destroy(dmffb_server* srv);
  *     cov_j[cov_ptr[i] .. cov_ptr[i+1]-1] with nbond cov_nb[...]); all three NULL means nbond 0.
  *   pairs_out: device [capacity*3] rows (i, j, nbond), i < j, sorted by i; *npairs_out = count.
  * Limits: n_atoms <= DMFFB_NOALLOC_MAX_ATOMS (larger -> DMFFB_SCRATCH_TOO_SMALL); the cell grid
- * is coarsened to at most DMFFB_NOALLOC_MAX_CELLS cells.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  Every call on a device shares the one array and each call
- * re-zeroes what it accumulates into; calls that overlap on the GPU (different streams, or
- * host threads) race on it and must be serialized by the caller. */
+ * is coarsened to at most DMFFB_NOALLOC_MAX_CELLS cells.  The first call on a device does a
+ * one-time set-up: it looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture begins.  Every call reads the pair
+ * count back to the host and waits for its stream to finish before it returns.  Every call on a
+ * device shares the one array and each call re-zeroes what it accumulates into; calls that
+ * overlap on the GPU (different streams, or host threads) race on it and must be serialized by
+ * the caller. */
 #define DMFFB_NOALLOC_MAX_ATOMS 65536
 #define DMFFB_NOALLOC_MAX_CELLS 32768
 int dmffb_build_neighbors_noalloc(void* stream, const double* pos, int32_t n_atoms, const double* box, double rc,

@@ -1133,6 +1133,10 @@ def brute_force_pairs(positions, box, rc, nbond_of=None):
         r2 = e[0] * e[0] + e[1] * e[1]
         r2 = r2 + e[2] * e[2]
         js = np.nonzero(np.sqrt(r2) < rc)[0] + i + 1
-        for j in js:
-            out.append((i, j, 0 if nbond_of is None else nbond_of(i, j)))
-    return np.asarray(out, dtype=np.int64).reshape(-1, 3)
+        if nbond_of is None:
+            out.append(np.stack([np.full(len(js), i, dtype=np.int64), js, np.zeros(len(js), dtype=np.int64)], 1))
+        else:
+            out.append(np.asarray([(i, j, nbond_of(i, j)) for j in js], dtype=np.int64).reshape(-1, 3))
+    if not out:
+        return np.zeros((0, 3), dtype=np.int64)
+    return np.concatenate(out, axis=0).astype(np.int64)

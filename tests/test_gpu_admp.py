@@ -20,11 +20,20 @@ def _run(eng, sysd, pairs):
     return res, F.cpu().numpy(), U.cpu().numpy()
 
 
+# the float64 oracle's energy of the c0_small fixture, reproduced bit for bit on every host it has
+# been run on (any thread count); a host whose CPU arithmetic gives another value cannot check the
+# FP64 tolerances below, and says so here instead of failing them
+C0_SMALL_ORACLE_E = -398.00509400279407
+
+
 @pytest.fixture(scope="module")
 def c0_small():
     s = water_box(64, 12.4, seed=10, lmax=2, pol=False, rc=6.0)
     pr = oracle_pairs(s)
-    return s, pr, oracle_reference(s, pr)
+    ref = oracle_reference(s, pr)
+    assert abs(ref["E"] - C0_SMALL_ORACLE_E) <= 1e-12 * abs(C0_SMALL_ORACLE_E), (
+        f"the float64 oracle is not reproducible on this host: {ref['E']!r} != {C0_SMALL_ORACLE_E!r}")
+    return s, pr, ref
 
 
 @pytest.fixture(scope="module")

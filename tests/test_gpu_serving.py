@@ -100,3 +100,29 @@ def test_arrival_times_are_respected(systems):
     for r in reqs:
         assert r.c.t_start >= r.c.t_arrival - 1e-6
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+
+
+LARGE = [1000, 2500, 5000, 10000, 100, 150]
+
+
+def test_large_requests_same_alone_and_in_the_mix_and_fp64():
+    """The serving stream's upper end (up to 10000 waters / 30000 atoms, 66.9 A boxes) mixed with
+    small boxes: each result is the same alone and in the mix within the FP32 tolerances, and the
+    FP32 server matches the FP64 one-at-a-time path."""
+    systems = [serving_system(n, 100 + k) for k, n in enumerate(LARGE)]
+    cap = 3 * max(LARGE)
+    srv = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp32")
+    alone = _run(srv, systems)[0]
+    srv.close()
+    srv = AdmpServer(n_slots=4, capacity_atoms=cap, precision="fp32")
+    mix = _run(srv, systems)[0]
+    srv.close()
+    assert len({r.c.slot for r in mix}) > 1
+    srv = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp64", cg_tol=1e-8, use_graphs=False)
+    plain = _run(srv, systems)[0]
+    srv.close()
+    for a, b, p in zip(alone, mix, plain):
+        assert abs(a.energy - b.energy) <= 1e-5 * abs(a.energy)
+        assert rel_force_rms(b.forces, a.forces) < 1e-4
+        assert abs(a.energy - p.energy) <= 1e-5 * abs(p.energy)
+        assert rel_force_rms(a.forces, p.forces) < 1e-4

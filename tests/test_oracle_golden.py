@@ -70,6 +70,44 @@ def test_dimer_nonpol_and_mono_are_exact():
     assert abs(E1 - GOLD["dimer_pol_lmax0_steppol5"]["value"]) < 1e-9
 
 
+def test_dimer_lmax2_pol_golden_lies_below_the_energy_minimum():
+    """The lmax-2 polarizable dimer golden (tests/test_admp/test_compute.py:55, asserted there to one
+    decimal) cannot come from the reference's current energy function: the 5-step fixed-point
+    iteration is converged (6 to 30 steps agree to 1e-10), the energy is a minimum in the induced
+    dipoles (random displacements of the converged dipoles only raise it), and that minimum lies
+    0.040 kJ/mol above the golden.  The same restated function reproduces the dimer's lmax-0
+    polarizable and lmax-2 non-polarizable goldens to 1e-9 and the 996-water polarizable PME box to
+    7.5e-7, so the golden dates from another version of the reference's code or data."""
+    pdb = PDBFile(_data("water_dimer.pdb"))
+    top, box_nm = pdb.topology, pdb.topology.getPeriodicBoxVectors()
+    E5, U5, _ = oracle_from_xml(_data("admp.xml"), top, pdb.positions, box_nm, 0.4, "CutoffPeriodic", 5)
+    E30, U30, _ = oracle_from_xml(_data("admp.xml"), PDBFile(_data("water_dimer.pdb")).topology, pdb.positions,
+                                  box_nm, 0.4, "CutoffPeriodic", 30)
+    assert abs(E5 - E30) < 1e-9
+    # energy at displaced dipoles: rebuild the oracle's energy function for the same system
+    H = Hamiltonian(_data("admp.xml"))
+    pot = H.createPotential(PDBFile(_data("water_dimer.pdb")).topology, nonbondedMethod="CutoffPeriodic",
+                            nonbondedCutoff=0.4, ethresh=5e-4, step_pol=30)
+    g = H.generators["ADMPPmeForce"]
+    pf = g.pme_force
+    P = H.paramset["ADMPPmeForce"]
+    mp = torch.as_tensor(pot.meta["ADMPPmeForce_map_poltype"])
+    pos, box = torch.tensor(pdb.positions * 10), torch.tensor(box_nm * 10)
+    cov = top.buildCovMat()
+    pairs = R.brute_force_pairs(pos.numpy(), box.numpy(), pf.rc, lambda i, j: int(cov.lookup(i, j)))
+    f = R.ADMPPmeForce(box.numpy(), pf.axis_type, pf.axis_indices, pf.rc, 5e-4, pf.lmax, True, lpme=False)
+    args = (pos, box, pairs, P["Q_local"][torch.as_tensor(pf.map_atomtype)])
+    rest = (P["pol"][mp], P["thole"][mp], torch.tensor(g.mScales), torch.tensor(g.pScales), torch.tensor(g.dScales))
+    Emin = f.energy_fn(*args, U30, *rest).item()
+    rng = np.random.default_rng(0)
+    polar = (P["pol"][mp] > 0).numpy()[:, None]
+    for _ in range(8):
+        dU = torch.tensor(rng.normal(0.0, 1e-3, size=U30.shape) * polar)
+        assert f.energy_fn(*args, U30 + dU, *rest).item() > Emin
+    gold = GOLD["dimer_pol_lmax2_steppol5"]["value"]
+    assert gold < Emin - 0.03
+
+
 def _waterbox_topology():
     d = np.load(_data("waterbox_996.npz"))
     t = DMFFTopology()
