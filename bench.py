@@ -1,10 +1,15 @@
 """Benchmark of the ADMP polarizable PME energy/force/virial step on B200.
 
-Workload (default): 4096 rigid waters (12288 atoms) in a 49.7 A box, lmax=2 multipoles with
-local frames, isotropic polarizabilities (O 1.0, H 0.5 A^3), Thole 0.33, rc = 8 A,
+Workload (default, the headline line): 4096 rigid waters (12288 atoms) in a 49.7 A box, lmax=2
+multipoles with local frames, isotropic polarizabilities (O 1.0, H 0.5 A^3), Thole 0.33, rc = 8 A,
 ethresh = 5e-4 (kappa 0.3285/A, 50^3 mesh); seeded synthetic coordinates and parameters.
 One step = cell-list neighbour rebuild + induced-dipole CG solve (from U = 0) + energy,
 forces and box gradient, FP32 pair / mesh arithmetic with FP64 accumulation.
+
+The same line carries two more measurements of this path at N = 1:
+  "c4": the 100 000-atom classical polymer + water box (LJ + Coulomb PME + bonded, rc 10 A);
+  "c3": the serving stream (2000 polarizable water boxes of 100-10000 molecules, Poisson
+        arrivals at 50 ... 2000 requests/s) on the batched FP32 server and on the plain FP64 path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -28,6 +33,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "atom-evals/s"
 L2_FLUSH_BYTES = 256 << 20
+POL_CONV, MAX_N_POL = 1.0, 30  # the reference's dipole iteration limits (dmff/admp/settings.py:2-3)
 
 
 def parse():
@@ -36,24 +42,27 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="c1")
+    p.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c4"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--serving-requests", type=int, default=300,
+    p.add_argument("--no-c4", action="store_true", help="skip the classical 100k-atom sub-measurement")
+    p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the serving stream measured beside the step (0: skip)")
-    p.add_argument("--serving-rates", default="100,500,2000", help="Poisson arrival rates (req/s)")
+    p.add_argument("--serving-rates", default="50,100,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     p.add_argument("--serving-slots", type=int, default=12)
     p.add_argument("--serving-budget-gb", type=float, default=2.0)
     return p.parse_args()
 
 
-def workload_config(name, s, K):
+def workload_config(name, s, world=1):
+    """config of the JSON line; the same keys on both arms."""
     return {"workload": {"c1": "polarizable ADMP water box, 4096 waters / 12288 atoms, 49.7 A, rc 8 A",
                          "c0": "ADMP water box, 216 waters / 648 atoms, 18.6 A, rc 6 A, no polarization",
                          "c2": "polarizable ADMP water box, 2048 waters / 6144 atoms, 40 A, rc 8 A"}[name],
             "n_atoms": int(s["n_atoms"]), "lmax": int(s["lmax"]), "polarizable": bool(s["lpol"]),
-            "rc_A": s["rc"], "ethresh": s["ethresh"], "pme_mesh": list(s["K"]),
+            "rc_A": s["rc"], "ethresh": s["ethresh"], "pme_mesh": [int(k) for k in s["K"]],
             "cg_tol_rel": 1e-6, "l2": "flushed between timed steps (256 MiB write)",
-            "step": "cell-list rebuild + CG dipole solve from U=0 + energy/forces/box gradient"}
+            "step": "cell-list rebuild + dipole solve from U=0 + energy/forces/box gradient",
+            "parallelism": f"replicas x{world}"}
 
 
 # ---------------------------------------------------------------------------------- clocks
@@ -106,104 +115,162 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-# DRAM bytes per launch from one ncu capture of this workload (profiles/kernels_admp_pol_12288.md:
-# dram__bytes_read.sum + dram__bytes_write.sum, 12288-atom polarizable step)
-NCU_DRAM_BYTES = {"pair_matvec": 33.11e6, "spread": 2.77e6, "neighbors": 0.5 * (0.52e6 + 2.79e6)}
+def measure_fp32_peak(dev):
+    """FP32 CUDA-core throughput measured in this run: cuBLAS SGEMM 8192^3 with TF32 off (FFMA
+    only), best of 5 (TFLOP/s).  The pair kernels are FP32 CUDA-core code, so this is their bound."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn((n, n), device=dev, dtype=torch.float32)
+        b = torch.randn((n, n), device=dev, dtype=torch.float32)
+        c = a @ b
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b, out=c)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        del a, b, c
+        return 2.0 * n ** 3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
 
 
-def roofline(stats, s, npairs, peaks, peak_src):
-    """Roofline of the CG matvec (k_matvec_apply: the kernel with the largest share of the step in
-    the ncu launch list, profiles/launches_admp_pol_12288.md), plus every kernel class's achieved
-    rate against its bound.  Algorithmic work per launch (fixed convention): matvec 12 B per CSR
-    entry (2 entries per pair: packed j + two FP32 coefficients); pair FULL polarizable 1900
-    flop/pair, FIELD 600 flop/pair; spread N(12 + 4(l+1)^2) + 4K^3 B; gather 4K^3 + N(12 + 4(l+1)^2
-    + 24) B; convolution 16 K^3 B; neighbour build 12N + 12 Np B."""
-    n = s["n_atoms"]
-    K3 = float(np.prod(s["K"]))
-    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12  # TFLOP/s, nominal at max clock
-    models = {"pair_matvec": ("hbm", 12.0 * 2 * npairs), "pair_full": ("fp32", 1900.0 * npairs),
-              "pair_field": ("fp32", 600.0 * npairs), "spread": ("hbm", n * (12 + 4 * 9) + 4 * K3),
-              "gather_full": ("hbm", 4 * K3 + n * (12 + 4 * 9 + 24)), "gather_field": ("hbm", 4 * K3 + n * (12 + 16 + 24)),
-              "conv": ("hbm", 16 * K3), "neighbors": ("hbm", 12 * n + 12 * npairs)}
+def class_rooflines(stats, steps, work, fp32_peak, hbm_peak):
+    """Per kernel class: launches per step, device time per step and per launch (CUDA events around
+    every launch of that class, summed over ``steps`` instrumented steps), and the achieved rate of
+    its algorithmic work per launch against its bound.  ``work[cls] = (bound, units per launch)``
+    with bound 'fp32' (flop) or 'hbm' (bytes)."""
     out = {}
-    for cls, (bound, work) in models.items():
-        ms, launches = stats.get(cls, (0.0, 0))
+    total = sum(v[0] for v in stats.values())
+    for cls, (ms, launches) in stats.items():
         if launches == 0:
             continue
         per = ms / 1e3 / launches
-        if bound == "fp32":
-            ach = work / per / 1e12
-            out[cls] = {"bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
-                        "avg_launch_us": per * 1e6, "launches": launches}
-        else:
-            ach = work / per / 1e9
-            out[cls] = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                        "frac": ach / peaks["hbm_gbs"], "avg_launch_us": per * 1e6, "launches": launches}
-    main = dict(out["pair_matvec"], kernel="k_matvec_apply (CG matvec)", traffic=NCU_DRAM_BYTES["pair_matvec"],
-                peak_source=f"hbm_gbs ({peak_src})",
-                traffic_source="ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, this workload")
-    main["by_class"] = {k: {"frac": round(v["frac"], 4), "achieved": round(v["achieved"], 2), "unit": v["unit"],
-                            "avg_launch_us": round(v["avg_launch_us"], 2)} for k, v in out.items()}
-    return main
+        row = {"ms_per_step": round(ms / steps, 4), "launches_per_step": launches / steps,
+               "avg_launch_us": round(per * 1e6, 2), "share": round(ms / total, 4) if total else None}
+        if cls in work and work[cls][1] > 0:
+            bound, units = work[cls]
+            if bound == "fp32":
+                ach = units / per / 1e12
+                row.update(bound="fp32", achieved=round(ach, 3), unit="TFLOP/s", frac=round(ach / fp32_peak, 4))
+            elif bound == "fp64":
+                ach = units / per / 1e12
+                row.update(bound="fp64 (rows with a topological scale)", achieved=round(ach, 3), unit="TFLOP/s")
+            else:
+                ach = units / per / 1e9
+                row.update(bound="hbm", achieved=round(ach, 1), unit="GB/s", frac=round(ach / hbm_peak, 4))
+        out[cls] = row
+    return out
+
+
+def admp_work(s, n_pairs, n_scaled):
+    """Algorithmic work per launch of each class for a polarizable ADMP step (fixed convention:
+    FMA = 2 flop, exp / erf / erfc / sqrt / div = 1 flop): pair FULL polarizable 1900 flop/pair,
+    FIELD 600 flop/pair, the CG matvec 12 B per CSR entry (two entries per pair: packed j + two
+    FP32 coefficients), its coefficient set-up 200 flop/pair, dipole spread N(12 + 4*4) + 4K^3 B,
+    field gather 4K^3 + N(12 + 4*4 + 24) B, convolution 16 K^3 B, neighbour build 12N + 12Np B per
+    step (its launches share it).  Pair classes count the rows they run over: the FP32 launches
+    take the unscaled rows, the FP64 launches the n_scaled rows with a topological scale."""
+    n = s["n_atoms"]
+    K3 = float(np.prod(s["K"]))
+    un = n_pairs - n_scaled
+    return {"pair_full": ("fp32", 1900.0 * un), "pair_field": ("fp32", 600.0 * un),
+            "pair_full_scaled": ("fp64", 1900.0 * n_scaled), "pair_field_scaled": ("fp64", 600.0 * n_scaled),
+            "pair_matvec": ("hbm", 12.0 * 2 * n_pairs), "matvec_coef": ("fp32", 200.0 * n_pairs),
+            "spread": ("hbm", n * (12 + 4 * 4) + 4 * K3), "gather_field": ("hbm", 4 * K3 + n * (12 + 16 + 24)),
+            "conv": ("hbm", 16 * K3)}
+
+
+def headline_roofline(classes, per_launch_bytes, traffic, peak, peak_src, kernel, cls):
+    """The roofline object of the line: the dominant kernel's achieved rate of algorithmic bytes
+    per launch (live CUDA events over the instrumented steps) against the measured HBM peak."""
+    row = classes[cls]
+    ach = per_launch_bytes / (row["avg_launch_us"] * 1e-6) / 1e9
+    return {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+            "traffic": traffic, "kernel": kernel, "kernel_class": cls, "avg_launch_us": row["avg_launch_us"],
+            "share_of_step": row["share"], "peak_source": f"hbm_gbs ({peak_src})"}
 
 
 # ---------------------------------------------------------------------------------- CPU side
-def cpu_reference_timing(s, n_ref_iter, want_ef=True):
-    """Float64 CPU restatement of the reference path (the oracle) on all host threads: one dE/dU
-    pass (the unit of the dipole solve) and one energy+forces pass of the same workload."""
+def cpu_sample_system():
+    """The bounded CPU sample of the c1 workload: 512 waters (1536 atoms) in a 24.85 A box, the same
+    density, seed, force field, rc 8 A and ethresh (so the same kappa and mesh spacing, 25^3)."""
+    from dmff_b200.synthetic import water_box
+    return water_box(512, 49.7 / 2, seed=1, lmax=2, pol=True, rc=8.0)
+
+
+def cpu_reference_evaluation(s, f, pr, tensors):
+    """One complete evaluation by the reference's own algorithm, restated in float64 (the oracle):
+    the fixed-point dipole iteration to POL_CONV (max |dE/dU| < 1 over sites with pol > 0.001,
+    at most MAX_N_POL steps, dmff/admp/pme.py:373-401) from U = 0, then energy + forces + box
+    gradient by autograd (jax.value_and_grad over positions and box, pme.py:339).  Returns
+    (seconds, iterations)."""
+    import torch
+    Ql, pol, th, ms, ps, ds = tensors
+    t0 = time.perf_counter()
+    pos = torch.tensor(s["pos"])
+    box = torch.tensor(s["box"])
+    U, _, n_it = f.optimize_Uind(pos, box, pr, Ql, pol, th, ms, ps, ds, steps_pol=None, maxiter=MAX_N_POL,
+                                 thresh=POL_CONV)
+    p = pos.clone().requires_grad_(True)
+    b = box.clone().requires_grad_(True)
+    E = f.energy_fn(p, b, pr, Ql, U.detach(), pol, th, ms, ps, ds)
+    torch.autograd.grad(E, (p, b))
+    return time.perf_counter() - t0, int(n_it)
+
+
+def cpu_reference_runner():
+    """Set-up of the CPU sample (untimed: pair list and parameters); returns a callable that runs
+    one timed evaluation, and the thread count used."""
     import torch
     import oracle.admp_ref as R
     from dmff_b200.synthetic import pairs_nbond
     torch.set_num_threads(os.cpu_count())
+    s = cpu_sample_system()
     pr = R.brute_force_pairs(s["pos"], s["box"], s["rc"])
     pr[:, 2] = pairs_nbond(pr, s["cov_rows"], s["n_atoms"])
     f = R.ADMPPmeForce(s["box"], s["axis_types"], s["axis_indices"], s["rc"], s["ethresh"], s["lmax"], s["lpol"],
                        kappa=s["kappa"], K=s["K"])
-    Ql = torch.tensor(s["Q_local"])
-    rest = (torch.tensor(s["pol"]), torch.tensor(s["thole"]), torch.tensor(s["mscales"]),
-            torch.tensor(s["pscales"]), torch.tensor(s["dscales"]))
-    pos = torch.tensor(s["pos"])
-    box = torch.tensor(s["box"])
-    U0 = torch.zeros((s["n_atoms"], 3), dtype=torch.float64)
-    t0 = time.perf_counter()
-    f.grad_U(pos, box, pr, Ql, U0, *rest)
-    t_g = time.perf_counter() - t0
-    t_ef = None
-    if want_ef:
-        p = pos.clone().requires_grad_(True)
-        b = box.clone().requires_grad_(True)
-        t0 = time.perf_counter()
-        E = f.energy_fn(p, b, pr, Ql, U0, *rest)
-        torch.autograd.grad(E, (p, b))
-        t_ef = time.perf_counter() - t0
-    return t_g, t_ef, torch.get_num_threads()
+    tensors = (torch.tensor(s["Q_local"]), torch.tensor(s["pol"]), torch.tensor(s["thole"]),
+               torch.tensor(s["mscales"]), torch.tensor(s["pscales"]), torch.tensor(s["dscales"]))
+    return s, (lambda: cpu_reference_evaluation(s, f, pr, tensors)), torch.get_num_threads()
 
 
-def run_reference(args, s, rank):
-    """--impl reference: the reference's own CPU path (float64 oracle restatement; the JAX
-    reference cannot be installed here) on the host cores, same workload/metric/unit."""
+def cpu_sample_text(s, iters, secs):
+    return (f"complete evaluations of a {s['n_atoms']}-atom sample of the workload ({s['n_atoms'] // 3} waters, "
+            f"24.85 A, same density / rc / ethresh, {s['K'][0]}^3 mesh) by the float64 restatement of the "
+            f"reference: fixed-point dipole iteration to POL_CONV 1.0 (max {MAX_N_POL} steps; took "
+            f"{statistics.median(iters):.0f}) + energy/forces/box gradient by autograd; median "
+            f"{statistics.median(secs):.2f} s per evaluation")
+
+
+def run_reference(args, s_full, rank):
+    """--impl reference: the reference's own CPU algorithm for the path (float64 restatement; JAX
+    is not installed) on all host cores, on a bounded sample of the workload; every step is one
+    complete, timed evaluation."""
     if rank != 0:
         return
-    n_ref_iter = 30  # the reference's MAX_N_POL (dmff/admp/settings.py:3)
-    warm = min(args.warmup, 1)
-    steps = min(args.steps, 3)
-    t_ef = None
-    for _ in range(max(warm, 1)):
-        _, t_ef, cores = cpu_reference_timing(s, n_ref_iter, want_ef=True)
-    tg = []
-    for _ in range(steps):
-        g, _, cores = cpu_reference_timing(s, n_ref_iter, want_ef=False)
-        tg.append(g)
-    t_eval = t_ef + n_ref_iter * statistics.median(tg)
-    value = s["n_atoms"] / t_eval
-    sample = (f"per step: one dE/dU pass of the {s['n_atoms']}-atom box (median of {steps}); one energy+forces "
-              f"pass timed in warm-up ({t_ef:.2f} s); evaluation = E+F + {n_ref_iter} dE/dU passes "
-              f"(the reference's MAX_N_POL)")
+    s, run, cores = cpu_reference_runner()
+    for _ in range(args.warmup):
+        run()
+    secs, iters = [], []
+    for _ in range(args.steps):
+        t, it = run()
+        secs.append(t)
+        iters.append(it)
+    total = sum(secs)
+    value = args.steps * s["n_atoms"] / total
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": args.gpus,
-           "steps": steps, "warmup": warm, "ms_per_step": t_eval * 1e3, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": workload_config(args.workload, s, s["K"]),
-           "cpu_baseline": {"value": value, "unit": "atom-evals/s", "cores": cores, "kind": "port", "sample": sample},
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": workload_config(args.workload, s_full, args.gpus),
+           "cpu_baseline": {"value": value, "unit": "atom-evals/s", "cores": cores, "kind": "port",
+                            "sample": cpu_sample_text(s, iters, secs)},
            "e2e": {"value": value, "unit": "atom-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -216,12 +283,31 @@ def make_serving_systems(n_req, seed=3):
     from dmff_b200.synthetic import serving_sizes, serving_system
     sizes = serving_sizes(2000, seed=seed)[:n_req]
     with mp.get_context("spawn").Pool(max(1, min(os.cpu_count() or 1, 32))) as pool:
-        return pool.starmap_async(serving_system, [(int(n), k) for k, n in enumerate(sizes)]).get(timeout=900)
+        return pool.starmap_async(serving_system, [(int(n), k) for k, n in enumerate(sizes)]).get(timeout=1800)
 
 
-def bench_serving(args, systems, dev):
-    """Continuous-batching FP32 server vs the plain FP64 path (one request at a time, no graphs)
-    on the same requests; latency = completion - arrival."""
+def serving_ideal_seconds(systems, iters, peaks, fp32_peak):
+    """Ideal time t* of a set of polarizable evaluations (fixed convention): FP32 pair flops at the
+    FP32 peak plus the memory-bound stages' bytes at the HBM peak.  Per request: pairs Np from the
+    molecule density (0.1002 atoms/A^3 within rc), flops 1900 Np (FULL) + 600 Np (FIELD) + 200 Np
+    (matvec set-up), bytes 12N + 12Np (neighbours) + per CG iteration 24 Np (matvec) + dipole spread
+    N*28 + 4K^3 + gather 4K^3 + N*52 + convolution 16 K^3, cuFFT counted as 2 x 2.5 K^3 log2 K^3
+    flops per iteration."""
+    flops = 0.0
+    byts = 0.0
+    for s, it in zip(systems, iters):
+        n = s["n_atoms"]
+        npairs = n * 0.5 * (4.0 / 3.0) * math.pi * s["rc"] ** 3 * 0.1002
+        K3 = float(np.prod(s["K"]))
+        flops += (1900 + 600 + 200) * npairs + it * 2 * 2.5 * K3 * math.log2(K3)
+        byts += 12 * n + 12 * npairs + it * (24 * npairs + 28 * n + 8 * K3 + 52 * n + 16 * K3)
+    return flops / (fp32_peak * 1e12) + byts / (peaks["hbm_gbs"] * 1e9)
+
+
+def bench_serving(args, systems, dev, peaks, fp32_peak):
+    """The serving stream: continuous-batching FP32 server (saturation and Poisson arrivals) and the
+    plain FP64 path (one request at a time, no graphs) on the same requests; latency = completion -
+    arrival."""
     from dmff_b200.serving import AdmpServer, ServingRequest
     from dmff_b200.synthetic import serving_arrivals
     cap = max(s["n_atoms"] for s in systems)
@@ -231,49 +317,46 @@ def bench_serving(args, systems, dev):
     warm = sorted(by_k.values(), key=lambda s: -s["n_atoms"])  # largest first: buffers grow once
     out = {"requests": len(systems), "atoms": int(sum(s["n_atoms"] for s in systems)),
            "sizes": "log-uniform 100-10000 waters (seed 3), 0.0334 molecules/A^3, rc 8 A (rc' = L/2 when L < 16 A)",
+           "small_boxes_rc_reduced": int(sum(1 for s in systems if s["rc"] < 8.0)),
            "slots": args.serving_slots, "hbm_budget_GB": args.serving_budget_gb,
            "cg_tol_rel": 1e-6, "step": "polarizable ADMP energy + forces + virial, host buffers in and out"}
     srv = AdmpServer(n_slots=args.serving_slots, capacity_atoms=cap, precision="fp32",
                      hbm_budget_bytes=int(args.serving_budget_gb * (1 << 30)), device=dev)
     srv.prewarm([ServingRequest(s) for s in warm])
-
-    def median_run(server, syss, repeats=3):
-        # a stream lasts a fraction of a second: report the median of a few runs (and all rates)
-        runs = [server.run_stream(syss, np.zeros(len(syss))) for _ in range(repeats)]
-        runs.sort(key=lambda r: r[1]["atom_evals_per_s"])
-        reqs_m, st_m = runs[len(runs) // 2]
-        return reqs_m, dict(st_m, runs_atom_evals_per_s=[round(r[1]["atom_evals_per_s"]) for r in runs])
-
-    reqs, st = median_run(srv, systems)
+    reqs, st = srv.run_stream(systems, np.zeros(len(systems)))
     out["offline_fp32"] = st
     fp32 = reqs
+    iters = [r.c.n_iter for r in reqs]
+    t_ideal = serving_ideal_seconds(systems, iters, peaks, fp32_peak)
+    out["roofline"] = {"model": "ideal time t* = FP32 pair flops / measured FP32 peak + stage bytes / measured "
+                                "HBM peak, summed over the requests (see serving_ideal_seconds)",
+                       "t_ideal_s": round(t_ideal, 4), "t_measured_s": round(st["wall_s"], 4),
+                       "frac": round(t_ideal / st["wall_s"], 4)}
     for rate in [float(x) for x in args.serving_rates.split(",") if x]:
         _, st = srv.run_stream(systems, serving_arrivals(len(systems), rate, seed=33))
         out[f"poisson_{int(rate)}_per_s"] = st
     srv.close()
-    # plain path: FP64, one slot, graphs off, every 5th request back to back
-    sub = systems[::5]
+    # plain path: FP64, one slot, graphs off, every request back to back
     plain = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp64", use_graphs=False, cg_tol=1e-6, device=dev)
     # the same warm-up as the server: one request per mesh shape, so that neither timed run
     # includes cuFFT plan creation
     plain.prewarm([ServingRequest(s) for s in warm])
-    preqs, pst = median_run(plain, sub)
+    preqs, pst = plain.run_stream(systems, np.zeros(len(systems)))
     plain.close()
-    out["plain_fp64"] = dict(pst, sample="every 5th request of the stream, one at a time")
+    out["plain_fp64"] = dict(pst, sample="every request of the stream, one at a time")
     out["speedup_vs_plain"] = out["offline_fp32"]["atom_evals_per_s"] / pst["atom_evals_per_s"]
     # the same plain path with the reference's own dipole iteration (fixed-point steps, POL_CONV 1.0,
     # MAX_N_POL 30, pme.py:342-423) in place of CG: the reference's algorithm run on this GPU
     plain_r = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp64", use_graphs=False, solver="reference",
-                         cg_tol=1.0, max_iter=30, device=dev)
+                         cg_tol=POL_CONV, max_iter=MAX_N_POL, device=dev)
     plain_r.prewarm([ServingRequest(s) for s in warm])
-    _, rst = median_run(plain_r, sub)
+    _, rst = plain_r.run_stream(systems, np.zeros(len(systems)))
     plain_r.close()
-    out["plain_fp64_reference_solver"] = dict(rst, sample="every 5th request of the stream, one at a time",
+    out["plain_fp64_reference_solver"] = dict(rst, sample="every request of the stream, one at a time",
                                               solver="fixed-point dipole iteration, POL_CONV 1.0, MAX_N_POL 30")
     out["speedup_vs_plain_reference_solver"] = out["offline_fp32"]["atom_evals_per_s"] / rst["atom_evals_per_s"]
     errs_e, errs_f = [], []
-    for k, p in enumerate(preqs):
-        q = fp32[5 * k]
+    for q, p in zip(fp32, preqs):
         errs_e.append(abs(q.energy - p.energy) / abs(p.energy))
         errs_f.append(float(np.sqrt(np.mean((q.forces - p.forces) ** 2)) / np.sqrt(np.mean(p.forces ** 2))))
     out["fp32_vs_fp64"] = {"max_rel_energy": float(max(errs_e)), "max_rel_force_rms": float(max(errs_f))}
@@ -281,32 +364,24 @@ def bench_serving(args, systems, dev):
 
 
 # ---------------------------------------------------------------------------------- classical
-def run_classical(args, rank, world, local):
-    """--workload c4: large classical system (200 chains x 50 beads + 30000 waters, 70 A box,
-    ~100k atoms): LJ + Coulomb PME (rc 10 A, ethresh 1e-5, 154^3 mesh) + harmonic bonds / angles
-    + 3-term torsions.  One step = cell-list rebuild + energy / forces / box gradient, FP32 pair
-    and mesh arithmetic with FP64 accumulation.  --impl reference: the float64 oracle on a bounded
-    sample of pair rows (extrapolated per pair) plus the bonded terms and reciprocal part."""
-    import torch
+def c4_system():
     from dmff_b200.synthetic import polymer_water_box
-    s = polymer_water_box(200, 50, 30000, 70.0, seed=4, rc=10.0, ethresh=1e-5)
-    cfg = {"workload": "classical polymer + water, 200 x 50 beads + 30000 waters / 100000 atoms, 70 A, rc 10 A",
-           "n_atoms": int(s["n_atoms"]), "pme_mesh": list(s["K"]), "ethresh": s["ethresh"],
-           "terms": "LJ (LB) + Coulomb PME + harmonic bonds/angles + periodic torsions",
-           "l2": "inputs larger than L2 (pair list ~0.7 GB)", "step": "cell-list rebuild + energy/forces/box gradient"}
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        out = classical_cpu_reference(s, cfg, args)
-        print(json.dumps(out), flush=True)
-        return
+    return polymer_water_box(200, 50, 30000, 70.0, seed=4, rc=10.0, ethresh=1e-5)
+
+
+C4_CFG = {"workload": "classical polymer + water, 200 x 50 beads + 30000 waters / 100000 atoms, 70 A, rc 10 A",
+          "terms": "LJ (LB) + Coulomb PME + harmonic bonds/angles + periodic torsions",
+          "l2": "inputs larger than L2 (pair list ~0.7 GB)", "step": "cell-list rebuild + energy/forces/box gradient"}
+
+
+def measure_c4(args, dev, peaks, fp32_peak, world=1, dist=None):
+    """The 100k-atom classical step (200 chains x 50 beads + 30000 waters, 70 A box): LJ + Coulomb
+    PME (rc 10 A, ethresh 1e-5, 154^3 mesh) + harmonic bonds / angles + 3-term torsions.  One step
+    = cell-list rebuild + energy / forces / box gradient, FP32 pair and mesh arithmetic with FP64
+    accumulation.  Returns the measurement dict (value = atom-evals/s over all ranks)."""
+    import torch
     from dmff_b200.engine import ClassicalEngine
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    s = c4_system()
     eng = ClassicalEngine(s["n_atoms"], n_types=len(s["sigma"]), coulomb="pme", pbc=True, rc=s["rc"], kappa=s["kappa"],
                           K=s["K"], cov_rows=s["cov_rows"], mscales_coul=s["mscales_coul"], mscales_lj=s["mscales_lj"],
                           precision="fp32", device=dev)
@@ -326,24 +401,23 @@ def run_classical(args, rank, world, local):
     torch.cuda.synchronize()
     l0 = eng.counters()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
+    if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    with ClockSampler(dev.index or 0) as clk:
         for k in range(args.steps):
             evs[k][0].record(stream)
             res, F = step()
             evs[k][1].record(stream)
         torch.cuda.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    total = sum(step_ms)
+    total = sum(a.elapsed_time(b) for a, b in evs)
     l1 = eng.counters()
-    if world > 1:
+    if dist is not None:
         t = torch.tensor([total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total = float(t.item())
     value = world * args.steps * s["n_atoms"] / (total / 1e3)
-    # e2e: pinned host positions in, forces and energy out, through the public engine API
+    # e2e: pinned host positions in, forces out, through the public engine API
     pos_h = torch.tensor(s["pos"], dtype=torch.float64).pin_memory()
     F_h = torch.empty((s["n_atoms"], 3), dtype=torch.float64).pin_memory()
     e2e = []
@@ -356,37 +430,68 @@ def run_classical(args, rank, world, local):
         torch.cuda.synchronize()
         if k >= args.warmup:
             e2e.append(time.perf_counter() - t0)
-    e2e_value = world * args.steps * s["n_atoms"] / sum(e2e)
+    e2e_total = sum(e2e)
+    if dist is not None:
+        t = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * args.steps * s["n_atoms"] / e2e_total
+    # per-class device times over instrumented steps
     eng.set_profiling(True)
     for _ in range(args.steps):
         step()
     torch.cuda.synchronize()
     stats = eng.kernel_stats()
     eng.set_profiling(False)
+    n_pairs = int(res.n_pairs)
+    n_scaled = int((eng.internal_pairs()[:, 2] != 0).sum().item())
+    n = s["n_atoms"]
+    K3 = float(np.prod(s["K"]))
+    work = {"pair_full": ("fp32", 120.0 * (n_pairs - n_scaled)), "pair_full_scaled": ("fp64", 120.0 * n_scaled),
+            "spread": ("hbm", n * 16 + 4 * K3), "gather_full": ("hbm", 4 * K3 + n * 40), "conv": ("hbm", 16 * K3)}
+    nb_launches = stats["neighbors"][1] / args.steps
+    if nb_launches:
+        work["neighbors"] = ("hbm", (12.0 * n + 12.0 * n_pairs) / nb_launches)
+    classes = class_rooflines(stats, args.steps, work, fp32_peak, peaks["hbm_gbs"])
+    pf = classes.get("pair_full", {})
+    return {"metric": METRIC, "value": value, "unit": "atom-evals/s", "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total / args.steps, "config": dict(C4_CFG, n_atoms=int(n), pme_mesh=[int(k) for k in s["K"]],
+                                                               ethresh=s["ethresh"], parallelism=f"replicas x{world}"),
+            "e2e": {"value": e2e_value, "unit": "atom-evals/s", "h2d_bytes_per_step": 24 * n,
+                    "d2h_bytes_per_step": 24 * n, "path": "ClassicalEngine.compute, pinned host copies"},
+            "roofline": {"kernel": "k_nb_pair FP32 launch (LJ + erfc Coulomb, unscaled rows)", "bound": "fp32",
+                         "achieved": pf.get("achieved"), "peak": round(fp32_peak, 2), "unit": "TFLOP/s",
+                         "frac": pf.get("frac"), "traffic": None, "avg_launch_us": pf.get("avg_launch_us"),
+                         "peak_source": "cuBLAS FP32 SGEMM (TF32 off) measured in this run",
+                         "work": "120 flop per unscaled pair row"},
+            "by_class": classes, "clocks": clk.summary(), "gpu_launches": int(l1["launches"] - l0["launches"]),
+            "library_launches": {"cufft_execs": int(l1["fft_execs"] - l0["fft_execs"])},
+            "result": {"energy_kJmol": res.energy, "e_coul": res.e_coul_real + res.e_coul_recip + res.e_coul_self,
+                       "e_lj": res.e_lj, "e_bonded": res.e_bond + res.e_angle + res.e_torsion,
+                       "n_pairs": n_pairs, "n_pairs_scaled": n_scaled}}
+
+
+def run_classical(args, rank, world, local):
+    """--workload c4: the classical step alone as the line (the default line carries it as "c4")."""
+    import torch
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        print(json.dumps(classical_cpu_reference(c4_system(), dict(C4_CFG), args)), flush=True)
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     peaks, src = measured_peaks()
-    ms, nl = stats["pair_full"]
-    per = ms / 1e3 / max(nl, 1)
-    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    # pair launches: one FP32 launch over all rows and one FP64 launch over the scaled rows, plus
-    # the three bonded launches share the class; work per step = 120 flop per pair row
-    flops_step = 120.0 * res.n_pairs
-    ach = flops_step / (ms / 1e3 / args.steps) / 1e12
+    fp32_peak = measure_fp32_peak(dev)
+    m = measure_c4(args, dev, peaks, fp32_peak, world, dist)
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "fp32 pairs/mesh, fp64 accumulation", "data": "synthetic",
-               "config": dict(cfg, parallelism=f"replicas x{world}"),
-               "e2e": {"value": e2e_value, "unit": "atom-evals/s", "h2d_bytes_per_step": 24 * s["n_atoms"],
-                       "d2h_bytes_per_step": 24 * s["n_atoms"], "path": "ClassicalEngine.compute, pinned host copies"},
-               "roofline": {"kernel": "k_nb_pair (LJ + erfc Coulomb) + bonded terms", "bound": "fp32", "achieved": ach,
-                            "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak, "traffic": None,
-                            "avg_launch_us": per * 1e6, "peak_source": "nominal FP32 CUDA-core peak at max SM clock"},
-               "clocks": clk.summary(), "gpu_launches": int(l1["launches"] - l0["launches"]),
-               "library_launches": {"cufft_execs": int(l1["fft_execs"] - l0["fft_execs"])},
-               "result": {"energy_kJmol": res.energy, "e_coul": res.e_coul_real + res.e_coul_recip + res.e_coul_self,
-                          "e_lj": res.e_lj, "e_bonded": res.e_bond + res.e_angle + res.e_torsion,
-                          "n_pairs": int(res.n_pairs)},
-               "kernel_ms_per_step": {k: v[0] / args.steps for k, v in stats.items() if v[1]}}
+        out = dict(m, n_gpus=world, higher_is_better=True, scaling="weak", vs_baseline=None,
+                   dtype="fp32 pairs/mesh, fp64 accumulation", data="synthetic")
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()
@@ -403,7 +508,6 @@ def classical_cpu_reference(s, cfg, args):
     torch.set_num_threads(os.cpu_count())
     pos = torch.tensor(s["pos"])
     box = torch.tensor(s["box"])
-    # full pair count from the cell-list estimate over a sample of atoms
     rng = np.random.default_rng(0)
     n = s["n_atoms"]
     samp = rng.choice(n, 200, replace=False)
@@ -439,7 +543,9 @@ def classical_cpu_reference(s, cfg, args):
               f"bonded terms ({t_bonded:.2f} s); energies only (no forces), a lower bound on the reference's time")
     return {"impl": "reference", "metric": METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": args.gpus,
             "steps": 1, "warmup": 0, "ms_per_step": t_eval * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(cfg, n_atoms=int(n), pme_mesh=[int(k) for k in s["K"]], ethresh=s["ethresh"],
+                           parallelism=f"replicas x{args.gpus}"),
             "cpu_baseline": {"value": value, "unit": "atom-evals/s", "cores": torch.get_num_threads(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "atom-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -460,7 +566,7 @@ def main():
         run_reference(args, s, rank)
         return
     serving_systems = None
-    if args.serving_requests > 0 and world == 1:
+    if args.serving_requests > 0 and world == 1 and args.workload == "c1":
         serving_systems = make_serving_systems(args.serving_requests)
     import torch
     import torch.distributed as dist
@@ -470,11 +576,14 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    peaks, src = measured_peaks()
+    fp32_peak = measure_fp32_peak(dev)
     eng = AdmpEngine(s["n_atoms"], s["lmax"], s["lpol"], True, s["rc"], s["kappa"], s["K"], s["axis_types"],
                      s["axis_indices"], s["cov_rows"], s["mscales"], s["pscales"], s["dscales"], precision="fp32",
                      solver="cg", cg_tol=1e-6, max_iter=1000, device=dev)
     eng.set_params(s["Q_local"], s.get("pol"), s.get("thole"))
-    eng.set_zero_guess(True)  # every step solves from U = 0 (the reference's U_init = None)
+    if s["lpol"]:
+        eng.set_zero_guess(True)  # every step solves from U = 0 (the reference's U_init = None)
     pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
     box = s["box"]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -513,7 +622,7 @@ def main():
     value = world * args.steps * s["n_atoms"] / (total_ms / 1e3)
 
     # e2e through the host-buffer C-ABI entry (pinned positions in, forces + dipoles out to pinned
-    # caller-owned arrays)
+    # caller-owned arrays; the call rebuilds the neighbour list for the copied-in positions)
     pos_h = torch.tensor(s["pos"], dtype=torch.float64).pin_memory().numpy()
     F_out = torch.zeros((s["n_atoms"], 3), dtype=torch.float64).pin_memory().numpy()
     U_out = torch.zeros((s["n_atoms"], 3), dtype=torch.float64).pin_memory().numpy()
@@ -524,7 +633,7 @@ def main():
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        r_h, F_h, U_h = eng.compute_host(pos_h, box, forces_out=F_out, U_out=U_out)
+        eng.compute_host(pos_h, box, forces_out=F_out, U_out=U_out)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_total = sum(e2e_ms)
     if world > 1:
@@ -533,7 +642,7 @@ def main():
         e2e_total = float(t.item())
     e2e_value = world * args.steps * s["n_atoms"] / (e2e_total / 1e3)
 
-    # per-kernel device times over K instrumented steps (events around every launch)
+    # per-kernel-class device times over K instrumented steps (events around every launch)
     eng.set_profiling(True)
     for k in range(args.steps):
         flush.zero_()
@@ -541,38 +650,53 @@ def main():
     torch.cuda.synchronize()
     stats = eng.kernel_stats()
     eng.set_profiling(False)
-    peaks, src = measured_peaks()
-    roof = roofline(stats, s, int(res.n_pairs), peaks, src)
+    n_pairs = int(res.n_pairs)
+    n_scaled = int((eng.internal_pairs()[:, 2] != 0).sum().item())
+    classes = class_rooflines(stats, args.steps, admp_work(s, n_pairs, n_scaled), fp32_peak, peaks["hbm_gbs"])
+    # the kernel with the largest share of the launch list (profiles/ summary of the ncu launch
+    # list agrees on the shares): the CG matvec, 12 B per CSR entry
+    roof = headline_roofline(classes, 12.0 * 2 * n_pairs, None, peaks["hbm_gbs"], src, "k_matvec_apply (CG matvec)",
+                             "pair_matvec")
+
+    c4 = None
+    if world == 1 and not args.no_c4 and args.workload == "c1":
+        del flush
+        torch.cuda.empty_cache()
+        c4 = measure_c4(args, dev, peaks, fp32_peak)
 
     out = None
     if rank == 0:
-        n_iter = int(statistics.median(iters))
+        n_iter = int(statistics.median(iters)) if s["lpol"] else 0
         out = {"metric": METRIC, "value": value, "unit": "atom-evals/s", "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "fp32 pairs/mesh, fp64 accumulation",
-               "data": "synthetic", "config": dict(workload_config(args.workload, s, s["K"]),
-                                                   parallelism=f"replicas x{world}"),
+               "data": "synthetic", "config": workload_config(args.workload, s, world),
                "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
                               "e2e_p50": float(np.percentile(e2e_ms, 50)), "e2e_p99": float(np.percentile(e2e_ms, 99))},
                "e2e": {"value": e2e_value, "unit": "atom-evals/s", "h2d_bytes_per_step": 3 * 8 * s["n_atoms"],
                        "d2h_bytes_per_step": 2 * 3 * 8 * s["n_atoms"],
                        "path": "dmffb_admp_compute_host (C ABI, host buffers)"},
-               "roofline": roof, "clocks": clk.summary(),
+               "roofline": roof, "fp32_peak_tflops": round(fp32_peak, 2),
+               "fp32_peak_source": "cuBLAS FP32 SGEMM 8192^3 (TF32 off), measured in this run",
+               "by_class": classes, "clocks": clk.summary(),
                "gpu_launches": int(launches1["launches"] - launches0["launches"]),
                "library_launches": {"cufft_execs": int(launches1["fft_execs"] - launches0["fft_execs"])},
                "result": {"energy_kJmol": res.energy, "cg_iters": n_iter, "converged": int(res.converged),
-                          "n_pairs": int(res.n_pairs)},
-               "kernel_ms_per_step": {k: v[0] / args.steps for k, v in stats.items() if v[1]}}
+                          "n_pairs": n_pairs, "n_pairs_scaled": n_scaled}}
         if world == 1 and not args.no_cpu_baseline:
-            t_g, t_ef, cores = cpu_reference_timing(s, n_iter)
-            t_eval = t_ef + n_iter * t_g
-            out["cpu_baseline"] = {
-                "value": s["n_atoms"] / t_eval, "unit": "atom-evals/s", "cores": cores, "kind": "port",
-                "sample": (f"one dE/dU pass ({t_g:.2f} s) and one energy+forces pass ({t_ef:.2f} s) of the same "
-                           f"box with the float64 oracle; evaluation = E+F + {n_iter} dE/dU passes (the GPU's CG "
-                           f"iteration count)")}
+            cs, run, cores = cpu_reference_runner()
+            run()  # warm-up
+            secs, its = [], []
+            for _ in range(2):
+                t, it = run()
+                secs.append(t)
+                its.append(it)
+            out["cpu_baseline"] = {"value": cs["n_atoms"] / statistics.median(secs), "unit": "atom-evals/s",
+                                   "cores": cores, "kind": "port", "sample": cpu_sample_text(cs, its, secs)}
+        if c4 is not None:
+            out["c4"] = c4
         if serving_systems is not None:
-            out["serving"] = bench_serving(args, serving_systems, dev)
+            out["c3"] = bench_serving(args, serving_systems, dev, peaks, fp32_peak)
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.barrier()

@@ -47,7 +47,8 @@ DMFFB_TERM_ANGLE = 1
 DMFFB_TERM_TORSION = 2
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
-                  "gather_field", "self_frames", "vector", "neighbors", "matvec_coef"]
+                  "gather_field", "self_frames", "vector", "neighbors", "matvec_coef", "pair_full_scaled",
+                  "pair_field_scaled", "param_grads", "bonded"]
 
 
 class AdmpDesc(ctypes.Structure):

@@ -107,8 +107,8 @@ struct dmffb_engine {
     bool prof = false;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, int>> prof_marks;  // (class, event index of start)
-    double kstat_ms[16] = {0};
-    int64_t kstat_n[16] = {0};
+    double kstat_ms[32] = {0};  // indexed by kernel class (KC_*), KC_COUNT <= 32
+    int64_t kstat_n[32] = {0};
     int64_t n_launch = 0, n_fft = 0;
     int64_t cg_graph_launches = 0, cg_graph_ffts = 0;  // per replay of the two-iteration CG graph
     // ---- last result book-keeping
@@ -263,7 +263,10 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // kernel classes for dmffb_get_kernel_stats
 enum { KC_PREP = 0, KC_PAIR_FULL, KC_PAIR_FIELD, KC_PAIR_MATVEC, KC_SPREAD, KC_FFT, KC_CONV, KC_GATHER_FULL,
-       KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_MVCOEF, KC_COUNT };
+       KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_MVCOEF,
+       // FP64 launches over the topologically scaled rows, parameter-adjoint pair kernels, bonded terms
+       KC_PAIR_FULL_SCALED, KC_PAIR_FIELD_SCALED, KC_PGRAD, KC_BONDED, KC_COUNT };
+static_assert(KC_COUNT <= 32, "kernel-class statistics arrays hold 32 classes");
 
 inline void prof_begin(dmffb_engine* h, cudaStream_t s, int cls) {
     if (!h->prof) return;
@@ -796,7 +799,7 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
             a.rowmap = h->d_srows;
             a.nrowmap = h->n_srows;
             if (h->n_srows > 0)
-                LAUNCH(h, sr, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(h->n_srows, 128), 128, 0, sr>>>(a));
+                LAUNCH(h, sr, KC_PAIR_FIELD_SCALED, k_admp_pair<T, true, PAIR_FIELD, ROWS_SCALED><<<nblk(h->n_srows, 128), 128, 0, sr>>>(a));
         } else {
             LAUNCH(h, sr, KC_PAIR_FIELD, k_admp_pair<T, true, PAIR_FIELD><<<nblk(npairs, 128), 128, 0, sr>>>(a));
         }
@@ -1039,12 +1042,12 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
                 LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, sp>>>(a));
                 a.rowmap = h->d_srows;
                 a.nrowmap = h->n_srows;
-                if (nbs) LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, sp>>>(a));
+                if (nbs) LAUNCH(h, sp, KC_PAIR_FULL_SCALED, k_admp_pair<T, true, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, sp>>>(a));
             } else {
                 LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_UNSCALED><<<nbk, 128, 0, sp>>>(a));
                 a.rowmap = h->d_srows;
                 a.nrowmap = h->n_srows;
-                if (nbs) LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, sp>>>(a));
+                if (nbs) LAUNCH(h, sp, KC_PAIR_FULL_SCALED, k_admp_pair<T, false, PAIR_FULL, ROWS_SCALED><<<nbs, 128, 0, sp>>>(a));
             }
         } else {
             if (h->lpol) LAUNCH(h, sp, KC_PAIR_FULL, k_admp_pair<T, true, PAIR_FULL><<<nbk, 128, 0, sp>>>(a));
@@ -1090,19 +1093,19 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
             if (sizeof(T) == 4) {
                 const unsigned nbs = nblk(h->n_srows, 128);
                 if (h->lpol) {
-                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
+                    LAUNCH(h, s, KC_PGRAD, k_admp_pgrad<T, true, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
                     g.p.rowmap = h->d_srows;
                     g.p.nrowmap = h->n_srows;
-                    if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true, ROWS_SCALED><<<nbs, 128, 0, s>>>(g));
+                    if (nbs) LAUNCH(h, s, KC_PGRAD, k_admp_pgrad<T, true, ROWS_SCALED><<<nbs, 128, 0, s>>>(g));
                 } else {
-                    LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
+                    LAUNCH(h, s, KC_PGRAD, k_admp_pgrad<T, false, ROWS_UNSCALED><<<nbk, 128, 0, s>>>(g));
                     g.p.rowmap = h->d_srows;
                     g.p.nrowmap = h->n_srows;
-                    if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false, ROWS_SCALED><<<nbs, 128, 0, s>>>(g));
+                    if (nbs) LAUNCH(h, s, KC_PGRAD, k_admp_pgrad<T, false, ROWS_SCALED><<<nbs, 128, 0, s>>>(g));
                 }
             } else {
-                if (h->lpol) LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, true><<<nbk, 128, 0, s>>>(g));
-                else LAUNCH(h, s, KC_PAIR_FULL, k_admp_pgrad<T, false><<<nbk, 128, 0, s>>>(g));
+                if (h->lpol) LAUNCH(h, s, KC_PGRAD, k_admp_pgrad<T, true><<<nbk, 128, 0, s>>>(g));
+                else LAUNCH(h, s, KC_PGRAD, k_admp_pgrad<T, false><<<nbk, 128, 0, s>>>(g));
             }
         }
         LocalGradArgs la;
@@ -1314,12 +1317,12 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
                 LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 1, true><<<nbk, 128, 0, s>>>(a));
                 a.rowmap = h->d_srows;
                 a.nrowmap = h->n_srows;
-                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, true><<<nbs, 128, 0, s>>>(a));
+                if (nbs) LAUNCH(h, s, KC_PAIR_FULL_SCALED, k_disp_pair<T, 2, true><<<nbs, 128, 0, s>>>(a));
             } else {
                 LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 1, false><<<nbk, 128, 0, s>>>(a));
                 a.rowmap = h->d_srows;
                 a.nrowmap = h->n_srows;
-                if (nbs) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 2, false><<<nbs, 128, 0, s>>>(a));
+                if (nbs) LAUNCH(h, s, KC_PAIR_FULL_SCALED, k_disp_pair<T, 2, false><<<nbs, 128, 0, s>>>(a));
             }
         } else {
             if (h->tt) LAUNCH(h, s, KC_PAIR_FULL, k_disp_pair<T, 0, true><<<nbk, 128, 0, s>>>(a));
@@ -1429,7 +1432,7 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
             LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 1><<<nbk, 128, 0, s>>>(a));
             a.rowmap = h->d_srows;
             a.nrowmap = h->n_srows;
-            if (h->n_srows > 0) LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 2><<<nblk(h->n_srows, 128), 128, 0, s>>>(a));
+            if (h->n_srows > 0) LAUNCH(h, s, KC_PAIR_FULL_SCALED, k_nb_pair<T, 2><<<nblk(h->n_srows, 128), 128, 0, s>>>(a));
         } else {
             LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 0><<<nbk, 128, 0, s>>>(a));
         }
@@ -1455,9 +1458,9 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
         b.dprm = pg ? h->d_tdprm[kind] : nullptr;
         b.scal = h->d_scal + 12 + kind;
         const unsigned nbk = nblk(h->nterm[kind], 128);
-        if (kind == 0) LAUNCH(h, s, KC_PAIR_FULL, k_bonds<<<nbk, 128, 0, s>>>(b));
-        else if (kind == 1) LAUNCH(h, s, KC_PAIR_FULL, k_angles<<<nbk, 128, 0, s>>>(b));
-        else LAUNCH(h, s, KC_PAIR_FULL, k_torsions<<<nbk, 128, 0, s>>>(b));
+        if (kind == 0) LAUNCH(h, s, KC_BONDED, k_bonds<<<nbk, 128, 0, s>>>(b));
+        else if (kind == 1) LAUNCH(h, s, KC_BONDED, k_angles<<<nbk, 128, 0, s>>>(b));
+        else LAUNCH(h, s, KC_BONDED, k_torsions<<<nbk, 128, 0, s>>>(b));
         CK(cudaGetLastError());
     }
     if (forces)
@@ -2481,7 +2484,7 @@ int dmffb_get_timings(const dmffb_engine* h, double* ms_out, int32_t n) {
 int dmffb_set_profiling(dmffb_engine* h, int32_t enabled) {
     if (!h) return DMFFB_BAD_ARG;
     h->prof = enabled != 0;
-    for (int k = 0; k < 16; ++k) { h->kstat_ms[k] = 0; h->kstat_n[k] = 0; }
+    for (int k = 0; k < 32; ++k) { h->kstat_ms[k] = 0; h->kstat_n[k] = 0; }
     return DMFFB_OK;
 }
 

@@ -166,7 +166,9 @@ int dmffb_set_timing(dmffb_engine* h, int32_t enabled);
  * on its stream and its duration is added to its class.  Classes: 0 prepare/frames, 1 pair FULL,
  * 2 pair FIELD, 3 pair MATVEC, 4 spread, 5 FFT (cuFFT), 6 convolution, 7 gather FULL,
  * 8 gather FIELD, 9 self+frame forces, 10 vector/CG ops, 11 neighbour build, 12 CG matvec
- * pair-tensor set-up. */
+ * pair-tensor set-up, 13 pair FULL over the topologically scaled rows (FP64), 14 pair FIELD over
+ * the scaled rows (FP64), 15 parameter-adjoint pair kernels, 16 bonded terms.  Classes 1 and 2
+ * hold only the launches over the unscaled rows (kernel precision). */
 int dmffb_set_profiling(dmffb_engine* h, int32_t enabled);
 int dmffb_get_kernel_stats(const dmffb_engine* h, double* ms_out, int64_t* launches_out, int32_t n);
 /* [0] launches of this library's kernels since create, [1] cuFFT executions. */
