@@ -653,8 +653,7 @@ def main():
     n_pairs = int(res.n_pairs)
     n_scaled = int((eng.internal_pairs()[:, 2] != 0).sum().item())
     classes = class_rooflines(stats, args.steps, admp_work(s, n_pairs, n_scaled), fp32_peak, peaks["hbm_gbs"])
-    # the kernel with the largest share of the launch list (profiles/ summary of the ncu launch
-    # list agrees on the shares): the CG matvec, 12 B per CSR entry
+    # the kernel with the largest share of the step's launches: the CG matvec, 12 B per CSR entry
     roof = headline_roofline(classes, 12.0 * 2 * n_pairs, None, peaks["hbm_gbs"], src, "k_matvec_apply (CG matvec)",
                              "pair_matvec")
 

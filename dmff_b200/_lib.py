@@ -34,7 +34,8 @@ EXPORTED = [
     "dmffb_disp_create", "dmffb_disp_set_params", "dmffb_disp_compute", "dmffb_disp_param_grads", "dmffb_disp_set_param_grads",
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
-    "dmffb_set_graphs", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
+    "dmffb_classical_set_cell_pass",
+    "dmffb_set_graphs", "dmffb_admp_backward", "dmffb_admp_param_grads_host", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
     "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy",
 ]
 
@@ -87,6 +88,29 @@ class AdmpResult(ctypes.Structure):
         ("converged", ctypes.c_int32),
         ("residual_rms", ctypes.c_double),
         ("n_pairs", ctypes.c_int64),
+    ]
+
+
+class AdmpCotangent(ctypes.Structure):
+    _fields_ = [
+        ("pos", ctypes.c_void_p),
+        ("box", ctypes.c_double * 9),
+        ("Q_local", ctypes.c_void_p),
+        ("pol", ctypes.c_void_p),
+        ("thole", ctypes.c_void_p),
+    ]
+
+
+class AdmpSecond(ctypes.Structure):
+    _fields_ = [
+        ("pos", ctypes.c_void_p),
+        ("box", ctypes.c_double * 9),
+        ("Q_local", ctypes.c_void_p),
+        ("pol", ctypes.c_void_p),
+        ("thole", ctypes.c_void_p),
+        ("n_iter", ctypes.c_int32),
+        ("residual_rms", ctypes.c_double),
+        ("step", ctypes.c_double),
     ]
 
 
@@ -200,7 +224,8 @@ class Request(ctypes.Structure):
 
 
 # C struct name of each ctypes mirror (layout checked against the header by the CPU tests)
-STRUCTS = {"dmffb_admp_desc": AdmpDesc, "dmffb_admp_result": AdmpResult, "dmffb_disp_desc": DispDesc,
+STRUCTS = {"dmffb_admp_desc": AdmpDesc, "dmffb_admp_result": AdmpResult, "dmffb_admp_cotangent": AdmpCotangent,
+           "dmffb_admp_second": AdmpSecond, "dmffb_disp_desc": DispDesc,
            "dmffb_disp_result": DispResult, "dmffb_classical_desc": ClassicalDesc,
            "dmffb_classical_result": ClassicalResult, "dmffb_server_desc": ServerDesc, "dmffb_request": Request}
 
@@ -232,6 +257,8 @@ def load():
     lib.dmffb_admp_set_param_grads.argtypes = [vp, i32]
     lib.dmffb_admp_set_zero_guess.argtypes = [vp, i32]
     lib.dmffb_admp_param_grads.argtypes = [vp, vp, vp, vp, vp, vp]
+    lib.dmffb_admp_backward.argtypes = [vp, vp, P(AdmpCotangent), P(AdmpSecond)]
+    lib.dmffb_admp_param_grads_host.argtypes = [vp, vp, vp, vp]
     lib.dmffb_build_neighbors.argtypes = [vp, vp, vp, vp, dbl, vp, i64, P(i64)]
     lib.dmffb_admp_build_neighbors.argtypes = [vp, vp, vp, vp]
     lib.dmffb_engine_pairs.argtypes = [vp, vp, vp, i64, P(i64)]
@@ -250,6 +277,7 @@ def load():
     lib.dmffb_classical_set_params.argtypes = [vp, vp, vp, vp, vp]
     lib.dmffb_classical_set_terms.argtypes = [vp, i32, i64, vp, vp]
     lib.dmffb_classical_set_param_grads.argtypes = [vp, i32]
+    lib.dmffb_classical_set_cell_pass.argtypes = [vp, i32]
     lib.dmffb_classical_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, P(ClassicalResult)]
     lib.dmffb_classical_param_grads.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     lib.dmffb_set_graphs.argtypes = [vp, i32]

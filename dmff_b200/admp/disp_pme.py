@@ -65,6 +65,43 @@ class ADMPDispPmeForce:
                                       self.cov_rows, ms, tt=self.tt, precision=self.precision, device=self.device)
         return self._engine
 
+    def second_order(self, point, pairs, with_tt, cot):
+        """Vector-Jacobian product through the first derivatives at ``point`` = (positions, box,
+        c_list, a, b, q) with cotangents ``cot``: central differences of the engine's analytic
+        first derivatives along ``cot`` (``_hvp.central_hvp``), on an FP64 engine of the same
+        system with its pair list built at the evaluation's positions."""
+        from .._hvp import central_hvp
+        from ..engine import DispEngine
+        eng0 = self._engine
+        if self.precision == "fp64":
+            eng = eng0
+        else:
+            if getattr(self, "_engine64", None) is None or self._engine64.n != eng0.n:
+                self._engine64 = DispEngine(eng0.n, self.pmax, self.lpme, self.rc, self.kappa,
+                                            (self.K1, self.K2, self.K3), self.cov_rows, eng0.mscales, tt=self.tt,
+                                            precision="fp64", device=self.device)
+            eng = self._engine64
+        pos0, box0 = point[0], point[1]
+        dev = eng.device
+        eng.rebuild_internal_pairs(pos0.detach().to(dev, torch.float64).contiguous(), box0.detach())
+        want_p = any(t is not None for t in point[2:])
+
+        def grad_at(z):
+            pos, box, c, a, b, q = z
+            eng.set_params(c.detach(), *((a.detach(), b.detach(), q.detach()) if with_tt else (None, None, None)))
+            _, first = _disp_first(eng, pos.detach().to(dev, torch.float64).contiguous(), box.detach(), pairs,
+                                   with_tt, want_p)
+            return [first[0].to(pos.device), first[1].to(box.device)] + [
+                None if t is None else (torch.zeros_like(t) if v is None else v.to(t.device))
+                for v, t in zip(first[2:], z[2:])]
+
+        scales = [1.0, 1.0] + [1.0 if t is None else float(t.detach().abs().max()) for t in point[2:]]
+        direction = [None if c is None else c.detach() for c in cot]
+        hv, step = central_hvp(grad_at, [None if t is None else t.detach().to(torch.float64) for t in point],
+                               direction, scales)
+        self.last_second_order = {"step": step}
+        return hv
+
     def get_energy(self, positions, box, pairs, c_list, mScales, tt=None):
         from .pme import _as_cuda_pairs
         positions = torch.as_tensor(positions, dtype=torch.float64)
@@ -81,44 +118,77 @@ class ADMPDispPmeForce:
 class _DispEnergy(torch.autograd.Function):
     """E_lr, or E_sr - E_lr with TT damping, of (positions, box, c_list, a, b, q); backward gives
     position / box gradients and, when the parameter tensors require grad, the engine's
-    parameter adjoints."""
+    parameter adjoints.  The first derivatives come out of ``_DispFirstDerivs``, so that they are
+    differentiable in turn (``create_graph=True``)."""
 
     @staticmethod
     def forward(ctx, positions, box, c_list, a, b, q, eng, pairs, force, with_tt):
         pos = positions.detach().to(device=eng.device, dtype=torch.float64).contiguous()
         want_p = any(ctx.needs_input_grad[2:6])
-        eng.set_param_grads(want_p)
-        res, F = eng.compute(pos, box, pairs=pairs)
+        res, first = _disp_first(eng, pos, box, pairs, with_tt, want_p)
         force.last_result = res
         E = (res.e_sr - res.energy) if with_tt else res.energy
-        g_sr = torch.tensor(list(res.box_grad_sr), dtype=torch.float64).reshape(3, 3)
-        g_lr = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
-        # forces from the engine are -dE_lr/dpos (disp) and -dE_sr/dpos (TT) separately
-        Flr, Fsr = F
-        grad = (-(Fsr - Flr)) if with_tt else (-Flr)
-        ctx.save_for_backward(grad.clone())
-        ctx.box_grad = (g_sr - g_lr) if with_tt else g_lr
-        ctx.devs = (positions.device, box.device)
-        ctx.pdevs = [None if t is None else t.device for t in (c_list, a, b, q)]
-        ctx.with_tt = with_tt
-        ctx.pg = None
-        if want_p:
-            pg = eng.param_grads()
-            if with_tt:
-                dc = -pg["c"].clone()
-                dc[:, 0] += pg["c6"]
-                ctx.pg = (dc, pg["a"], pg["b"], pg["q"])
-            else:
-                ctx.pg = (pg["c"], None, None, None)
+        ctx.payload = {"force": force, "pairs": pairs, "with_tt": with_tt, "first": first, "want_p": want_p}
+        ctx.save_for_backward(positions, box, c_list, a, b, q)
         return torch.tensor(E, dtype=torch.float64, device=positions.device)
 
     @staticmethod
     def backward(ctx, g):
-        (grad,) = ctx.saved_tensors
-        outs = [None] * 4
-        if ctx.pg is not None:
-            for k, t in enumerate(ctx.pg):
-                if t is not None and ctx.pdevs[k] is not None:
-                    outs[k] = (t * g.to(t.device)).to(ctx.pdevs[k])
-        return ((grad * g.to(grad.device)).to(ctx.devs[0]), (ctx.box_grad.to(ctx.devs[1]) * g.to(ctx.devs[1])),
-                *outs, None, None, None, None)
+        saved = ctx.saved_tensors
+        d = _DispFirstDerivs.apply(*saved, ctx.payload)
+        outs = []
+        for k, t in enumerate(d):
+            if t is None or (k >= 2 and not (ctx.payload["want_p"] and ctx.needs_input_grad[k])):
+                outs.append(None)
+            else:
+                outs.append(t * g.to(t.device))
+        return (*outs, None, None, None, None)
+
+
+def _disp_first(eng, pos, box, pairs, with_tt, want_p):
+    """One engine evaluation; returns (result, [dE/dpos, dE/dbox, dE/dc [n, 3], dE/da, dE/db, dE/dq])
+    of E = E_lr, or E_sr - E_lr with TT (parameter blocks None without adjoints)."""
+    eng.set_param_grads(want_p)
+    res, F = eng.compute(pos, box, pairs=pairs)
+    g_sr = torch.tensor(list(res.box_grad_sr), dtype=torch.float64).reshape(3, 3)
+    g_lr = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
+    # forces from the engine are -dE_lr/dpos (disp) and -dE_sr/dpos (TT) separately
+    Flr, Fsr = F
+    first = [(-(Fsr - Flr)) if with_tt else (-Flr).clone(), (g_sr - g_lr) if with_tt else g_lr, None, None, None, None]
+    if want_p:
+        pg = eng.param_grads()
+        if with_tt:
+            dc = -pg["c"].clone()
+            dc[:, 0] += pg["c6"]
+            first[2:] = [dc, pg["a"].clone(), pg["b"].clone(), pg["q"].clone()]
+        else:
+            first[2] = pg["c"].clone()
+    return res, first
+
+
+class _DispFirstDerivs(torch.autograd.Function):
+    """(dE/dpositions, dE/dbox, dE/dc_list, dE/da, dE/db, dE/dq) of the forward's evaluation as a
+    function of those inputs; its backward is the Hessian-vector product by central differences
+    of the engine's analytic first derivatives (``_hvp.central_hvp``)."""
+
+    @staticmethod
+    def forward(ctx, positions, box, c_list, a, b, q, payload):
+        ctx.payload = payload
+        ctx.save_for_backward(positions, box, c_list, a, b, q)
+        like = (positions, box, c_list, a, b, q)
+        out = []
+        for v, t in zip(payload["first"], like):
+            if t is None:
+                out.append(None)
+            elif v is None:
+                out.append(torch.zeros_like(t, dtype=torch.float64))
+            else:
+                out.append(v.to(t.device).clone())
+        return tuple(out)
+
+    @staticmethod
+    def backward(ctx, *cot):
+        saved = ctx.saved_tensors
+        p = ctx.payload
+        sec = p["force"].second_order(saved, p["pairs"], p["with_tt"], cot)
+        return (*[None if t is None else g.to(t.device) for g, t in zip(sec, saved)], None)

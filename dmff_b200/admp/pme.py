@@ -55,9 +55,11 @@ def _as_cuda_pairs(pairs, device):
 
 
 class _AdmpEnergy(torch.autograd.Function):
-    """E(positions, box, Q_local, pol, tholes); backward returns -forces, dE/dbox and, when the
-    parameter tensors require grad, the engine's parameter adjoints (dE/dQ_local, dE/dpol,
-    dE/dthole at the converged dipoles, where E is stationary in U)."""
+    """E(positions, box, Q_local, pol, tholes); backward returns dE/dpositions (-forces), dE/dbox
+    and, when the parameter tensors require grad, the engine's parameter adjoints (dE/dQ_local,
+    dE/dpol, dE/dthole at the converged dipoles, where E is stationary in U).  Those first
+    derivatives come out of ``_AdmpFirstDerivs``, so that with ``create_graph=True`` they are
+    differentiable in turn (a loss on forces or on the virial, force matching)."""
 
     @staticmethod
     def forward(ctx, positions, box, Q_local, pol, tholes, force, pairs, U0, aux):
@@ -77,30 +79,63 @@ class _AdmpEnergy(torch.autograd.Function):
             aux["U_ind"] = U * 0.1  # Angstrom -> nm, as pme.py:225
             aux["lconverg"] = bool(res.converged)
             aux["n_cycle"] = int(res.n_iter)
-        ctx.save_for_backward(forces.clone())
-        ctx.box_grad = torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3)
-        ctx.pos_device, ctx.box_device = positions.device, box.device if torch.is_tensor(box) else None
-        ctx.pg = eng.param_grads() if want_p else None
-        ctx.pshapes = [None if t is None else (tuple(t.shape), t.device) for t in (Q_local, pol, tholes)]
+        pg = eng.param_grads() if want_p else None
+        z = lambda t: None if t is None else torch.zeros_like(t, dtype=torch.float64)
+        first = {"pos": -forces.clone(), "box": torch.tensor(list(res.box_grad), dtype=torch.float64).reshape(3, 3),
+                 "Q_local": pg["Q_local"] if pg is not None else None,
+                 "pol": pg["pol"] if pg is not None else None, "thole": pg["thole"] if pg is not None else None}
+        ctx.payload = {"force": force, "pairs": pairs, "U": None if U is None else U.clone(), "first": first,
+                       "zero": (z(Q_local), z(pol), z(tholes))}
+        ctx.save_for_backward(positions, box, Q_local, pol, tholes)
         return torch.tensor(res.energy, dtype=torch.float64, device=positions.device)
 
     @staticmethod
     def backward(ctx, g):
-        (forces,) = ctx.saved_tensors
-        gpos = (-forces * g.to(forces.device)).to(ctx.pos_device)
-        gbox = None
-        if ctx.box_device is not None:
-            gbox = (ctx.box_grad.to(ctx.box_device) * g.to(ctx.box_device))
+        positions, box, Q_local, pol, tholes = ctx.saved_tensors
+        d = _AdmpFirstDerivs.apply(positions, box, Q_local, pol, tholes, ctx.payload)
+        gpos = d[0] * g.to(d[0].device)
+        gbox = d[1] * g.to(d[1].device)
         gq = gp = gt = None
-        if ctx.pg is not None:
-            if ctx.pshapes[0] is not None:
-                shp, dv = ctx.pshapes[0]
-                gq = (ctx.pg["Q_local"][:, : shp[1]] * g.to(ctx.pg["Q_local"].device)).to(dv)
-            if ctx.pshapes[1] is not None:
-                gp = (ctx.pg["pol"] * g.to(ctx.pg["pol"].device)).to(ctx.pshapes[1][1])
-            if ctx.pshapes[2] is not None:
-                gt = (ctx.pg["thole"] * g.to(ctx.pg["thole"].device)).to(ctx.pshapes[2][1])
+        if ctx.payload["first"]["Q_local"] is not None:
+            gq = d[2] * g.to(d[2].device) if ctx.needs_input_grad[2] else None
+            gp = d[3] * g.to(d[3].device) if ctx.needs_input_grad[3] and d[3] is not None else None
+            gt = d[4] * g.to(d[4].device) if ctx.needs_input_grad[4] and d[4] is not None else None
         return gpos, gbox, gq, gp, gt, None, None, None, None
+
+
+class _AdmpFirstDerivs(torch.autograd.Function):
+    """(dE/dpositions, dE/dbox, dE/dQ_local, dE/dpol, dE/dthole) of the forward's evaluation, as
+    a function of (positions, box, Q_local, pol, tholes) with the induced dipoles following.  Its
+    backward is the engine's second-order pass (dmffb_admp_backward): one adjoint CG solve for the
+    dipole response instead of differentiating through the iteration."""
+
+    @staticmethod
+    def forward(ctx, positions, box, Q_local, pol, tholes, payload):
+        ctx.payload = payload
+        ctx.save_for_backward(positions, box, Q_local, pol, tholes)
+        f, zero = payload["first"], payload["zero"]
+
+        def out(v, like, zz):
+            if like is None:
+                return None
+            if v is None:
+                return zz.clone()
+            v = v[:, : like.shape[1]] if like.dim() == 2 and v.dim() == 2 else v
+            return v.to(like.device).clone()
+
+        return (f["pos"].to(positions.device).clone(), f["box"].to(box.device).clone(),
+                out(f["Q_local"], Q_local, zero[0]), out(f["pol"], pol, zero[1]), out(f["thole"], tholes, zero[2]))
+
+    @staticmethod
+    def backward(ctx, c_pos, c_box, c_Q, c_pol, c_th):
+        positions, box, Q_local, pol, tholes = ctx.saved_tensors
+        p = ctx.payload
+        sec = p["force"].second_order(positions, box, Q_local, pol, tholes, p["pairs"], p["U"], c_pos, c_box, c_Q,
+                                      c_pol, c_th)
+        gQ = None if Q_local is None else sec["Q_local"][:, : Q_local.shape[1]].to(Q_local.device)
+        gp = None if pol is None else sec["pol"].to(pol.device)
+        gt = None if tholes is None else sec["thole"].to(tholes.device)
+        return sec["pos"].to(positions.device), sec["box"].to(box.device), gQ, gp, gt, None
 
 
 class ADMPPmeForce:
@@ -171,6 +206,39 @@ class ADMPPmeForce:
             self._scales = scales
         self.engine.set_params(Q_local, pol if self.lpol else None, tholes if self.lpol else None)
         self._param_key = key
+
+    def second_order(self, positions, box, Q_local, pol, tholes, pairs, U, c_pos, c_box, c_Q, c_pol, c_thole):
+        """Vector-Jacobian product through the first derivatives of an evaluation (the backward of
+        ``_AdmpFirstDerivs``), on an FP64 engine: the forward's engine when it is FP64, else an FP64
+        engine of the same system kept for this purpose.  The engine is brought back to the
+        evaluation's point (parameters, positions, pairs; the dipole solve restarts from the
+        forward's converged dipoles) and runs dmffb_admp_backward."""
+        if self.precision == "fp64":
+            eng = self.engine
+        else:
+            if getattr(self, "_engine64", None) is None:
+                ms, ps, ds = self._scales if getattr(self, "_scales", None) else ([0, 0, 1, 1, 1, 1],) * 3
+                self._engine64 = AdmpEngine(
+                    self.n_atoms, self.lmax, self.lpol, self.lpme, self.rc, self.kappa, (self.K1, self.K2, self.K3),
+                    self.axis_type if self.lmax > 0 else None, self.axis_indices if self.lmax > 0 else None,
+                    self.cov_rows, ms, ps, ds, precision="fp64", solver="cg", cg_tol=min(self.cg_tol, 1e-10),
+                    max_iter=max(self.max_iter, 1000), device=self.device)
+            eng = self._engine64
+        self._param_key = None  # the engine's parameters are set below: the value cache is stale
+        eng.set_params(Q_local.detach(), pol.detach() if self.lpol else None, tholes.detach() if self.lpol else None)
+        eng.set_param_grads(False)
+        pos = positions.detach().to(device=eng.device, dtype=torch.float64).contiguous()
+        Ui = None if U is None else U.detach().to(device=eng.device, dtype=torch.float64).contiguous().clone()
+        if pairs is None:  # the engine's own list, built at this evaluation's positions
+            eng.rebuild_internal_pairs(pos, box.detach())
+        eng.compute(pos, box.detach(), pairs=pairs, U=Ui)
+        cQ = None
+        if c_Q is not None:
+            cQ = torch.zeros((self.n_atoms, 9), dtype=torch.float64, device=eng.device)
+            cQ[:, : c_Q.shape[1]] = c_Q.detach().to(eng.device, torch.float64)
+        out = eng.backward(c_pos, c_box, cQ, c_pol if self.lpol else None, c_thole if self.lpol else None)
+        self.last_second_order = {"n_iter": out["n_iter"], "residual_rms": out["residual_rms"], "step": out["step"]}
+        return out
 
     def get_energy(self, positions, box, pairs, Q_local, pol=None, tholes=None, mScales=None, pScales=None,
                    dScales=None, U_init=None, aux=None):

@@ -28,6 +28,7 @@
 #pragma once
 #include "common.cuh"
 #include "admp_real.cuh"
+#include "nblist.cuh"
 
 namespace dmffb {
 
@@ -57,6 +58,7 @@ struct NbPairArgs {
     double* scal;          // [0] E_coul real space, [1] E_lj, [2..10] box gradient
     const int32_t* rowmap = nullptr;  // ROWS == 2 launches: indices of the rows with nbond != 0
     int64_t nrowmap = 0;
+    double cut = 0.0;  // > 0: only rows whose minimum-image distance is < cut (the list build's test)
 };
 
 // energies and d/dr of one pair; phi = dE_coul / d(q_i q_j)
@@ -109,7 +111,8 @@ __global__ void __launch_bounds__(128) k_nb_pair(NbPairArgs<T> a) {
         j = a.pairs[3 * row + 1];
         nb = a.pairs[3 * row + 2];
     }
-    const bool valid = (row < a.npairs) && i >= 0 && i < j && j < a.n && (ROWS == 0 || (ROWS == 1) == (nb == 0));
+    bool valid = (row < a.npairs) && i >= 0 && i < j && j < a.n && (ROWS == 0 || (ROWS == 1) == (nb == 0));
+    if (valid && a.cut > 0.0) valid = within_rc(a.boxd, a.pos + 3 * i, a.pos + 3 * j, a.cut);
     const int key = valid ? i : -1;
     T g[3] = {T(0), T(0), T(0)};
     double red[11];

@@ -22,6 +22,7 @@
 #include "nblist.cuh"
 #include "disp.cuh"
 #include "classical.cuh"
+#include "nbcells.cuh"
 
 using namespace dmffb;
 
@@ -143,6 +144,10 @@ struct dmffb_engine {
     double* d_tprm[3] = {nullptr, nullptr, nullptr};
     double* d_tdprm[3] = {nullptr, nullptr, nullptr};
     bool want_pgrad = false, charges_set = false;
+    bool cell_pass = false;  // dmffb_classical_set_cell_pass: pairs from the cell grid, no list
+    int32_t* d_covrows = nullptr;  // [n_covrows*3] covalent rows (i < j, nbond)
+    int64_t n_covrows = 0;
+    int32_t *d_cov_lo = nullptr, *d_cov_hi = nullptr;  // [n] covalent partner index range
     bool zero_guess = false;  // dipole solves start from U = 0 (dmffb_admp_set_zero_guess)
     bool u_zeroed = false;    // this call's U was zeroed by the host-buffer entry point
     // ---- ADMP parameter adjoints (dmffb_admp_set_param_grads)
@@ -169,6 +174,15 @@ struct dmffb_engine {
     int bmod_cap = 0;
     uint32_t* d_nbmask = nullptr;  // candidate keep masks of the neighbour count pass
     int64_t nbmask_cap = 0;
+    // ---- second-order pass (dmffb_admp_backward): the point of the last compute and scratch
+    bool fixed_U = false;  // compute_impl takes U as given (no dipole solve)
+    bool have_last = false;
+    const int32_t* last_pairs = nullptr;
+    int64_t last_npairs = 0;
+    double* last_U = nullptr;
+    std::vector<double> h_Qloc, h_pol, h_thole;  // host copies of the last set_params
+    double* d_bk = nullptr;  // [52 n] scratch of the second-order pass
+    int64_t bk_cap = 0;
     std::map<std::array<int, 3>, std::pair<cufftHandle, cufftHandle>> plan_cache;  // mesh -> (R2C, C2R)
 };
 
@@ -830,16 +844,18 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     return DMFFB_OK;
 }
 
+// Solves A U = -b for the induced dipoles, b the permanent field (dE/dU at U = 0), A = d2E/dU2.
+// With rhs (the second-order pass) it solves A U = -rhs from U = 0 by CG instead.
 template <typename T>
 int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
-                  int64_t npairs, double* U, dmffb_admp_result* res) {
+                  int64_t npairs, double* U, dmffb_admp_result* res, const double* rhs = nullptr) {
     const int n = h->n;
     const unsigned nb3 = nblk(3 * n, 256);
     double* sc = h->d_scal + S_CG;
     int st;
     if ((st = build_csr(h, s, pairs, npairs))) return st;
     if ((st = matvec_alloc<T>(h))) return st;
-    if (h->solver == DMFFB_SOLVER_REFERENCE) {
+    if (h->solver == DMFFB_SOLVER_REFERENCE && !rhs) {
         if ((st = matvec_coef_launch<T>(h, s, bx, pairs, npairs))) return st;
         int it = 0;
         bool conv = false;
@@ -878,11 +894,16 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         CK(cudaMemsetAsync(h->d_grid2, 0, (size_t)h->K[0] * h->K[1] * h->K[2] * sizeof(T), s));
         if ((st = stencil_prep<T>(h, s, pos, bx))) return st;
     }
-    if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b, nullptr, nullptr, nullptr, true)))
+    if (rhs) {
+        if ((st = matvec_coef_launch<T>(h, s, bx, pairs, npairs))) return st;
+        CK(cudaMemcpyAsync(h->d_b, rhs, (size_t)3 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else if ((st = field_eval<T>(h, s, pos, bx, pairs, npairs, nullptr, true, h->d_b, nullptr, nullptr, nullptr,
+                                   true))) {
         return st;
+    }
     // from U = 0 the residual is -b: no A U pass
-    const bool u0 = h->zero_guess || h->u_zeroed;
-    if (h->zero_guess) CK(cudaMemsetAsync(U, 0, (size_t)3 * n * sizeof(double), s));
+    const bool u0 = h->zero_guess || h->u_zeroed || rhs;
+    if (h->zero_guess || rhs) CK(cudaMemsetAsync(U, 0, (size_t)3 * n * sizeof(double), s));
     if (!u0 && (st = field_eval<T>(h, s, pos, bx, pairs, npairs, U, false, h->d_Ap))) return st;
     LAUNCH(h, s, KC_VEC, k_cg_init<<<nb3, 256, 0, s>>>(n, h->d_b, u0 ? nullptr : h->d_Ap, h->d_pol, h->d_r, h->d_z,
                                                      h->d_p));
@@ -996,6 +1017,10 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
         npairs = h->npairs;
     }
     res->n_pairs = npairs;
+    h->last_pairs = pairs;
+    h->last_npairs = npairs;
+    h->last_U = U;
+    h->have_last = true;
     if (sizeof(T) == 4 && npairs > 0)
         if ((st = scaled_rows(h, s, pairs, npairs))) return st;
     if (h->timing) CK(cudaEventRecord(h->ev[0], s));
@@ -1018,7 +1043,7 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
     CK(cudaGetLastError());
     if (h->timing) CK(cudaEventRecord(h->ev[1], s));
-    if (h->lpol) {
+    if (h->lpol && !h->fixed_U) {
         if ((st = solve_dipoles<T>(h, s, pos, bx, pairs, npairs, U, res))) return st;
     } else {
         res->converged = 1;
@@ -1369,6 +1394,66 @@ __global__ void k_self_dq(int n, const double* q, double c, double* dq) {
     if (i < n) dq[i] += c * q[i];
 }
 
+// Half-width cell grid of the cell pass: at least 5 cells of width >= rc/2 per axis (the 5^3
+// stencil then covers every pair within rc), at most 64 per axis.
+bool half_cells(const dmffb_engine* h, const Box& bx, int nc[3]) {
+    const double* m = bx.h;
+    const double V = fabs(det3(m));
+    for (int k = 0; k < 3; ++k) {
+        const double* u = m + 3 * ((k + 1) % 3);
+        const double* w = m + 3 * ((k + 2) % 3);
+        const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+        nc[k] = (int)floor(V / sqrt(cx * cx + cy * cy + cz * cz) / (0.5 * h->rc));
+        if (nc[k] > 64) nc[k] = 64;
+        if (nc[k] < 5) return false;
+    }
+    return true;
+}
+
+// FP32 positions and the counting sort of the atoms into the cells nc (the binning of the list
+// build): cell_start / cell_atoms.
+int bin_cells(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int nc[3]) {
+    const int n = h->n;
+    int st;
+    if (!h->d_pcount) {
+        const int cap = h->n_cap;
+        if ((st = dalloc(h, &h->d_pcount, cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_poff, (cap + 1) * sizeof(int64_t)))) return st;
+        if ((st = dalloc(h, &h->d_atom_cell, cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_atoms, cap * sizeof(int32_t)))) return st;
+    }
+    if (!h->d_posf) {
+        if ((st = dalloc(h, &h->d_posf, 4 * h->n_cap * sizeof(float)))) return st;
+        if ((st = dalloc(h, &h->d_pcount_f, h->n_cap * sizeof(int32_t)))) return st;
+    }
+    const int ncell = nc[0] * nc[1] * nc[2];
+    if (ncell + 1 > h->ncell_cap) {
+        if (h->d_cell_count) { cudaFree(h->d_cell_count); cudaFree(h->d_cell_start); cudaFree(h->d_cell_cursor); }
+        h->ncell_cap = ncell + 1;
+        if ((st = dalloc(h, &h->d_cell_count, h->ncell_cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_start, h->ncell_cap * sizeof(int32_t)))) return st;
+        if ((st = dalloc(h, &h->d_cell_cursor, h->ncell_cap * sizeof(int32_t)))) return st;
+    }
+    size_t need = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, (int32_t*)nullptr, (int32_t*)nullptr, ncell + 1);
+    if (need > h->cub_bytes) {
+        if (h->d_cub) cudaFree(h->d_cub);
+        h->cub_bytes = need;
+        if ((st = dalloc(h, &h->d_cub, need))) return st;
+    }
+    LAUNCH(h, s, KC_NBLIST, k_pos_f32<<<nblk(n, 256), 256, 0, s>>>(n, pos, h->d_posf));
+    CK(cudaMemsetAsync(h->d_cell_count, 0, (ncell + 1) * sizeof(int32_t), s));
+    CK(cudaMemsetAsync(h->d_cell_cursor, 0, (ncell + 1) * sizeof(int32_t), s));
+    LAUNCH(h, s, KC_NBLIST, k_cell_count<<<nblk(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], h->d_atom_cell,
+                                                                     h->d_cell_count));
+    size_t tb = h->cub_bytes;
+    LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_cell_count, h->d_cell_start, ncell + 1, s));
+    LAUNCH(h, s, KC_NBLIST, k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(n, h->d_atom_cell, h->d_cell_start,
+                                                                    h->d_cell_cursor, h->d_cell_atoms));
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
 template <typename T>
 int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const double* box,
                            const int32_t* pairs, int64_t npairs, double* forces, dmffb_classical_result* res) {
@@ -1379,7 +1464,10 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
     memset(res, 0, sizeof(*res));
     const int n = h->n;
     int st;
-    if (nonbonded && !pairs) {
+    // the cell pass: every pair within rc straight from the cell grid of these positions
+    int ncf[3] = {0, 0, 0};
+    const bool cellpass = nonbonded && !pairs && h->cell_pass && h->pbc && !h->want_pgrad && half_cells(h, bx, ncf);
+    if (nonbonded && !pairs && !cellpass) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
         if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
@@ -1398,6 +1486,41 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
             CK(cudaMemsetAsync(h->d_dsig, 0, (size_t)h->ntypes * h->ntypes * sizeof(double), s));
             CK(cudaMemsetAsync(h->d_deps, 0, (size_t)h->ntypes * h->ntypes * sizeof(double), s));
         }
+    }
+    if (cellpass) {
+        if ((st = bin_cells(h, s, pos, bx, ncf))) return st;
+        NbCellArgs<T> c;
+        c.n = n;
+        c.pos = pos;
+        c.posf = h->d_posf;
+        c.boxd = bx;
+        c.rc = h->rc;
+        for (int k = 0; k < 3; ++k) c.nc[k] = ncf[k];
+        c.cell_start = h->d_cell_start;
+        c.cell_atoms = h->d_cell_atoms;
+        c.cov.cov_ptr = h->d_cov_ptr;
+        c.cov.cov_j = h->d_cov_j;
+        c.cov.cov_nb = h->d_cov_nb;
+        c.cov_lo = h->d_cov_lo;
+        c.cov_hi = h->d_cov_hi;
+        c.qT = (const T*)h->d_qT;
+        c.type = h->ntypes > 0 ? h->d_type : nullptr;
+        c.ntypes = h->ntypes;
+        c.sig_tt = (const T*)h->d_sigtt;
+        c.eps_tt = (const T*)h->d_epstt;
+        c.mc = (T)h->ms[5];
+        c.ml = (T)h->mlj[5];
+        c.kappa = (T)h->kappa;
+        c.krf = (T)h->krf;
+        c.crf = (T)h->crf;
+        c.coul = h->coul;
+        c.grad = (T*)h->d_glr;
+        c.scal = h->d_scal;
+        LAUNCH(h, s, KC_PAIR_FULL, k_nb_cells<T><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(c));
+        CK(cudaGetLastError());
+        // rows with a topological scale: the covalent rows within rc, FP64 for FP32 engines
+        pairs = h->d_covrows;
+        npairs = h->n_covrows;
     }
     if (npairs > 0) {
         NbPairArgs<T> a;
@@ -1427,7 +1550,11 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
         a.deps = (pg && h->ntypes > 0) ? h->d_deps : nullptr;
         a.scal = h->d_scal;
         const unsigned nbk = nblk(npairs, 128);
-        if (sizeof(T) == 4) {
+        if (cellpass) {
+            a.cut = h->rc;
+            a.dq = a.dsig = a.deps = nullptr;
+            LAUNCH(h, s, KC_PAIR_FULL_SCALED, k_nb_pair<T, 2><<<nbk, 128, 0, s>>>(a));
+        } else if (sizeof(T) == 4) {
             if ((st = scaled_rows(h, s, pairs, npairs))) return st;
             LAUNCH(h, s, KC_PAIR_FULL, k_nb_pair<T, 1><<<nbk, 128, 0, s>>>(a));
             a.rowmap = h->d_srows;
@@ -1470,6 +1597,7 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
     CK(cudaStreamSynchronize(s));
     prof_collect(h);
     const double* sc = h->h_scal;
+    if (cellpass) res->n_pairs = (int64_t)llround(sc[11]);
     res->e_coul_real = sc[0];
     res->e_lj = sc[1];
     res->e_bond = sc[12];
@@ -1725,6 +1853,7 @@ int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* d) {
     }
     h->cg_key.clear();
     h->params_set = false;
+    h->have_last = false;
     return DMFFB_OK;
 }
 
@@ -1739,7 +1868,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask};
+                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -1758,6 +1887,7 @@ void dmffb_destroy(dmffb_engine* h) {
     if (h->e_fork) cudaEventDestroy(h->e_fork);
     if (h->e_build) cudaEventDestroy(h->e_build);
     if (h->e_join) cudaEventDestroy(h->e_join);
+    if (h->d_bk) cudaFree(h->d_bk);
     delete h;
 }
 
@@ -1767,6 +1897,11 @@ int dmffb_admp_set_params(dmffb_engine* h, const double* Q_local, const double* 
     const int n = h->n;
     // ordered on the engine stream (no device-wide synchronisation: other engines keep running)
     cudaStream_t s = h->s1;
+    h->h_Qloc.assign(Q_local, Q_local + 9 * (size_t)n);
+    if (pol) h->h_pol.assign(pol, pol + n);
+    else h->h_pol.assign(n, 0.0);
+    if (thole) h->h_thole.assign(thole, thole + n);
+    else h->h_thole.assign(n, 0.0);
     CK(cudaMemcpyAsync(h->d_Qloc, Q_local, 9 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     if (pol) CK(cudaMemcpyAsync(h->d_pol, pol, n * sizeof(double), cudaMemcpyHostToDevice, s));
     else CK(cudaMemsetAsync(h->d_pol, 0, n * sizeof(double), s));
@@ -1843,6 +1978,251 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
     if (forces_out) CK(cudaMemcpyAsync(forces_out, h->d_forces, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (h->lpol && U_inout) CK(cudaMemcpyAsync(U_inout, h->d_U, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    return st;
+}
+
+}  // extern "C"
+
+// dE/dU at (pos, box, U) with the engine's current parameters: frames and global multipoles,
+// the CSR and matvec tensors of these positions, then the field pass.
+template <typename T>
+int field_at(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs, int64_t npairs,
+             const double* U, double* field_out) {
+    const int n = h->n;
+    PrepArgs<T> pa;
+    pa.f.n = n;
+    pa.f.pos = pos;
+    pa.f.axis_type = h->d_axis_type;
+    pa.f.axis_idx = h->d_axis_idx;
+    pa.f.box = bx;
+    pa.Qloc = h->d_Qloc;
+    pa.lmax = h->lmax;
+    pa.posT = (T*)h->d_posT;
+    pa.QgT = (T*)h->d_QgT;
+    pa.Qg = h->d_Qg;
+    h->cur_pos = pos;
+    LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
+    int st;
+    if (sizeof(T) == 4 && npairs > 0 && (st = scaled_rows(h, s, pairs, npairs))) return st;
+    // the matvec of U needs this call's CSR and pair tensors (not a previous compute's)
+    if ((st = build_csr(h, s, pairs, npairs))) return st;
+    if ((st = matvec_alloc<T>(h))) return st;
+    return field_eval<T>(h, s, pos, bx, pairs, npairs, U, true, field_out, nullptr, nullptr, nullptr, true);
+}
+
+__global__ void k_lin(int64_t m, double* out, const double* x0, double a, const double* d) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = x0[i] + (d ? a * d[i] : 0.0);
+}
+
+__global__ void k_cdiff(int64_t m, double* out, const double* p, const double* q, double scale) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] = (p[i] - q[i]) * scale;
+}
+
+// Second-order pass at the point of the last compute (see dmffb_admp_backward in the header).
+// With Phi(z) = E(z, U*(z)), z = (positions, box, Q_local, pol, thole) and U* the converged
+// dipoles, the vector-Jacobian product of the first derivatives with a cotangent c is the
+// Hessian-vector product H_Phi c (the Hessian is symmetric).  Implicit differentiation of
+// dE/dU (z, U*(z)) = 0 gives dU*/dz c = dU with
+//     A dU = -g,  A = d2E/dU2 (the dipole-solve matrix),  g = d2E/dU dz c,
+// solved by the engine's CG (no unrolling of the solve), and then
+//     H_Phi c = d2E/dz2 c + d2E/dz dU dU = d/de [dE/dz (z + e c, U* + e dU)] at e = 0.
+// Both directional derivatives are central differences of the engine's analytic first
+// derivatives (dE/dU, forces, box gradient, parameter adjoints) over a step e along c with the
+// pair list fixed; dE/dU and dE/dz are polynomial in U (E is quadratic in U), so the U
+// direction is exact and the truncation error, O(e^2), comes from the z direction alone.
+template <typename T>
+int admp_backward_impl(dmffb_engine* h, cudaStream_t s, const dmffb_admp_cotangent* c, dmffb_admp_second* out) {
+    const int n = h->n;
+    const int64_t n3 = 3 * (int64_t)n, n9 = 9 * (int64_t)n;
+    int st;
+    if ((int64_t)52 * n > h->bk_cap) {
+        if (h->d_bk) cudaFree(h->d_bk);
+        h->d_bk = nullptr;
+        h->bk_cap = (int64_t)52 * n;
+        if ((st = dalloc(h, &h->d_bk, (size_t)h->bk_cap * sizeof(double)))) return st;
+    }
+    double* b = h->d_bk;
+    double *pos_s = b, *U_s = b + n3, *g = b + 2 * n3, *dU = b + 3 * n3, *Fp = b + 4 * n3, *Fm = b + 5 * n3;
+    double* Q0 = b + 6 * n3;
+    double *pol0 = Q0 + n9, *th0 = pol0 + n, *th_s = th0 + n, *Qp = th_s + n, *Qm = Qp + n9;
+    double *pp = Qm + n9, *pm = pp + n, *tp = pm + n, *tm = tp + n;
+    // the point of the last compute
+    const double* pos0 = h->cur_pos;
+    const Box bx0 = h->last_box;
+    const int32_t* pairs = h->last_pairs;
+    const int64_t npairs = h->last_npairs;
+    double* U0 = h->last_U;
+    // step: at most eps of each quantity's own scale along c (1 A for positions and box)
+    std::vector<double> hc;
+    auto maxabs_dev = [&](const double* d, int64_t m, double* out_max) -> int {
+        *out_max = 0.0;
+        if (!d) return DMFFB_OK;
+        hc.resize(m);
+        CK(cudaMemcpyAsync(hc.data(), d, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        for (double v : hc) *out_max = std::max(*out_max, fabs(v));
+        return DMFFB_OK;
+    };
+    auto maxabs_host = [](const std::vector<double>& v) {
+        double m = 0.0;
+        for (double x : v) m = std::max(m, fabs(x));
+        return m;
+    };
+    double mpos, mQ, mpol, mth, mbox = 0.0;
+    if ((st = maxabs_dev(c->pos, n3, &mpos)) || (st = maxabs_dev(c->Q_local, n9, &mQ)) ||
+        (st = maxabs_dev(h->lpol ? c->pol : nullptr, n, &mpol)) || (st = maxabs_dev(h->lpol ? c->thole : nullptr, n, &mth)))
+        return st;
+    for (int k = 0; k < 9; ++k) mbox = std::max(mbox, fabs(c->box[k]));
+    const double sQ = std::max(maxabs_host(h->h_Qloc), 1e-12);
+    const double sp = std::max(maxabs_host(h->h_pol), 1e-12), sth = std::max(maxabs_host(h->h_thole), 1e-12);
+    const double rate = std::max(std::max(std::max(mpos, mbox), std::max(mQ / sQ, mpol / sp)), mth / sth);
+    out->n_iter = 0;
+    out->residual_rms = 0.0;
+    auto zero_out = [&]() -> int {
+        if (out->pos) CK(cudaMemsetAsync(out->pos, 0, n3 * sizeof(double), s));
+        if (out->Q_local) CK(cudaMemsetAsync(out->Q_local, 0, n9 * sizeof(double), s));
+        if (out->pol) CK(cudaMemsetAsync(out->pol, 0, n * sizeof(double), s));
+        if (out->thole) CK(cudaMemsetAsync(out->thole, 0, n * sizeof(double), s));
+        for (int k = 0; k < 9; ++k) out->box[k] = 0.0;
+        CK(cudaStreamSynchronize(s));
+        return DMFFB_OK;
+    };
+    if (!(rate > 0.0)) {
+        out->step = 0.0;
+        return zero_out();
+    }
+    const double eps = sizeof(T) == 8 ? 1e-4 : 3e-3;
+    const double e = eps / rate;
+    out->step = e;
+    // unperturbed parameters
+    CK(cudaMemcpyAsync(Q0, h->d_Qloc, n9 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(pol0, h->d_pol, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(th0, h->h_thole.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    // parameters and positions at z + a c (a = 0 restores the unperturbed parameters)
+    double box_s[9];
+    auto set_point = [&](double a) -> int {
+        LAUNCH(h, s, KC_VEC, k_lin<<<nblk(n3, 256), 256, 0, s>>>(n3, pos_s, pos0, a, c->pos));
+        for (int k = 0; k < 9; ++k) box_s[k] = bx0.h[k] + a * c->box[k];
+        LAUNCH(h, s, KC_VEC, k_lin<<<nblk(n9, 256), 256, 0, s>>>(n9, h->d_Qloc, Q0, a, c->Q_local));
+        if (h->lpol) {
+            LAUNCH(h, s, KC_VEC, k_lin<<<nblk(n, 256), 256, 0, s>>>(n, h->d_pol, pol0, a, c->pol));
+            LAUNCH(h, s, KC_VEC, k_lin<<<nblk(n, 256), 256, 0, s>>>(n, th_s, th0, a, c->thole));
+            LAUNCH(h, s, KC_VEC, k_set_thole<T><<<nblk(n, 128), 128, 0, s>>>(n, h->d_pol, th_s, (T*)h->d_thole,
+                                                                             (T*)h->d_polsix));
+        }
+        CK(cudaGetLastError());
+        return DMFFB_OK;
+    };
+    const bool pg_was = h->admp_pgrad;
+    const int solver_was = h->solver;
+    double bgp[9], bgm[9];
+    auto body = [&]() -> int {
+        Box bxs;
+        if (h->lpol) {
+            // g = d2E/dU dz c: the field at fixed U* on both sides of z
+            if ((st = set_point(e))) return st;
+            make_box(box_s, bxs);
+            if ((st = field_at<T>(h, s, pos_s, bxs, pairs, npairs, U0, Fp))) return st;
+            if ((st = set_point(-e))) return st;
+            make_box(box_s, bxs);
+            if ((st = field_at<T>(h, s, pos_s, bxs, pairs, npairs, U0, Fm))) return st;
+            LAUNCH(h, s, KC_VEC, k_cdiff<<<nblk(n3, 256), 256, 0, s>>>(n3, g, Fp, Fm, 0.5 / e));
+            // tangent (adjoint) solve at z: A dU = -g, by CG from zero
+            if ((st = set_point(0.0))) return st;
+            PrepArgs<T> pa;
+            pa.f.n = n;
+            pa.f.pos = pos0;
+            pa.f.axis_type = h->d_axis_type;
+            pa.f.axis_idx = h->d_axis_idx;
+            pa.f.box = bx0;
+            pa.Qloc = h->d_Qloc;
+            pa.lmax = h->lmax;
+            pa.posT = (T*)h->d_posT;
+            pa.QgT = (T*)h->d_QgT;
+            pa.Qg = h->d_Qg;
+            h->cur_pos = pos0;
+            LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
+            if (sizeof(T) == 4 && npairs > 0 && (st = scaled_rows(h, s, pairs, npairs))) return st;
+            h->solver = DMFFB_SOLVER_CG;
+            dmffb_admp_result r2;
+            memset(&r2, 0, sizeof(r2));
+            if ((st = solve_dipoles<T>(h, s, pos0, bx0, pairs, npairs, dU, &r2, g))) return st;
+            h->solver = solver_was;
+            out->n_iter = r2.n_iter;
+            out->residual_rms = r2.residual_rms;
+        }
+        // d/de of (dE/dpos, dE/dbox, dE/dparams) at (z + e c, U* + e dU)
+        h->admp_pgrad = true;
+        h->fixed_U = true;
+        dmffb_admp_result rp, rm;
+        for (int side = 0; side < 2; ++side) {
+            const double a = side == 0 ? e : -e;
+            if ((st = set_point(a))) return st;
+            if (h->lpol) LAUNCH(h, s, KC_VEC, k_lin<<<nblk(n3, 256), 256, 0, s>>>(n3, U_s, U0, a, dU));
+            dmffb_admp_result* r = side == 0 ? &rp : &rm;
+            if ((st = compute_impl<T>(h, s, pos_s, box_s, pairs, npairs, h->lpol ? U_s : nullptr, side == 0 ? Fp : Fm, r)))
+                return st;
+            double* bg = side == 0 ? bgp : bgm;
+            for (int k = 0; k < 9; ++k) bg[k] = r->box_grad[k];
+            CK(cudaMemcpyAsync(side == 0 ? Qp : Qm, h->d_dQloc, n9 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            if (h->lpol) {
+                CK(cudaMemcpyAsync(side == 0 ? pp : pm, h->d_dpol, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                CK(cudaMemcpyAsync(side == 0 ? tp : tm, h->d_dth, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            }
+        }
+        const double inv = 0.5 / e;
+        // forces are -dE/dpos
+        if (out->pos) LAUNCH(h, s, KC_VEC, k_cdiff<<<nblk(n3, 256), 256, 0, s>>>(n3, out->pos, Fm, Fp, inv));
+        if (out->Q_local) LAUNCH(h, s, KC_VEC, k_cdiff<<<nblk(n9, 256), 256, 0, s>>>(n9, out->Q_local, Qp, Qm, inv));
+        if (out->pol) {
+            if (h->lpol) LAUNCH(h, s, KC_VEC, k_cdiff<<<nblk(n, 256), 256, 0, s>>>(n, out->pol, pp, pm, inv));
+            else CK(cudaMemsetAsync(out->pol, 0, n * sizeof(double), s));
+        }
+        if (out->thole) {
+            if (h->lpol) LAUNCH(h, s, KC_VEC, k_cdiff<<<nblk(n, 256), 256, 0, s>>>(n, out->thole, tp, tm, inv));
+            else CK(cudaMemsetAsync(out->thole, 0, n * sizeof(double), s));
+        }
+        for (int k = 0; k < 9; ++k) out->box[k] = (bgp[k] - bgm[k]) * inv;
+        CK(cudaGetLastError());
+        return DMFFB_OK;
+    };
+    st = body();
+    // restore the engine: parameters, flags and the point of the last compute
+    h->fixed_U = false;
+    h->admp_pgrad = pg_was;
+    h->solver = solver_was;
+    h->have_pgrad = false;  // the last compute's parameter adjoints were overwritten
+    int st2 = set_point(0.0);
+    h->cur_pos = pos0;
+    h->last_box = bx0;
+    h->last_pairs = pairs;
+    h->last_npairs = npairs;
+    h->last_U = U0;
+    h->have_last = true;
+    if (cudaStreamSynchronize(s) != cudaSuccess && !st) st = fail(h, DMFFB_CUDA_ERROR, "second-order pass");
+    return st ? st : st2;
+}
+
+extern "C" {
+
+int dmffb_admp_backward(dmffb_engine* h, void* stream, const dmffb_admp_cotangent* c, dmffb_admp_second* out) {
+    if (!h || h->kind != 0) return fail(h, DMFFB_BAD_ARG, "ADMP engine required");
+    if (!c || !out) return fail(h, DMFFB_BAD_ARG, "null cotangent or output");
+    if (!h->have_last || !h->cur_pos) return fail(h, DMFFB_BAD_ARG, "dmffb_admp_backward needs a preceding compute");
+    int st;
+    if (!h->d_dQloc) {  // allocate the adjoint buffers without switching them on for later computes
+        const bool was = h->admp_pgrad;
+        if ((st = dmffb_admp_set_param_grads(h, 1))) return st;
+        h->admp_pgrad = was;
+    }
+    cudaStream_t caller = (cudaStream_t)stream;
+    CK(cudaEventRecord(h->e_in, caller));
+    CK(cudaStreamWaitEvent(h->s1, h->e_in, 0));
+    st = h->prec == DMFFB_FP32 ? admp_backward_impl<float>(h, h->s1, c, out) : admp_backward_impl<double>(h, h->s1, c, out);
+    cudaEventRecord(h->e_out, h->s1);
+    cudaStreamWaitEvent(caller, h->e_out, 0);
     return st;
 }
 
@@ -1933,6 +2313,24 @@ int dmffb_admp_param_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, d
         if (h->lpol) CK(cudaMemcpyAsync(dE_dthole, h->d_dth, n * sizeof(double), cudaMemcpyDeviceToDevice, cs));
         else CK(cudaMemsetAsync(dE_dthole, 0, n * sizeof(double), cs));
     }
+    return DMFFB_OK;
+}
+
+int dmffb_admp_param_grads_host(dmffb_engine* h, double* dE_dQlocal, double* dE_dpol, double* dE_dthole) {
+    if (!h || h->kind != 0) return fail(h, DMFFB_BAD_ARG, "ADMP engine required");
+    if (!h->have_pgrad) return fail(h, DMFFB_BAD_ARG, "enable dmffb_admp_set_param_grads before compute");
+    cudaStream_t s = h->s1;
+    const size_t n = h->n;
+    if (dE_dQlocal) CK(cudaMemcpyAsync(dE_dQlocal, h->d_dQloc, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (dE_dpol) {
+        if (h->lpol) CK(cudaMemcpyAsync(dE_dpol, h->d_dpol, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        else memset(dE_dpol, 0, n * sizeof(double));
+    }
+    if (dE_dthole) {
+        if (h->lpol) CK(cudaMemcpyAsync(dE_dthole, h->d_dth, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        else memset(dE_dthole, 0, n * sizeof(double));
+    }
+    CK(cudaStreamSynchronize(s));
     return DMFFB_OK;
 }
 
@@ -2373,6 +2771,35 @@ int dmffb_classical_create(const dmffb_classical_desc* d, dmffb_engine** out) {
         (st = dalloc(h, &h->d_dsig, tt * sizeof(double))) || (st = dalloc(h, &h->d_deps, tt * sizeof(double))) ||
         (st = dalloc(h, &h->d_glr, 3 * n * ts)))
         return st;
+    // covalent rows (i < j) and each atom's partner index range, for the cell pass
+    {
+        std::vector<int32_t> rows(3 * std::max<int64_t>(d->n_cov, 1)), lo(n, n), hi(n, -1);
+        for (int64_t r = 0; r < d->n_cov; ++r) {
+            const int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
+            const int a0 = std::min(i, j), a1 = std::max(i, j);
+            rows[3 * r] = a0;
+            rows[3 * r + 1] = a1;
+            rows[3 * r + 2] = d->cov_rows[3 * r + 2];
+            lo[a0] = std::min(lo[a0], a1);
+            hi[a0] = std::max(hi[a0], a1);
+            lo[a1] = std::min(lo[a1], a0);
+            hi[a1] = std::max(hi[a1], a0);
+        }
+        h->n_covrows = d->n_cov;
+        if ((st = dalloc(h, &h->d_covrows, rows.size() * sizeof(int32_t))) ||
+            (st = dalloc(h, &h->d_cov_lo, n * sizeof(int32_t))) || (st = dalloc(h, &h->d_cov_hi, n * sizeof(int32_t))))
+            return st;
+        CK(cudaMemcpyAsync(h->d_covrows, rows.data(), rows.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+        CK(cudaMemcpyAsync(h->d_cov_lo, lo.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+        CK(cudaMemcpyAsync(h->d_cov_hi, hi.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+        CK(cudaStreamSynchronize(h->s1));
+    }
+    return DMFFB_OK;
+}
+
+int dmffb_classical_set_cell_pass(dmffb_engine* h, int32_t enabled) {
+    if (!h || h->kind != 2) return fail(h, DMFFB_BAD_ARG, "classical engine required");
+    h->cell_pass = enabled != 0;
     return DMFFB_OK;
 }
 

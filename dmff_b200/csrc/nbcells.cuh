@@ -1,0 +1,179 @@
+// Lennard-Jones + point-charge Coulomb over the cell grid, without a pair list.
+//
+// The engine's own neighbour list (dmff/common/nblist.py:27-55 semantics: every i < j whose
+// minimum-image distance is < rc, nbond from the covalent map) is, for the classical terms,
+// written once per step and read once by the pair kernel: at 100 000 atoms and rc 10 A that is
+// 61 M rows, 0.74 GB out and back, plus j-side force atomics.  This pass evaluates the same pair
+// set straight from the cell binning of the step's positions:
+//   * one warp per atom i walks the 5^3 stencil of half-width cells as one concatenated
+//     candidate list (the layout of k_pairs_warp3), 32 candidates per batch;
+//   * FP32 prefilter on float positions, the exact FP64 test of the list build (within_rc on the
+//     lower/higher orientation) inside a 2e-3 A band around rc, so the kept set is the list's
+//     set bit for bit;
+//   * pairs with a topological scale (nbond != 0, a covalent partner whose index lies in the
+//     atom's [cov_lo, cov_hi] range) are skipped here: an FP64 pass over the covalent rows
+//     within rc evaluates them (k_nb_pair with a cut-off test);
+//   * every other kept pair is evaluated from both of its atoms: the FP64 minimum-image vector and
+//     distance of k_nb_pair, nb_eval in kernel precision, the force added to atom i only (lane
+//     registers, one warp sum and one store per atom: no atomics), half of the energy and of the
+//     box gradient per visit;
+//   * the count of kept pairs with j > i (scaled ones included) is the list's row count.
+// Energies and the box gradient accumulate in FP64 per lane and meet in one block reduction.
+#pragma once
+#include "classical.cuh"
+#include "nblist.cuh"
+
+namespace dmffb {
+
+template <typename T>
+struct NbCellArgs {
+    int n;
+    const double* pos;        // [3n] FP64
+    const float* posf;        // [4n] FP32 x, y, z (prefilter)
+    Box boxd;
+    double rc;
+    int nc[3];                // half-width cells per axis (>= 5)
+    const int32_t* cell_start;
+    const int32_t* cell_atoms;
+    NbArgs cov;               // covalent-map lookup (cov_ptr / cov_j / cov_nb over i < j)
+    const int32_t* cov_lo;    // [n] smallest / largest covalent partner index (lo > hi: none)
+    const int32_t* cov_hi;
+    const T* qT;              // [n] charges in kernel precision
+    const int32_t* type;      // [n] LJ type or null
+    int ntypes;
+    const T* sig_tt;
+    const T* eps_tt;
+    T mc, ml;                 // scales of nbond 0 (the trailing 1.0 entries)
+    T kappa, krf, crf;
+    int coul;
+    T* grad;                  // [3n] dE/dpos, written once per atom
+    double* scal;             // [0] E_coul, [1] E_lj, [2..10] box gradient, [11] pairs i < j within rc
+};
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
+    constexpr int S = 2, W = 2 * S + 1, NQ = W * W * W;
+    __shared__ int s_beg[kNbWarps][NQ];
+    __shared__ int s_off[kNbWarps][NQ + 1];
+    const int wl = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const bool live = i < a.n;  // warps past the end still take part in the block reduction
+    double red[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) red[k] = 0.0;
+    if (live) {
+        const double* pi = a.pos + 3 * i;
+        const float pix = a.posf[4 * i], piy = a.posf[4 * i + 1], piz = a.posf[4 * i + 2];
+        float hf[9], hif[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { hf[k] = (float)a.boxd.h[k]; hif[k] = (float)a.boxd.hinv[k]; }
+        BoxT<double> bxd;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { bxd.h[k] = a.boxd.h[k]; bxd.hinv[k] = a.boxd.hinv[k]; }
+        const float rlo = (float)(a.rc - 2e-3), rhi = (float)(a.rc + 2e-3);
+        const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
+        int c3[3];
+        cell_of(a.boxd, a.nc, pi, c3);
+        int carry = 0;
+        if (lane == 0) s_off[wl][0] = 0;
+        for (int q0 = 0; q0 < NQ; q0 += 32) {
+            const int q = q0 + lane;
+            int cnt = 0;
+            if (q < NQ) {
+                const int dx = q / (W * W) - S, dy = (q / W) % W - S, dz = q % W - S;
+                const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
+                const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
+                const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
+                const int cc = (cx * a.nc[1] + cy) * a.nc[2] + cz;
+                const int cs = a.cell_start[cc];
+                cnt = a.cell_start[cc + 1] - cs;
+                s_beg[wl][q] = cs;
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (q < NQ) s_off[wl][q + 1] = carry + incl;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncwarp();
+        const int total = carry;
+        const int lo = a.cov_lo[i], hi = a.cov_hi[i];
+        const bool lj = a.type != nullptr;
+        const int ti = lj ? a.type[i] : 0;
+        const T qi = a.qT[i];
+        T g0 = T(0), g1 = T(0), g2 = T(0);
+        int qc = 0;
+        for (int base = 0; base < total; base += 32) {
+            const int t = base + lane;
+            bool keep = false;
+            int j = -1;
+            if (t < total) {
+                while (t >= s_off[wl][qc + 1]) ++qc;
+                j = a.cell_atoms[s_beg[wl][qc] + (t - s_off[wl][qc])];
+                if (j != i) {
+                    const float d0 = a.posf[4 * j] - pix, d1 = a.posf[4 * j + 1] - piy, d2 = a.posf[4 * j + 2] - piz;
+                    bool amb = false;
+                    float sf[3];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const float tt = d0 * hif[q] + d1 * hif[3 + q] + d2 * hif[6 + q];
+                        sf[q] = tt - floorf(tt + 0.5f);
+                        amb |= fabsf(sf[q]) > 0.4999f;
+                    }
+                    const float e0 = sf[0] * hf[0] + sf[1] * hf[3] + sf[2] * hf[6];
+                    const float e1 = sf[0] * hf[1] + sf[1] * hf[4] + sf[2] * hf[7];
+                    const float e2 = sf[0] * hf[2] + sf[1] * hf[5] + sf[2] * hf[8];
+                    const float r2 = e0 * e0 + e1 * e1 + e2 * e2;
+                    if (!amb && r2 < rlo2) keep = true;
+                    else if (!amb && r2 > rhi2) keep = false;
+                    else keep = j > i ? within_rc(a.boxd, pi, a.pos + 3 * j, a.rc)
+                                      : within_rc(a.boxd, a.pos + 3 * j, pi, a.rc);
+                }
+            }
+            if (keep && j > i) red[11] += 1.0;
+            // topologically scaled pairs belong to the FP64 covalent pass
+            if (keep && j >= lo && j <= hi) {
+                const int nbd = j > i ? lookup_nbond(a.cov, i, j) : lookup_nbond(a.cov, j, i);
+                if (nbd != 0) keep = false;
+            }
+            if (keep) {
+                // the pair geometry of k_nb_pair: FP64 minimum image of r_i - r_j
+                double dr[3] = {pi[0] - a.pos[3 * j], pi[1] - a.pos[3 * j + 1], pi[2] - a.pos[3 * j + 2]};
+                double nimg[3];
+                pbc_shift(bxd, dr[0], dr[1], dr[2], nimg);
+                const double r = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+                int tp = 0;
+                if (lj) tp = ti * a.ntypes + a.type[j];
+                T ec, dec, phi, el, del, ds, dp;
+                nb_eval<T>((T)r, qi * a.qT[j], a.mc, a.ml, lj ? a.sig_tt[tp] : T(0), lj ? a.eps_tt[tp] : T(0), lj,
+                           a.coul, a.kappa, a.krf, a.crf, ec, dec, phi, el, del, ds, dp);
+                red[0] += 0.5 * (double)ec;
+                red[1] += 0.5 * (double)el;
+                const double de = (double)dec + (double)del;
+                const double s = de / r;
+                g0 += (T)(s * dr[0]);
+                g1 += (T)(s * dr[1]);
+                g2 += (T)(s * dr[2]);
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) red[2 + 3 * k + c] -= 0.5 * nimg[k] * s * dr[c];
+            }
+        }
+        g0 = warp_sum(g0);
+        g1 = warp_sum(g1);
+        g2 = warp_sum(g2);
+        if (lane == 0) {
+            a.grad[3 * i] = g0;
+            a.grad[3 * i + 1] = g1;
+            a.grad[3 * i + 2] = g2;
+        }
+    }
+    block_reduce_add<12>(red, a.scal);
+}
+
+}  // namespace dmffb

@@ -242,6 +242,45 @@ class AdmpEngine:
     def multipole_grads(self):
         return self.param_grads()["Q_global"]
 
+    def backward(self, c_pos=None, c_box=None, c_Q=None, c_pol=None, c_thole=None):
+        """Second-order pass at the last compute (dmffb_admp_backward): the derivatives of
+        <c_pos, dE/dpos> + <c_box, dE/dbox> + <c_Q, dE/dQ_local> + <c_pol, dE/dpol> + <c_thole, dE/dthole>
+        with respect to positions, box, Q_local [n, 9], pol and thole, the induced dipoles following
+        (one adjoint CG solve).  Cotangents: cuda float64 tensors (or None); returns a dict of
+        tensors (box: [3, 3] host) plus the adjoint solve's iteration count and the step used."""
+        dev = self.device
+        n = self.n
+
+        def dv(t, shape):
+            if t is None:
+                return None
+            return t.detach().to(device=dev, dtype=torch.float64).reshape(shape).contiguous()
+
+        cp, cq = dv(c_pos, (n, 3)), dv(c_Q, (n, 9))
+        cpo, cth = dv(c_pol, (n,)), dv(c_thole, (n,))
+        c = L.AdmpCotangent()
+        c.pos = cp.data_ptr() if cp is not None else None
+        c.Q_local = cq.data_ptr() if cq is not None else None
+        c.pol = cpo.data_ptr() if cpo is not None else None
+        c.thole = cth.data_ptr() if cth is not None else None
+        if c_box is not None:
+            b = np.asarray(c_box.detach().cpu() if torch.is_tensor(c_box) else c_box, np.float64).reshape(9)
+            for k in range(9):
+                c.box[k] = float(b[k])
+        out = {"pos": torch.empty((n, 3), dtype=torch.float64, device=dev),
+               "Q_local": torch.empty((n, 9), dtype=torch.float64, device=dev),
+               "pol": torch.empty(n, dtype=torch.float64, device=dev),
+               "thole": torch.empty(n, dtype=torch.float64, device=dev)}
+        o = L.AdmpSecond()
+        o.pos, o.Q_local = out["pos"].data_ptr(), out["Q_local"].data_ptr()
+        o.pol, o.thole = out["pol"].data_ptr(), out["thole"].data_ptr()
+        s = torch.cuda.current_stream(dev)
+        self._check(self.lib.dmffb_admp_backward(self.h, ctypes.c_void_p(s.cuda_stream), ctypes.byref(c),
+                                                 ctypes.byref(o)))
+        out["box"] = torch.tensor(list(o.box), dtype=torch.float64).reshape(3, 3)
+        out["n_iter"], out["residual_rms"], out["step"] = int(o.n_iter), float(o.residual_rms), float(o.step)
+        return out
+
     def build_neighbors(self, pos, box, rc, capacity=None):
         """All i<j within rc (FP64 minimum-image test) as a cuda int32 [np,3] tensor sorted by i."""
         b = self._box(box)
@@ -478,6 +517,11 @@ class ClassicalEngine:
         if bool(on) != self._pgrad:
             self._check(self.lib.dmffb_classical_set_param_grads(self.h, int(bool(on))))
             self._pgrad = bool(on)
+
+    def set_cell_pass(self, on=True):
+        """Computes without pairs evaluate every pair within rc straight from the cell grid of the
+        positions given (no pair list written); see dmffb_classical_set_cell_pass."""
+        self._check(self.lib.dmffb_classical_set_cell_pass(self.h, int(bool(on))))
 
     def compute(self, pos, box, pairs=None):
         """Returns (result, forces); forces = -dE/dpos (kJ/mol/A), device [n, 3] FP64."""

@@ -296,33 +296,59 @@ def polymer_water_box(n_chains, n_beads, n_waters, L, seed=4, rc=10.0, ethresh=1
                 mscales_lj=np.array([0.0, 0.0, 0.5, 1.0, 1.0, 1.0]))
 
 
-def water_positions_fast(n_waters, L, rng, min_inter=1.7, max_rounds=100):
+def water_positions_fast(n_waters, L, rng, min_inter=1.7, max_rounds=400):
     """Vectorised variant of ``water_positions`` for streams of many boxes: lattice centres with
     U(+-0.3 A) jitter and uniform random orientations; in rounds, one molecule of every pair with
     an intermolecular atom contact below ``min_inter`` (periodic k-d tree query; the later one in
-    even rounds, the earlier one in odd rounds) gets a new jitter and orientation, until no contact
-    is left."""
+    even rounds, the earlier one in odd rounds) gets a new jitter and orientation.  After 50 rounds
+    a molecule still in contact also moves to the free lattice site with the fewest occupied
+    neighbours when the box has one (a
+    seeded subset of the m^3 sites is used when n < m^3), and from round 100 on the re-drawn
+    molecules sit on their sites without jitter.  Raises when contacts remain after
+    ``max_rounds`` rounds, so that no box with overlapping molecules is ever returned."""
     from scipy.spatial import cKDTree
     m = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9))
-    sites = np.array([(i, j, k) for i in range(m) for j in range(m) for k in range(m)], dtype=np.float64)
+    all_sites = np.array([(i, j, k) for i in range(m) for j in range(m) for k in range(m)], dtype=np.float64)
+    used = np.arange(m ** 3)
     if n_waters < m ** 3:
-        sites = sites[np.sort(rng.choice(m ** 3, n_waters, replace=False))]
-    centers = (sites + 0.5) * (L / m) + rng.uniform(-0.3, 0.3, size=(n_waters, 3))
+        used = np.sort(rng.choice(m ** 3, n_waters, replace=False))
+    free = np.setdiff1d(np.arange(m ** 3), used)
+    base = (all_sites[used] + 0.5) * (L / m)
+    centers = base + rng.uniform(-0.3, 0.3, size=(n_waters, 3))
     body = _body()
     R = _random_rotations(rng, n_waters)
     pos = centers[:, None, :] + np.einsum("nij,aj->nai", R, body)
-    base = (sites + 0.5) * (L / m)
     for rnd in range(max_rounds):
         flat = pos.reshape(-1, 3) % L
         pr = cKDTree(flat, boxsize=L).query_pairs(min_inter, output_type="ndarray")
         mol = pr // 3
         mol = mol[mol[:, 0] != mol[:, 1]]
         if len(mol) == 0:
-            break
+            return pos.reshape(-1, 3)
         bad = np.unique(mol.max(axis=1) if rnd % 2 == 0 else mol.min(axis=1))
-        centers[bad] = base[bad] + rng.uniform(-0.3, 0.3, size=(len(bad), 3))
+        if rnd >= 50 and len(free):
+            # move to the free sites with the fewest occupied face neighbours (ties at random)
+            occ = np.zeros(m ** 3, dtype=bool)
+            occ[used] = True
+            for mv in rng.permutation(bad)[: len(free)]:
+                fs = all_sites[free].astype(np.int64)
+                cnt = np.zeros(len(free), dtype=np.int64)
+                for ax in range(3):
+                    for sh in (-1, 1):
+                        nb_ = fs.copy()
+                        nb_[:, ax] = (nb_[:, ax] + sh) % m
+                        cnt += occ[(nb_[:, 0] * m + nb_[:, 1]) * m + nb_[:, 2]]
+                best = np.flatnonzero(cnt == cnt.min())
+                pick = best[rng.integers(len(best))]
+                occ[used[mv]] = False
+                occ[free[pick]] = True
+                used[mv], free[pick] = free[pick], used[mv]
+                base[mv] = (all_sites[used[mv]] + 0.5) * (L / m)
+        jitter = 0.3 if rnd < 100 else 0.0  # late rounds: the re-drawn molecules sit on their sites
+        centers[bad] = base[bad] + rng.uniform(-jitter, jitter, size=(len(bad), 3))
         pos[bad] = centers[bad][:, None, :] + np.einsum("nij,aj->nai", _random_rotations(rng, len(bad)), body)
-    return pos.reshape(-1, 3)
+    raise RuntimeError(f"water_positions_fast: contacts below {min_inter} A remain after {max_rounds} rounds "
+                       f"({n_waters} waters, L = {L:.2f} A)")
 
 
 def serving_system(n_waters, index, density=0.0334, rc=8.0, ethresh=5e-4, lmax=2, seed=3):

@@ -137,8 +137,49 @@ int dmffb_admp_set_zero_guess(dmffb_engine* h, int32_t enabled);
  * dE/dthole [n]. */
 int dmffb_admp_param_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal,
                            double* dE_dpol, double* dE_dthole);
+/* The same adjoints copied to HOST arrays (dE/dQ_local [n*9], dE/dpol [n], dE/dthole [n], each may
+ * be NULL): for callers of dmffb_admp_compute_host that hold no device memory. */
+int dmffb_admp_param_grads_host(dmffb_engine* h, double* dE_dQlocal, double* dE_dpol, double* dE_dthole);
 /* dE/dQ_global and dE/dQ_local only (same requirements as dmffb_admp_param_grads). */
 int dmffb_admp_multipole_grads(dmffb_engine* h, void* stream, double* dE_dQglobal, double* dE_dQlocal);
+
+/* Second-order pass: the vector-Jacobian product through the first derivatives of the last
+ * dmffb_admp_compute, i.e. the derivatives of
+ *     L = <c.pos, dE/dpos> + <c.box, dE/dbox> + <c.Q_local, dE/dQ_local> + <c.pol, dE/dpol>
+ *         + <c.thole, dE/dthole>
+ * with respect to positions, box and every atom's Q_local / pol / thole, with the induced dipoles
+ * following their parameters and positions (total derivatives of the converged solution).  This
+ * is what a loss on forces or on the virial needs for its parameter gradients (force matching,
+ * dmff/optimize.py:30-84 over jax.grad of forces); the reference's jax.grad cannot give it because
+ * its dipole solve is stop-gradiented (dmff/admp/pme.py:212-213, 363-371).  The dipole response
+ * comes from one adjoint linear solve with the engine's CG (A dU = -d2E/dU dz c, A the dipole
+ * matrix), not from unrolling the iteration; the directional derivatives of the engine's analytic
+ * first derivatives along c are central differences with a step of 1e-4 (FP64 engines; 3e-3 for
+ * FP32) of each quantity's own scale (1 A for positions and box), the pair list held fixed.
+ * Requirements: a preceding dmffb_admp_compute whose positions, pairs and U_inout arrays still
+ * hold the values of that call, converged dipoles (CG solver), the same parameters.  The pass
+ * overwrites the last compute's parameter adjoints (dmffb_admp_param_grads needs a new compute).
+ * Device arrays; each cotangent and each output may be NULL (zero / not wanted). */
+typedef struct {
+    const double* pos;      /* [n*3] cotangent of dE/dpos (= -forces) */
+    double box[9];          /* cotangent of dE/dbox (host) */
+    const double* Q_local;  /* [n*9] cotangent of dE/dQ_local */
+    const double* pol;      /* [n] */
+    const double* thole;    /* [n] */
+} dmffb_admp_cotangent;
+
+typedef struct {
+    double* pos;          /* [n*3] dL/dpos */
+    double box[9];        /* dL/dbox (host) */
+    double* Q_local;      /* [n*9] dL/dQ_local */
+    double* pol;          /* [n] dL/dpol */
+    double* thole;        /* [n] dL/dthole */
+    int32_t n_iter;       /* CG iterations of the adjoint solve (0 without polarization) */
+    double residual_rms;  /* its final RMS residual */
+    double step;          /* the finite-difference step along c */
+} dmffb_admp_second;
+
+int dmffb_admp_backward(dmffb_engine* h, void* stream, const dmffb_admp_cotangent* c, dmffb_admp_second* out);
 
 /* Cell-list neighbour build: NeighborList.allocate (dmff/common/nblist.py:27-55) semantics —
  * all i < j with minimum-image distance < rc (FP64 test), nbond from the covalent map.
@@ -269,6 +310,14 @@ int dmffb_classical_set_param_grads(dmffb_engine* h, int32_t enabled);
 int dmffb_classical_compute(dmffb_engine* h, void* stream, const double* pos, const double* box,
                             const int32_t* pairs, int64_t npairs, double* forces_out,
                             dmffb_classical_result* result);
+/* Cell pass on/off for the following computes (off by default).  When on, a compute with pairs ==
+ * NULL evaluates every pair within rc at the positions it is given straight from a cell binning of
+ * those positions, without writing a pair list: the same pairs (the list build's exact FP64
+ * cut-off test), scales and results as dmffb_admp_build_neighbors followed by a compute on the
+ * engine's list.  Pairs with a topological scale run in FP64 from the covalent rows.  Needs
+ * periodic boxes at least 5 half cut-offs wide; parameter adjoints and narrower boxes take the
+ * list path.  No counterpart in the reference (its potentials always take a pair list). */
+int dmffb_classical_set_cell_pass(dmffb_engine* h, int32_t enabled);
 /* Parameter adjoints of the last compute (param grads enabled), device arrays, each may be NULL:
  * dE_dq [n], dE_dsig [n_types^2], dE_deps [n_types^2], dE_dbond / dE_dangle / dE_dtorsion
  * [n_terms*2] = (dE/dk, dE/d(r0 | theta0 | psi)). */

@@ -1,8 +1,9 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference checkout.
 
-Run from the repository root (needs the read-only reference tree at /root/reference):
+Run from the repository root with the path of a reference checkout (the argument, or the
+environment variable DMFF_REFERENCE):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <path to deepmodeling/DMFF>
 
 It copies the reference's small force-field XML / PDB inputs, converts the 996-water box
 to a compact .npz, extracts the reference's golden energies (test files and example
@@ -18,10 +19,11 @@ import os
 import pickle
 import re
 import shutil
+import sys
 
 import numpy as np
 
-REF = "/root/reference"
+REF = None  # the reference checkout, set by main() from argv or DMFF_REFERENCE
 HERE = os.path.dirname(os.path.abspath(__file__))
 DATA = os.path.join(HERE, "data")
 
@@ -86,6 +88,11 @@ def read_pdb_positions(path):
 
 
 def main():
+    global REF
+    REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DMFF_REFERENCE")
+    if not REF or not os.path.isdir(REF):
+        sys.exit("usage: python tests/golden/make_golden.py <path to a deepmodeling/DMFF checkout> "
+                 "(or set DMFF_REFERENCE)")
     os.makedirs(DATA, exist_ok=True)
     wf = f"{REF}/examples/water_fullpol"
     copies = {

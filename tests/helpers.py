@@ -86,3 +86,53 @@ def classical_oracle(H, pos_nm, box_nm, pairs, names=None):
             E = E + R.lj_energy(pos, box, pairs, P["epsilon"], P["sigma"], g.map_prm, g.mscales_lj, pbc=g.pbc,
                                 map_nbfix=g.nbfix, epsfix=P["epsilon_nbfix"], sigfix=P["sigma_nbfix"])
     return E, pos, box
+
+
+def oracle_force_loss_grads(sysd, pairs, w, tol=1e-12):
+    """Exact derivatives of L = <w, dE/dpos> with respect to positions, Q_local, pol and thole, the
+    converged induced dipoles following, by implicit differentiation through the float64 oracle
+    (double autograd): with E_U(z, U*) = 0 and A = d2E/dU2,
+        dL/dz = d/dz <w, E_x>|_U - d/dz <lam, E_U>|_U,   A lam = d/dU <w, E_x>,
+    lam solved by CG on exact A-products (E is quadratic in U)."""
+    import oracle.admp_ref as R
+    f = R.ADMPPmeForce(sysd["box"], sysd["axis_types"], sysd["axis_indices"], sysd["rc"], sysd["ethresh"],
+                       sysd["lmax"], True, kappa=sysd["kappa"], K=sysd["K"])
+    pos = torch.tensor(sysd["pos"], dtype=torch.float64, requires_grad=True)
+    box = torch.tensor(sysd["box"], dtype=torch.float64)
+    Q = torch.tensor(sysd["Q_local"], dtype=torch.float64, requires_grad=True)
+    pol = torch.tensor(sysd["pol"], dtype=torch.float64, requires_grad=True)
+    th = torch.tensor(sysd["thole"], dtype=torch.float64, requires_grad=True)
+    sc = tuple(torch.tensor(sysd[k]) for k in ("mscales", "pscales", "dscales"))
+    Ustar, ok, _ = f.solve_Uind_cg(pos.detach(), box, pairs, Q.detach(), pol.detach(), th.detach(), *sc, tol=tol)
+    assert ok
+    U = Ustar.detach().clone().requires_grad_(True)
+    E = f.energy_fn(pos, box, pairs, Q, U, pol, th, *sc)
+    gx, gU = torch.autograd.grad(E, (pos, U), create_graph=True)
+    w = torch.as_tensor(w, dtype=torch.float64)
+    Lx = (w * gx).sum()
+    (rhs,) = torch.autograd.grad(Lx, U, retain_graph=True)
+
+    def Ap(p):
+        (r,) = torch.autograd.grad((gU * p).sum(), U, retain_graph=True)
+        return r
+
+    Minv = (torch.clamp(pol.detach(), min=1e-8) / R.DIELECTRIC)[:, None]
+    lam = torch.zeros_like(rhs)
+    r = rhs.clone()
+    z = Minv * r
+    p = z.clone()
+    rz = (r * z).sum()
+    for _ in range(500):
+        if float(torch.sqrt((r * r).mean())) < 1e-13 * max(float(torch.sqrt((rhs * rhs).mean())), 1e-300):
+            break
+        q = Ap(p)
+        alpha = rz / (p * q).sum()
+        lam = lam + alpha * p
+        r = r - alpha * q
+        z = Minv * r
+        rz_new = (r * z).sum()
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+    total = Lx - (lam.detach() * gU).sum()
+    gpos, gQ, gpol, gth = torch.autograd.grad(total, (pos, Q, pol, th))
+    return dict(L=float(Lx.detach()), pos=gpos.numpy(), Q=gQ.numpy(), pol=gpol.numpy(), thole=gth.numpy())
