@@ -36,7 +36,8 @@ EXPORTED = [
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
     "dmffb_classical_set_cell_pass",
     "dmffb_set_graphs", "dmffb_admp_backward", "dmffb_admp_param_grads_host", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
-    "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy",
+    "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy", "dmffb_md_force_create",
+    "dmffb_md_force_execute", "dmffb_md_force_last_result", "dmffb_md_force_dipoles", "dmffb_md_force_destroy",
 ]
 
 DMFFB_COUL_NONE = 0
@@ -111,6 +112,19 @@ class AdmpSecond(ctypes.Structure):
         ("n_iter", ctypes.c_int32),
         ("residual_rms", ctypes.c_double),
         ("step", ctypes.c_double),
+    ]
+
+
+class MdContext(ctypes.Structure):
+    _fields_ = [
+        ("posq", ctypes.c_void_p),
+        ("posq_double", ctypes.c_int32),
+        ("force_buffer", ctypes.c_void_p),
+        ("atom_index", ctypes.c_void_p),
+        ("num_atoms", ctypes.c_int32),
+        ("padded_num_atoms", ctypes.c_int32),
+        ("box_nm", ctypes.c_double * 9),
+        ("stream", ctypes.c_void_p),
     ]
 
 
@@ -225,7 +239,7 @@ class Request(ctypes.Structure):
 
 # C struct name of each ctypes mirror (layout checked against the header by the CPU tests)
 STRUCTS = {"dmffb_admp_desc": AdmpDesc, "dmffb_admp_result": AdmpResult, "dmffb_admp_cotangent": AdmpCotangent,
-           "dmffb_admp_second": AdmpSecond, "dmffb_disp_desc": DispDesc,
+           "dmffb_admp_second": AdmpSecond, "dmffb_md_context": MdContext, "dmffb_disp_desc": DispDesc,
            "dmffb_disp_result": DispResult, "dmffb_classical_desc": ClassicalDesc,
            "dmffb_classical_result": ClassicalResult, "dmffb_server_desc": ServerDesc, "dmffb_request": Request}
 
@@ -288,11 +302,17 @@ def load():
     lib.dmffb_server_destroy.argtypes = [vp]
     lib.dmffb_server_clock.argtypes = [vp]
     lib.dmffb_request_footprint.argtypes = [i32, dbl, P(i32), dbl, i32]
+    lib.dmffb_md_force_create.argtypes = [P(AdmpDesc), vp, vp, vp, P(vp)]
+    lib.dmffb_md_force_execute.argtypes = [vp, P(MdContext), i32, P(dbl)]
+    lib.dmffb_md_force_last_result.argtypes = [vp, P(AdmpResult)]
+    lib.dmffb_md_force_dipoles.argtypes = [vp, vp, vp]
+    lib.dmffb_md_force_destroy.argtypes = [vp]
     for name in EXPORTED:
         if name not in ("dmffb_destroy", "dmffb_last_error", "dmffb_server_destroy", "dmffb_server_clock",
-                        "dmffb_request_footprint"):
+                        "dmffb_request_footprint", "dmffb_md_force_destroy"):
             getattr(lib, name).restype = ctypes.c_int
     lib.dmffb_server_destroy.restype = None
+    lib.dmffb_md_force_destroy.restype = None
     lib.dmffb_server_clock.restype = dbl
     lib.dmffb_request_footprint.restype = i64
     _lib = lib

@@ -6,5 +6,5 @@ OUT="$HERE/../libdmffb200.so"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
 "$NVCC" -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -std=c++17 \
     -Xcompiler -fPIC -shared ${DMFFB_NVCC_EXTRA} \
-    -o "$OUT" "$HERE/engine.cu" "$HERE/noalloc.cu" "$HERE/serving.cpp" -lcufft -lpthread
+    -o "$OUT" "$HERE/engine.cu" "$HERE/noalloc.cu" "$HERE/md_force.cu" "$HERE/serving.cpp" -lcufft -lpthread
 echo "built $OUT"

@@ -13,12 +13,13 @@
 //   * pairs with a topological scale (nbond != 0, a covalent partner whose index lies in the
 //     atom's [cov_lo, cov_hi] range) are skipped here: an FP64 pass over the covalent rows
 //     within rc evaluates them (k_nb_pair with a cut-off test);
-//   * every other kept pair is evaluated from both of its atoms: the FP64 minimum-image vector and
-//     distance of k_nb_pair, nb_eval in kernel precision, the force added to atom i only (lane
-//     registers, one warp sum and one store per atom: no atomics), half of the energy and of the
-//     box gradient per visit;
+//   * every other kept pair is queued in shared memory and evaluated 32 at a time (every lane
+//     busy) from both of its atoms: nb_eval in kernel precision on the FP64 minimum-image vector
+//     and distance of k_nb_pair, the force added to atom i only (lane registers, one warp sum and one store per atom: no atomics), half of the energy
+//     and of the box gradient per visit;
 //   * the count of kept pairs with j > i (scaled ones included) is the list's row count.
-// Energies and the box gradient accumulate in FP64 per lane and meet in one block reduction.
+// Energies and the box gradient accumulate per lane (about 40 pairs each) and meet in an FP64 block
+// reduction.
 #pragma once
 #include "classical.cuh"
 #include "nblist.cuh"
@@ -50,11 +51,47 @@ struct NbCellArgs {
     double* scal;             // [0] E_coul, [1] E_lj, [2..10] box gradient, [11] pairs i < j within rc
 };
 
+// One kept pair (i, j) seen from atom i: energy halves, box-gradient halves and the force on i.
+template <typename T>
+__device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int j, const double* pi, float pix,
+                                             float piy, float piz, const float hf[9], const float hif[9],
+                                             const BoxT<double>& bxd, bool lj, int ti, T qi, T& g0, T& g1, T& g2,
+                                             float (&acc)[11]) {
+    // the pair geometry of k_nb_pair: FP64 minimum image, then kernel precision
+    T e[3], r;
+    T nn[3];
+    {
+        double dr[3] = {a.pos[3 * j] - pi[0], a.pos[3 * j + 1] - pi[1], a.pos[3 * j + 2] - pi[2]};
+        double nd[3];
+        pbc_shift(bxd, dr[0], dr[1], dr[2], nd);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { e[c] = (T)dr[c]; nn[c] = (T)nd[c]; }
+        r = (T)sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+    }
+    int tp = 0;
+    if (lj) tp = ti * a.ntypes + a.type[j];
+    T ec, dec, phi, el, del, ds, dp;
+    nb_eval<T>(r, qi * a.qT[j], a.mc, a.ml, lj ? a.sig_tt[tp] : T(0), lj ? a.eps_tt[tp] : T(0), lj, a.coul, a.kappa,
+               a.krf, a.crf, ec, dec, phi, el, del, ds, dp);
+    // e = r_j - r_i (minimum image); dE/dr_i = -(dE/dr / r) e; image counts of r_i - r_j are -nn
+    const T s = (dec + del) / r;
+    g0 -= s * e[0];
+    g1 -= s * e[1];
+    g2 -= s * e[2];
+    acc[0] += (float)(T(0.5) * ec);
+    acc[1] += (float)(T(0.5) * el);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[2 + 3 * k + c] -= (float)(T(0.5) * nn[k] * s * e[c]);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
     constexpr int S = 2, W = 2 * S + 1, NQ = W * W * W;
     __shared__ int s_beg[kNbWarps][NQ];
     __shared__ int s_off[kNbWarps][NQ + 1];
+    __shared__ int s_q[kNbWarps][64];  // kept candidates waiting for a full 32-lane batch
     const int wl = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -106,6 +143,11 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
         const int ti = lj ? a.type[i] : 0;
         const T qi = a.qT[i];
         T g0 = T(0), g1 = T(0), g2 = T(0);
+        float acc[11];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) acc[k] = 0.f;
+        const unsigned lt = (1u << lane) - 1u;
+        int qn = 0;  // queued kept candidates (warp-uniform)
         int qc = 0;
         for (int base = 0; base < total; base += 32) {
             const int t = base + lane;
@@ -140,30 +182,23 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
                 const int nbd = j > i ? lookup_nbond(a.cov, i, j) : lookup_nbond(a.cov, j, i);
                 if (nbd != 0) keep = false;
             }
-            if (keep) {
-                // the pair geometry of k_nb_pair: FP64 minimum image of r_i - r_j
-                double dr[3] = {pi[0] - a.pos[3 * j], pi[1] - a.pos[3 * j + 1], pi[2] - a.pos[3 * j + 2]};
-                double nimg[3];
-                pbc_shift(bxd, dr[0], dr[1], dr[2], nimg);
-                const double r = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
-                int tp = 0;
-                if (lj) tp = ti * a.ntypes + a.type[j];
-                T ec, dec, phi, el, del, ds, dp;
-                nb_eval<T>((T)r, qi * a.qT[j], a.mc, a.ml, lj ? a.sig_tt[tp] : T(0), lj ? a.eps_tt[tp] : T(0), lj,
-                           a.coul, a.kappa, a.krf, a.crf, ec, dec, phi, el, del, ds, dp);
-                red[0] += 0.5 * (double)ec;
-                red[1] += 0.5 * (double)el;
-                const double de = (double)dec + (double)del;
-                const double s = de / r;
-                g0 += (T)(s * dr[0]);
-                g1 += (T)(s * dr[1]);
-                g2 += (T)(s * dr[2]);
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) red[2 + 3 * k + c] -= 0.5 * nimg[k] * s * dr[c];
+            // queue the kept candidates; evaluate them 32 at a time with every lane busy
+            const unsigned mk = __ballot_sync(0xffffffffu, keep);
+            if (keep) s_q[wl][qn + __popc(mk & lt)] = j;
+            qn += __popc(mk);
+            __syncwarp();
+            if (qn >= 32) {
+                nb_cell_pair<T>(a, i, s_q[wl][lane], pi, pix, piy, piz, hf, hif, bxd, lj, ti, qi, g0, g1, g2, acc);
+                __syncwarp();
+                if (lane < qn - 32) s_q[wl][lane] = s_q[wl][32 + lane];
+                qn -= 32;
+                __syncwarp();
             }
         }
+        if (lane < qn)
+            nb_cell_pair<T>(a, i, s_q[wl][lane], pi, pix, piy, piz, hf, hif, bxd, lj, ti, qi, g0, g1, g2, acc);
+#pragma unroll
+        for (int k = 0; k < 11; ++k) red[k] = (double)acc[k];
         g0 = warp_sum(g0);
         g1 = warp_sum(g1);
         g2 = warp_sum(g2);

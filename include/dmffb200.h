@@ -391,6 +391,41 @@ int64_t dmffb_request_footprint(int32_t n_atoms, double rc, const int32_t K[3], 
 int dmffb_server_prewarm(dmffb_server* srv, dmffb_request* reqs, int32_t n_reqs);
 void dmffb_server_destroy(dmffb_server* srv);
 
+/* ---------------------------------------------------------------------------------------
+ * MD-platform force: the polarizable ADMP engine inside an MD engine's step, in the device
+ * layout of OpenMM's CUDA platform.  Replaces the reference's OpenMM plugin kernel
+ * (backend/openmm_dmff_plugin/platforms/cuda/src/CudaDMFFKernels.cpp:118-220, addForces in
+ * kernels/DMFFForce.cu:1-9), which moves positions and forces through the host every step and
+ * keeps the induced dipoles on the host (last_U_ind, :193-195).  Here positions are gathered
+ * from the platform's posq array on the device, the neighbour list is built on the device, the
+ * dipoles stay in device memory from one step to the next (each solve starts from the previous
+ * step's), and the forces are added to the platform's fixed-point force buffer by an epilogue
+ * kernel.  include/dmffb200_openmm.hpp holds the C++ adapter an OpenMM kernel class wraps. */
+typedef struct {
+    const void* posq;           /* device [padded_num_atoms] float4 (double4 if posq_double): x, y, z in nm */
+    int32_t posq_double;
+    long long* force_buffer;    /* device [3 * padded_num_atoms]: force (kJ/mol/nm) * 2^32 as int64, x block first */
+    const int32_t* atom_index;  /* device [num_atoms]: the system atom held in each slot (NULL: identity) */
+    int32_t num_atoms, padded_num_atoms;
+    double box_nm[9];           /* periodic box, rows = lattice vectors, nm */
+    void* stream;               /* the platform's cudaStream_t */
+} dmffb_md_context;
+
+typedef struct dmffb_md_force dmffb_md_force;
+
+/* desc in Angstrom (as dmffb_admp_create); Q_local [n*9], pol [n], thole [n] host arrays. */
+int dmffb_md_force_create(const dmffb_admp_desc* desc, const double* Q_local, const double* pol, const double* thole,
+                          dmffb_md_force** out);
+/* One step: energy (kJ/mol) out; with include_forces the forces are added to ctx->force_buffer.
+ * Returns DMFFB_NOT_CONVERGED as a warning (results written). */
+int dmffb_md_force_execute(dmffb_md_force* f, const dmffb_md_context* ctx, int32_t include_forces,
+                           double* energy_kjmol);
+/* The engine result of the last step (CG iterations, energy terms, box gradient in kJ/mol/A). */
+int dmffb_md_force_last_result(const dmffb_md_force* f, dmffb_admp_result* out);
+/* Copy of the induced dipoles kept for the next step (device [n*3], e*A, system atom order). */
+int dmffb_md_force_dipoles(dmffb_md_force* f, void* stream, double* U_out);
+void dmffb_md_force_destroy(dmffb_md_force* f);
+
 /* Neighbour-list build that allocates no device memory.  No counterpart in the reference (DMFF
  * has no C ABI); same result as dmffb_build_neighbors for callers that cannot allocate on
  * demand: a host (an MD platform such as an OpenMM context, a framework with a caching
