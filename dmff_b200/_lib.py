@@ -35,10 +35,14 @@ EXPORTED = [
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
     "dmffb_classical_set_cell_pass",
-    "dmffb_set_graphs", "dmffb_admp_backward", "dmffb_admp_param_grads_host", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
+    "dmffb_set_graphs", "dmffb_set_fused_fft", "dmffb_fused_fft_cluster", "dmffb_admp_backward", "dmffb_admp_param_grads_host", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
     "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy", "dmffb_md_force_create",
     "dmffb_md_force_execute", "dmffb_md_force_last_result", "dmffb_md_force_dipoles", "dmffb_md_force_destroy",
+    "dmffb_pairwise_create", "dmffb_pairwise_set_params", "dmffb_pairwise_set_param_grads", "dmffb_pairwise_compute",
+    "dmffb_pairwise_param_grads",
 ]
+DMFFB_SR_TT_QQ, DMFFB_SR_SLATER_DISP, DMFFB_SR_SLATER, DMFFB_SR_TT_QQ_C6 = 0, 1, 2, 3
+SR_NPARAM = {0: 2, 1: 4, 2: 2, 3: 4}
 
 DMFFB_COUL_NONE = 0
 DMFFB_COUL_PME = 1
@@ -50,7 +54,7 @@ DMFFB_TERM_TORSION = 2
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
                   "gather_field", "self_frames", "vector", "neighbors", "matvec_coef", "pair_full_scaled",
-                  "pair_field_scaled", "param_grads", "bonded"]
+                  "pair_field_scaled", "param_grads", "bonded", "fft_conv_cluster"]
 
 
 class AdmpDesc(ctypes.Structure):
@@ -125,6 +129,27 @@ class MdContext(ctypes.Structure):
         ("padded_num_atoms", ctypes.c_int32),
         ("box_nm", ctypes.c_double * 9),
         ("stream", ctypes.c_void_p),
+    ]
+
+
+class PairwiseDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_atoms", ctypes.c_int32),
+        ("kind", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("rc", ctypes.c_double),
+        ("n_cov", ctypes.c_int64),
+        ("cov_rows", ctypes.POINTER(ctypes.c_int32)),
+        ("mscales", ctypes.c_double * 6),
+        ("sign", ctypes.c_double),
+    ]
+
+
+class PairwiseResult(ctypes.Structure):
+    _fields_ = [
+        ("energy", ctypes.c_double),
+        ("box_grad", ctypes.c_double * 9),
+        ("n_pairs", ctypes.c_int64),
     ]
 
 
@@ -239,7 +264,8 @@ class Request(ctypes.Structure):
 
 # C struct name of each ctypes mirror (layout checked against the header by the CPU tests)
 STRUCTS = {"dmffb_admp_desc": AdmpDesc, "dmffb_admp_result": AdmpResult, "dmffb_admp_cotangent": AdmpCotangent,
-           "dmffb_admp_second": AdmpSecond, "dmffb_md_context": MdContext, "dmffb_disp_desc": DispDesc,
+           "dmffb_admp_second": AdmpSecond, "dmffb_md_context": MdContext, "dmffb_pairwise_desc": PairwiseDesc,
+           "dmffb_pairwise_result": PairwiseResult, "dmffb_disp_desc": DispDesc,
            "dmffb_disp_result": DispResult, "dmffb_classical_desc": ClassicalDesc,
            "dmffb_classical_result": ClassicalResult, "dmffb_server_desc": ServerDesc, "dmffb_request": Request}
 
@@ -295,6 +321,8 @@ def load():
     lib.dmffb_classical_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, P(ClassicalResult)]
     lib.dmffb_classical_param_grads.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     lib.dmffb_set_graphs.argtypes = [vp, i32]
+    lib.dmffb_set_fused_fft.argtypes = [vp, i32]
+    lib.dmffb_fused_fft_cluster.argtypes = [vp]
     lib.dmffb_server_create.argtypes = [P(ServerDesc), P(vp)]
     lib.dmffb_server_submit.argtypes = [vp, P(Request)]
     lib.dmffb_server_wait.argtypes = [vp, dbl]
@@ -307,6 +335,11 @@ def load():
     lib.dmffb_md_force_last_result.argtypes = [vp, P(AdmpResult)]
     lib.dmffb_md_force_dipoles.argtypes = [vp, vp, vp]
     lib.dmffb_md_force_destroy.argtypes = [vp]
+    lib.dmffb_pairwise_create.argtypes = [P(PairwiseDesc), P(vp)]
+    lib.dmffb_pairwise_set_params.argtypes = [vp, vp]
+    lib.dmffb_pairwise_set_param_grads.argtypes = [vp, i32]
+    lib.dmffb_pairwise_compute.argtypes = [vp, vp, vp, vp, vp, i64, vp, P(PairwiseResult)]
+    lib.dmffb_pairwise_param_grads.argtypes = [vp, vp, vp]
     for name in EXPORTED:
         if name not in ("dmffb_destroy", "dmffb_last_error", "dmffb_server_destroy", "dmffb_server_clock",
                         "dmffb_request_footprint", "dmffb_md_force_destroy"):

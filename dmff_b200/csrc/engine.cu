@@ -23,6 +23,8 @@
 #include "disp.cuh"
 #include "classical.cuh"
 #include "nbcells.cuh"
+#include "admp_fftconv.cuh"
+#include "pairwise.cuh"
 
 using namespace dmffb;
 
@@ -145,9 +147,21 @@ struct dmffb_engine {
     double* d_tdprm[3] = {nullptr, nullptr, nullptr};
     bool want_pgrad = false, charges_set = false;
     bool cell_pass = false;  // dmffb_classical_set_cell_pass: pairs from the cell grid, no list
+    // dipole-solve convolution in one thread-block cluster (FP32, meshes up to 64 per axis)
+    bool fc_enabled = false;  // dmffb_set_fused_fft
+    int fc_cl = -1;          // CTAs per cluster for the current mesh (0: not available, -1: not decided)
+    float* d_fcG = nullptr;  // [K1*K2*Kh] influence function of the half spectrum
+    int64_t fcG_cap = 0;
     int32_t* d_covrows = nullptr;  // [n_covrows*3] covalent rows (i < j, nbond)
     int64_t n_covrows = 0;
     int32_t *d_cov_lo = nullptr, *d_cov_hi = nullptr;  // [n] covalent partner index range
+    float4* d_posc = nullptr;  // [n] cell-ordered positions of the cell pass
+    // ---- short-range pairwise terms (engines made by dmffb_pairwise_create, kind 3)
+    int sr_kind = 0;
+    double sr_sign = 1.0;
+    void* d_srp = nullptr;      // [4n] per-atom parameters in kernel precision, channel-major
+    double* d_srdp = nullptr;   // [4n] dE/dparameter
+    void* d_srgrad = nullptr;   // [3n] dE/dpos in kernel precision
     bool zero_guess = false;  // dipole solves start from U = 0 (dmffb_admp_set_zero_guess)
     bool u_zeroed = false;    // this call's U was zeroed by the host-buffer entry point
     // ---- ADMP parameter adjoints (dmffb_admp_set_param_grads)
@@ -279,7 +293,9 @@ inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 enum { KC_PREP = 0, KC_PAIR_FULL, KC_PAIR_FIELD, KC_PAIR_MATVEC, KC_SPREAD, KC_FFT, KC_CONV, KC_GATHER_FULL,
        KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_MVCOEF,
        // FP64 launches over the topologically scaled rows, parameter-adjoint pair kernels, bonded terms
-       KC_PAIR_FULL_SCALED, KC_PAIR_FIELD_SCALED, KC_PGRAD, KC_BONDED, KC_COUNT };
+       KC_PAIR_FULL_SCALED, KC_PAIR_FIELD_SCALED, KC_PGRAD, KC_BONDED,
+       KC_FFTCONV,  // the dipole solve's forward FFT + influence multiply + inverse FFT in one cluster
+       KC_COUNT };
 static_assert(KC_COUNT <= 32, "kernel-class statistics arrays hold 32 classes");
 
 inline void prof_begin(dmffb_engine* h, cudaStream_t s, int cls) {
@@ -516,6 +532,92 @@ int lmax_eff(const dmffb_engine* h) { return (h->lmax == 0 && h->lpol) ? 1 : h->
 // reciprocal pass: spread (Qg and/or U) -> FFT -> convolution -> inverse FFT -> gather
 // per-atom wrapped stencil origins and spline weights at these positions, for the cached dipole
 // spread and field gather of the dipole solve
+// Cluster size of the fused dipole-solve convolution for the current mesh: 16 CTAs (non-portable
+// size) or 8, when the kernel's shared memory fits and the device can place such a cluster; 0 when
+// the mesh is larger than 64 points on an axis or no cluster fits (the cuFFT path runs then).
+int fc_decide(dmffb_engine* h) {
+    if (h->fc_cl >= 0) return h->fc_cl;
+    h->fc_cl = 0;
+    if (h->prec != DMFFB_FP32 || !h->lpme) return 0;
+    for (int k = 0; k < 3; ++k) {
+        bool smooth = false;
+        fc_plan(h->K[k], &smooth);
+        if (h->K[k] < 2 || h->K[k] > kFcMaxK || !smooth) return 0;
+    }
+    for (int cl : {16, 8}) {
+        const size_t smem = fc_smem_bytes(h->K, cl);
+        if (smem > 227 * 1024) continue;
+        if (cudaFuncSetAttribute(k_fftconv_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            continue;
+        if (cl > 8 && cudaFuncSetAttribute(k_fftconv_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                          cudaSuccess)
+            continue;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cl);
+        cfg.blockDim = dim3(kFcThreads);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr;
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = cl;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, k_fftconv_cluster, &cfg) == cudaSuccess && nclusters > 0) {
+            h->fc_cl = cl;
+            break;
+        }
+        cudaGetLastError();  // clear a refused configuration
+    }
+    return h->fc_cl;
+}
+
+// influence-function table of the fused convolution for this box (once per dipole solve)
+int fc_prepare(dmffb_engine* h, cudaStream_t s, const Box& bx) {
+    const int Kh = h->K[2] / 2 + 1;
+    const int64_t m = (int64_t)h->K[0] * h->K[1] * Kh;
+    int st;
+    if (m > h->fcG_cap) {
+        if (h->d_fcG) cudaFree(h->d_fcG);
+        h->d_fcG = nullptr;
+        h->fcG_cap = m;
+        if ((st = dalloc(h, &h->d_fcG, m * sizeof(float)))) return st;
+    }
+    LAUNCH(h, s, KC_VEC, k_fc_gtable<<<nblk(m, 256), 256, 0, s>>>(h->K[0], h->K[1], h->K[2], Kh, bx, h->d_bmod,
+                                                                  h->kappa, fabs(det3(bx.h)), h->d_fcG));
+    CK(cudaGetLastError());
+    return DMFFB_OK;
+}
+
+int fc_launch(dmffb_engine* h, cudaStream_t s, float* in, float* out) {
+    FftConvArgs a;
+    for (int k = 0; k < 3; ++k) a.K[k] = h->K[k];
+    a.Kh = h->K[2] / 2 + 1;
+    a.cl = h->fc_cl;
+    a.grid_in = in;
+    a.grid_out = out;
+    a.G = h->d_fcG;
+    a.px = fc_plan(h->K[0]);
+    a.py = fc_plan(h->K[1]);
+    a.pz = fc_plan(h->K[2]);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(h->fc_cl);
+    cfg.blockDim = dim3(kFcThreads);
+    cfg.dynamicSmemBytes = fc_smem_bytes(h->K, h->fc_cl);
+    cfg.stream = s;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = h->fc_cl;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    LAUNCH(h, s, KC_FFTCONV, CK(cudaLaunchKernelEx(&cfg, k_fftconv_cluster, a)));
+    return DMFFB_OK;
+}
+
 template <typename T>
 int stencil_prep(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx) {
     const int n = h->n;
@@ -531,6 +633,7 @@ int stencil_prep(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& 
     }
     LAUNCH(h, s, KC_VEC, k_stencil_prep<T><<<nblk(n, 128), 128, 0, s>>>(n, pos, mesh_geom(bx, h->K), h->d_stc_org,
                                                                         (T*)h->d_stc_w));
+    if (sizeof(T) == 4 && h->fc_enabled && fc_decide(h) > 0 && (st = fc_prepare(h, s, bx))) return st;
     h->stencils_ready = true;
     return DMFFB_OK;
 }
@@ -677,6 +780,11 @@ int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, 
         if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
     LAUNCH(h, s, KC_SPREAD, k_spread_dip_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa, stencil_cache<T>(h)));
+    if (sizeof(T) == 4 && h->fc_enabled && h->fc_cl > 0) {
+        // forward FFT, influence multiply and inverse FFT in one cluster; it also clears grid2
+        int stc = fc_launch(h, s, (float*)h->d_grid2, (float*)h->d_grid);
+        if (stc) return stc;
+    } else {
     const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
     CKFFT(cufftSetStream(h->plan_f, s));
     CKFFT(cufftSetStream(h->plan_b, s));
@@ -704,6 +812,7 @@ int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, 
         FFTCALL(h, s, cufftExecC2R(h->plan_b, (cufftComplex*)h->d_cgrid, (cufftReal*)h->d_grid));
     else
         FFTCALL(h, s, cufftExecZ2D(h->plan_b, (cufftDoubleComplex*)h->d_cgrid, (cufftDoubleReal*)h->d_grid));
+    }
     FieldCombine cmb;
     const double k = h->kappa;
     cmb.U = h->d_p;
@@ -939,7 +1048,8 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     if (graphs) {
         std::vector<double> key = {(double)(uintptr_t)pos, (double)(uintptr_t)pairs, (double)npairs,
                                    (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T),
-                                   (double)(uintptr_t)h->d_mvcoef, (double)(uintptr_t)h->d_csr_off};
+                                   (double)(uintptr_t)h->d_mvcoef, (double)(uintptr_t)h->d_csr_off,
+                                   (double)(h->fc_enabled ? h->fc_cl : 0), (double)(uintptr_t)h->d_fcG};
         for (int k = 0; k < 9; ++k) key.push_back(bx.h[k]);
         if (!h->cg_exec || key != h->cg_key) {
             if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
@@ -1410,8 +1520,8 @@ bool half_cells(const dmffb_engine* h, const Box& bx, int nc[3]) {
     return true;
 }
 
-// FP32 positions and the counting sort of the atoms into the cells nc (the binning of the list
-// build): cell_start / cell_atoms.
+// Counting sort of the atoms into the cells nc (the binning of the list build): cell_start /
+// cell_atoms, and the cell-ordered float4 positions of the cell pass.
 int bin_cells(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int nc[3]) {
     const int n = h->n;
     int st;
@@ -1421,10 +1531,6 @@ int bin_cells(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx,
         if ((st = dalloc(h, &h->d_poff, (cap + 1) * sizeof(int64_t)))) return st;
         if ((st = dalloc(h, &h->d_atom_cell, cap * sizeof(int32_t)))) return st;
         if ((st = dalloc(h, &h->d_cell_atoms, cap * sizeof(int32_t)))) return st;
-    }
-    if (!h->d_posf) {
-        if ((st = dalloc(h, &h->d_posf, 4 * h->n_cap * sizeof(float)))) return st;
-        if ((st = dalloc(h, &h->d_pcount_f, h->n_cap * sizeof(int32_t)))) return st;
     }
     const int ncell = nc[0] * nc[1] * nc[2];
     if (ncell + 1 > h->ncell_cap) {
@@ -1441,7 +1547,6 @@ int bin_cells(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx,
         h->cub_bytes = need;
         if ((st = dalloc(h, &h->d_cub, need))) return st;
     }
-    LAUNCH(h, s, KC_NBLIST, k_pos_f32<<<nblk(n, 256), 256, 0, s>>>(n, pos, h->d_posf));
     CK(cudaMemsetAsync(h->d_cell_count, 0, (ncell + 1) * sizeof(int32_t), s));
     CK(cudaMemsetAsync(h->d_cell_cursor, 0, (ncell + 1) * sizeof(int32_t), s));
     LAUNCH(h, s, KC_NBLIST, k_cell_count<<<nblk(n, 256), 256, 0, s>>>(n, pos, bx, nc[0], nc[1], nc[2], h->d_atom_cell,
@@ -1450,6 +1555,8 @@ int bin_cells(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx,
     LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::ExclusiveSum(h->d_cub, tb, h->d_cell_count, h->d_cell_start, ncell + 1, s));
     LAUNCH(h, s, KC_NBLIST, k_cell_fill<<<nblk(n, 256), 256, 0, s>>>(n, h->d_atom_cell, h->d_cell_start,
                                                                     h->d_cell_cursor, h->d_cell_atoms));
+    if (!h->d_posc && (st = dalloc(h, &h->d_posc, (size_t)h->n_cap * sizeof(float4)))) return st;
+    LAUNCH(h, s, KC_NBLIST, k_pos_cells<<<nblk(n, 256), 256, 0, s>>>(n, pos, h->d_cell_atoms, h->d_posc));
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
@@ -1492,12 +1599,11 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
         NbCellArgs<T> c;
         c.n = n;
         c.pos = pos;
-        c.posf = h->d_posf;
+        c.posc = h->d_posc;
         c.boxd = bx;
         c.rc = h->rc;
         for (int k = 0; k < 3; ++k) c.nc[k] = ncf[k];
         c.cell_start = h->d_cell_start;
-        c.cell_atoms = h->d_cell_atoms;
         c.cov.cov_ptr = h->d_cov_ptr;
         c.cov.cov_j = h->d_cov_j;
         c.cov.cov_nb = h->d_cov_nb;
@@ -1696,6 +1802,7 @@ int upload_topology(dmffb_engine* h, const dmffb_admp_desc* d) {
 
 // PME mesh of h->K: grids grown to fit, B-spline moduli, cuFFT plans (cached per mesh shape)
 int setup_mesh(dmffb_engine* h) {
+    h->fc_cl = -1;  // the fused convolution's cluster size is decided again for this mesh
     const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
     const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
     const int64_t Kc = (int64_t)h->K[0] * h->K[1] * (h->K[2] / 2 + 1);
@@ -1868,7 +1975,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi};
+                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2728,6 +2835,139 @@ int dmffb_disp_param_grads(dmffb_engine* h, void* stream, double* dE_dc, double*
     return DMFFB_OK;
 }
 
+}  // extern "C"
+
+template <typename T>
+int pairwise_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const double* box, const int32_t* pairs,
+                          int64_t npairs, double* forces, dmffb_pairwise_result* res) {
+    if (!h->params_set) return fail(h, DMFFB_BAD_ARG, "dmffb_pairwise_set_params was not called");
+    if (!pos || !box || !res) return fail(h, DMFFB_BAD_ARG, "null pos/box/result");
+    Box bx;
+    make_box(box, bx);
+    memset(res, 0, sizeof(*res));
+    const int n = h->n;
+    int st;
+    if (!pairs) {
+        if (!h->have_pairs)
+            if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
+        pairs = h->d_pairs;
+        npairs = h->npairs;
+    }
+    res->n_pairs = npairs;
+    const bool pg = h->want_pgrad;
+    const int np = sr_nparam(h->sr_kind);
+    CK(cudaMemsetAsync(h->d_scal, 0, N_SCAL * sizeof(double), s));
+    CK(cudaMemsetAsync(h->d_srgrad, 0, (size_t)3 * n * sizeof(T), s));
+    if (pg) CK(cudaMemsetAsync(h->d_srdp, 0, (size_t)np * n * sizeof(double), s));
+    if (npairs > 0) {
+        SrArgs<T> a;
+        a.n = n;
+        a.npairs = npairs;
+        a.pairs = pairs;
+        a.pos = pos;
+        a.p = (const T*)h->d_srp;
+        for (int k = 0; k < 6; ++k) a.ms[k] = (T)h->ms[k];
+        a.sign = (T)h->sr_sign;
+        a.boxd = bx;
+        a.grad = (T*)h->d_srgrad;
+        a.dp = pg ? h->d_srdp : nullptr;
+        a.scal = h->d_scal;
+        const unsigned nbk = nblk(npairs, 128);
+        switch (h->sr_kind) {
+            case SR_TT_QQ: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_TT_QQ><<<nbk, 128, 0, s>>>(a)); break;
+            case SR_SLATER_DISP: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_SLATER_DISP><<<nbk, 128, 0, s>>>(a)); break;
+            case SR_SLATER: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_SLATER><<<nbk, 128, 0, s>>>(a)); break;
+            default: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_TT_QQ_C6><<<nbk, 128, 0, s>>>(a)); break;
+        }
+        CK(cudaGetLastError());
+    }
+    if (forces) LAUNCH(h, s, KC_VEC, k_sr_finalize<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_srgrad, forces));
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, N_SCAL * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    prof_collect(h);
+    res->energy = h->h_scal[0];
+    for (int k = 0; k < 9; ++k) res->box_grad[k] = h->h_scal[1 + k];
+    h->have_pgrad = pg;
+    if (!std::isfinite(res->energy)) return fail(h, DMFFB_NONFINITE, "non-finite energy");
+    return DMFFB_OK;
+}
+
+extern "C" {
+
+int dmffb_pairwise_create(const dmffb_pairwise_desc* d, dmffb_engine** out) {
+    if (!d || !out) return DMFFB_BAD_ARG;
+    *out = nullptr;
+    if (d->n_atoms <= 0 || d->kind < DMFFB_SR_TT_QQ || d->kind > DMFFB_SR_TT_QQ_C6 || !(d->rc > 0)) return DMFFB_BAD_ARG;
+    dmffb_admp_desc a;
+    memset(&a, 0, sizeof(a));
+    a.n_atoms = d->n_atoms;
+    a.precision = d->precision;
+    a.rc = d->rc;
+    a.n_cov = d->n_cov;
+    a.cov_rows = d->cov_rows;
+    for (int k = 0; k < 6; ++k) a.mscales[k] = a.pscales[k] = a.dscales[k] = d->mscales[k];
+    a.cg_tol = 1e-6;
+    a.max_iter = 1;
+    int st = dmffb_admp_create(&a, out);
+    dmffb_engine* h = *out;
+    if (st) return st;
+    h->kind = 3;
+    h->sr_kind = d->kind;
+    h->sr_sign = d->sign == 0.0 ? 1.0 : d->sign;
+    const int n = h->n;
+    const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
+    if ((st = dalloc(h, &h->d_srp, 4 * (size_t)n * ts)) || (st = dalloc(h, &h->d_srdp, 4 * (size_t)n * sizeof(double))) ||
+        (st = dalloc(h, &h->d_srgrad, 3 * (size_t)n * ts)))
+        return st;
+    return DMFFB_OK;
+}
+
+int dmffb_pairwise_set_params(dmffb_engine* h, const double* params) {
+    if (!h || h->kind != 3 || !params) return fail(h, DMFFB_BAD_ARG, "pairwise engine and parameters required");
+    const int np = sr_nparam(h->sr_kind);
+    const int64_t m = (int64_t)np * h->n;
+    cudaStream_t s = h->s1;
+    // staged in the gradient scratch, then converted to kernel precision
+    CK(cudaMemcpyAsync(h->d_srdp, params, m * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (h->prec == DMFFB_FP32) k_to_t<float><<<nblk(m, 256), 256, 0, s>>>((int)m, h->d_srdp, (float*)h->d_srp);
+    else k_to_t<double><<<nblk(m, 256), 256, 0, s>>>((int)m, h->d_srdp, (double*)h->d_srp);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    h->params_set = true;
+    h->have_pgrad = false;
+    return DMFFB_OK;
+}
+
+int dmffb_pairwise_set_param_grads(dmffb_engine* h, int32_t enabled) {
+    if (!h || h->kind != 3) return fail(h, DMFFB_BAD_ARG, "pairwise engine required");
+    h->want_pgrad = enabled != 0;
+    return DMFFB_OK;
+}
+
+int dmffb_pairwise_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                           int64_t npairs, double* forces_out, dmffb_pairwise_result* result) {
+    if (!h || h->kind != 3) return fail(h, DMFFB_BAD_ARG, "pairwise engine required");
+    if (pairs && npairs < 0) return fail(h, DMFFB_BAD_ARG, "negative npairs");
+    cudaStream_t caller = (cudaStream_t)stream;
+    CK(cudaEventRecord(h->e_in, caller));
+    CK(cudaStreamWaitEvent(h->s1, h->e_in, 0));
+    int st = h->prec == DMFFB_FP32 ? pairwise_compute_impl<float>(h, h->s1, pos, box, pairs, npairs, forces_out, result)
+                                   : pairwise_compute_impl<double>(h, h->s1, pos, box, pairs, npairs, forces_out, result);
+    cudaEventRecord(h->e_out, h->s1);
+    cudaStreamWaitEvent(caller, h->e_out, 0);
+    return st;
+}
+
+int dmffb_pairwise_param_grads(dmffb_engine* h, void* stream, double* dE_dparams) {
+    if (!h || h->kind != 3 || !dE_dparams) return fail(h, DMFFB_BAD_ARG, "pairwise engine and output required");
+    if (!h->have_pgrad) return fail(h, DMFFB_BAD_ARG, "enable dmffb_pairwise_set_param_grads before compute");
+    const int np = sr_nparam(h->sr_kind);
+    CK(cudaMemcpyAsync(dE_dparams, h->d_srdp, (size_t)np * h->n * sizeof(double), cudaMemcpyDeviceToDevice,
+                       (cudaStream_t)stream));
+    return DMFFB_OK;
+}
+
 int dmffb_classical_create(const dmffb_classical_desc* d, dmffb_engine** out) {
     if (!d || !out) return DMFFB_BAD_ARG;
     *out = nullptr;
@@ -2935,6 +3175,17 @@ int dmffb_set_timing(dmffb_engine* h, int32_t enabled) {
     if (!h) return DMFFB_BAD_ARG;
     h->timing = enabled != 0;
     return DMFFB_OK;
+}
+
+int dmffb_set_fused_fft(dmffb_engine* h, int32_t enabled) {
+    if (!h) return DMFFB_BAD_ARG;
+    h->fc_enabled = enabled != 0;
+    return DMFFB_OK;
+}
+
+int dmffb_fused_fft_cluster(const dmffb_engine* h) {
+    if (!h) return -1;
+    return h->fc_enabled && h->fc_cl > 0 ? h->fc_cl : 0;
 }
 
 int dmffb_set_graphs(dmffb_engine* h, int32_t enabled) {

@@ -6,7 +6,9 @@
 // 61 M rows, 0.74 GB out and back, plus j-side force atomics.  This pass evaluates the same pair
 // set straight from the cell binning of the step's positions:
 //   * one warp per atom i walks the 5^3 stencil of half-width cells as one concatenated
-//     candidate list (the layout of k_pairs_warp3), 32 candidates per batch;
+//     candidate list (the layout of k_pairs_warp3), 32 candidates per batch, reading a cell-ordered
+//     float4 copy of the positions (contiguous runs per cell, the atom index in the w slot);
+//     atoms are taken in cell order, so the warps of a block share their candidates through L1;
 //   * FP32 prefilter on float positions, the exact FP64 test of the list build (within_rc on the
 //     lower/higher orientation) inside a 2e-3 A band around rc, so the kept set is the list's
 //     set bit for bit;
@@ -30,12 +32,11 @@ template <typename T>
 struct NbCellArgs {
     int n;
     const double* pos;        // [3n] FP64
-    const float* posf;        // [4n] FP32 x, y, z (prefilter)
+    const float4* posc;       // [n] FP32 x, y, z and the atom index (as int bits), in cell order
     Box boxd;
     double rc;
     int nc[3];                // half-width cells per axis (>= 5)
     const int32_t* cell_start;
-    const int32_t* cell_atoms;
     NbArgs cov;               // covalent-map lookup (cov_ptr / cov_j / cov_nb over i < j)
     const int32_t* cov_lo;    // [n] smallest / largest covalent partner index (lo > hi: none)
     const int32_t* cov_hi;
@@ -53,10 +54,9 @@ struct NbCellArgs {
 
 // One kept pair (i, j) seen from atom i: energy halves, box-gradient halves and the force on i.
 template <typename T>
-__device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int j, const double* pi, float pix,
-                                             float piy, float piz, const float hf[9], const float hif[9],
+__device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int j, const double* pi,
                                              const BoxT<double>& bxd, bool lj, int ti, T qi, T& g0, T& g1, T& g2,
-                                             float (&acc)[11]) {
+                                             T (&acc)[11]) {
     // the pair geometry of k_nb_pair: FP64 minimum image, then kernel precision
     T e[3], r;
     T nn[3];
@@ -78,12 +78,12 @@ __device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int 
     g0 -= s * e[0];
     g1 -= s * e[1];
     g2 -= s * e[2];
-    acc[0] += (float)(T(0.5) * ec);
-    acc[1] += (float)(T(0.5) * el);
+    acc[0] += T(0.5) * ec;
+    acc[1] += T(0.5) * el;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[2 + 3 * k + c] -= (float)(T(0.5) * nn[k] * s * e[c]);
+        for (int c = 0; c < 3; ++c) acc[2 + 3 * k + c] -= T(0.5) * nn[k] * s * e[c];
 }
 
 template <typename T>
@@ -94,14 +94,18 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
     __shared__ int s_q[kNbWarps][64];  // kept candidates waiting for a full 32-lane batch
     const int wl = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const bool live = i < a.n;  // warps past the end still take part in the block reduction
+    // warps take the atoms in cell order: the warps of a block share one stencil, so their
+    // candidate reads (contiguous runs of the cell-ordered copy) hit L1 after the first
+    const int ks = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const bool live = ks < a.n;  // warps past the end still take part in the block reduction
     double red[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) red[k] = 0.0;
     if (live) {
+        const float4 p4 = a.posc[ks];
+        const int i = __float_as_int(p4.w);
         const double* pi = a.pos + 3 * i;
-        const float pix = a.posf[4 * i], piy = a.posf[4 * i + 1], piz = a.posf[4 * i + 2];
+        const float pix = p4.x, piy = p4.y, piz = p4.z;
         float hf[9], hif[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) { hf[k] = (float)a.boxd.h[k]; hif[k] = (float)a.boxd.hinv[k]; }
@@ -143,9 +147,9 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
         const int ti = lj ? a.type[i] : 0;
         const T qi = a.qT[i];
         T g0 = T(0), g1 = T(0), g2 = T(0);
-        float acc[11];
+        T acc[11];  // per-lane sums of about 40 pairs, in kernel precision
 #pragma unroll
-        for (int k = 0; k < 11; ++k) acc[k] = 0.f;
+        for (int k = 0; k < 11; ++k) acc[k] = T(0);
         const unsigned lt = (1u << lane) - 1u;
         int qn = 0;  // queued kept candidates (warp-uniform)
         int qc = 0;
@@ -155,9 +159,10 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
             int j = -1;
             if (t < total) {
                 while (t >= s_off[wl][qc + 1]) ++qc;
-                j = a.cell_atoms[s_beg[wl][qc] + (t - s_off[wl][qc])];
+                const float4 pj = a.posc[s_beg[wl][qc] + (t - s_off[wl][qc])];
+                j = __float_as_int(pj.w);
                 if (j != i) {
-                    const float d0 = a.posf[4 * j] - pix, d1 = a.posf[4 * j + 1] - piy, d2 = a.posf[4 * j + 2] - piz;
+                    const float d0 = pj.x - pix, d1 = pj.y - piy, d2 = pj.z - piz;
                     bool amb = false;
                     float sf[3];
 #pragma unroll
@@ -188,7 +193,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
             qn += __popc(mk);
             __syncwarp();
             if (qn >= 32) {
-                nb_cell_pair<T>(a, i, s_q[wl][lane], pi, pix, piy, piz, hf, hif, bxd, lj, ti, qi, g0, g1, g2, acc);
+                nb_cell_pair<T>(a, i, s_q[wl][lane], pi, bxd, lj, ti, qi, g0, g1, g2, acc);
                 __syncwarp();
                 if (lane < qn - 32) s_q[wl][lane] = s_q[wl][32 + lane];
                 qn -= 32;
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
             }
         }
         if (lane < qn)
-            nb_cell_pair<T>(a, i, s_q[wl][lane], pi, pix, piy, piz, hf, hif, bxd, lj, ti, qi, g0, g1, g2, acc);
+            nb_cell_pair<T>(a, i, s_q[wl][lane], pi, bxd, lj, ti, qi, g0, g1, g2, acc);
 #pragma unroll
         for (int k = 0; k < 11; ++k) red[k] = (double)acc[k];
         g0 = warp_sum(g0);

@@ -642,6 +642,14 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
     }
 }
 
+// cell-ordered float4 copy of the positions (x, y, z, atom index as int bits)
+static __global__ void k_pos_cells(int n, const double* pos, const int32_t* cell_atoms, float4* posc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int a = cell_atoms[k];
+    posc[k] = make_float4((float)pos[3 * a], (float)pos[3 * a + 1], (float)pos[3 * a + 2], __int_as_float(a));
+}
+
 static __global__ void k_pos_f32(int n, const double* pos, float* posf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;

@@ -318,6 +318,15 @@ class AdmpEngine:
                                                 ctypes.byref(need)))
         return buf[: need.value]
 
+    def set_fused_fft(self, on=True):
+        """The dipole solve's reciprocal convolution in one thread-block cluster (FP32, meshes up
+        to 64 per axis) or through cuFFT (dmffb_set_fused_fft)."""
+        self._check(self.lib.dmffb_set_fused_fft(self.h, int(bool(on))))
+
+    def fused_fft_cluster(self):
+        """CTAs per cluster of the last solve's convolution (0: cuFFT)."""
+        return int(self.lib.dmffb_fused_fft_cluster(self.h))
+
     def set_timing(self, on=True):
         self.lib.dmffb_set_timing(self.h, int(on))
 
@@ -551,4 +560,77 @@ class ClassicalEngine:
             _dev(out["eps_tt"]) if T else None, _dev(out["bond"]) if self.n_terms["bond"] else None,
             _dev(out["angle"]) if self.n_terms["angle"] else None,
             _dev(out["torsion"]) if self.n_terms["torsion"] else None))
+        return out
+
+
+class PairwiseEngine:
+    """Short-range pairwise term with per-atom parameters on one GPU (dmffb_pairwise_*): the
+    built-in kernels of dmff/admp/pairwise.py (``kind`` one of L.DMFFB_SR_*), Angstrom units,
+    parameters [nparam, n] in the order of the C header, ``sign`` -1 for the SlaterSr* terms."""
+
+    def __init__(self, n_atoms, kind, rc, cov_rows=None, mscales=(0, 0, 0, 1, 1, 1), sign=1.0, precision="fp32",
+                 device=None):
+        self.lib = L.load()
+        self.n = int(n_atoms)
+        self.kind = int(kind)
+        self.nparam = L.SR_NPARAM[self.kind]
+        self.mscales = tuple(float(x) for x in mscales)
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        d = L.PairwiseDesc()
+        d.n_atoms, d.kind, d.precision, d.rc = self.n, self.kind, _PREC[precision], float(rc)
+        cov = _i32(cov_rows if cov_rows is not None else np.zeros((0, 3)), (-1,))
+        self._keep = cov
+        d.n_cov = cov.size // 3
+        d.cov_rows = _ptr(cov)
+        for k in range(6):
+            d.mscales[k] = self.mscales[k]
+        d.sign = float(sign)
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            st = self.lib.dmffb_pairwise_create(ctypes.byref(d), ctypes.byref(h))
+        self.h = h
+        if st != L.DMFFB_OK:
+            msg = self.lib.dmffb_last_error(h).decode() if h.value else "invalid description"
+            if h.value:
+                self.lib.dmffb_destroy(h)
+            self.h = None
+            raise L.EngineError(st, msg)
+        self.forces = torch.zeros((self.n, 3), dtype=torch.float64, device=self.device)
+        self._pgrad = False
+
+    __del__ = AdmpEngine.__del__
+    _check = AdmpEngine._check
+    _box = staticmethod(AdmpEngine._box)
+    rebuild_internal_pairs = AdmpEngine.rebuild_internal_pairs
+    internal_pairs = AdmpEngine.internal_pairs
+    set_profiling = AdmpEngine.set_profiling
+    kernel_stats = AdmpEngine.kernel_stats
+
+    def set_params(self, params):
+        """params: [nparam, n] (array or tensor), Angstrom units."""
+        p = params.detach().cpu().numpy() if torch.is_tensor(params) else np.asarray(params)
+        p = np.ascontiguousarray(np.asarray(p, dtype=np.float64).reshape(self.nparam, self.n))
+        with torch.cuda.device(self.device):
+            self._check(self.lib.dmffb_pairwise_set_params(self.h, p.ctypes.data_as(ctypes.c_void_p)))
+
+    def set_param_grads(self, on=True):
+        self._check(self.lib.dmffb_pairwise_set_param_grads(self.h, int(bool(on))))
+        self._pgrad = bool(on)
+
+    def compute(self, pos, box, pairs=None):
+        """Returns (result, forces); forces = -dE/dpos, device [n, 3] FP64."""
+        assert pos.is_cuda and pos.dtype == torch.float64 and pos.is_contiguous()
+        b = self._box(box)
+        res = L.PairwiseResult()
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_pairwise_compute(
+            self.h, ctypes.c_void_p(s.cuda_stream), _dev(pos), b.ctypes.data_as(ctypes.c_void_p),
+            *_pairs_arg(pairs, self.device), _dev(self.forces), ctypes.byref(res)))
+        return res, self.forces
+
+    def param_grads(self):
+        """dE/dparameter [nparam, n] of the last compute."""
+        out = torch.empty((self.nparam, self.n), dtype=torch.float64, device=self.device)
+        s = torch.cuda.current_stream(self.device)
+        self._check(self.lib.dmffb_pairwise_param_grads(self.h, ctypes.c_void_p(s.cuda_stream), _dev(out)))
         return out

@@ -208,7 +208,8 @@ int dmffb_set_timing(dmffb_engine* h, int32_t enabled);
  * 2 pair FIELD, 3 pair MATVEC, 4 spread, 5 FFT (cuFFT), 6 convolution, 7 gather FULL,
  * 8 gather FIELD, 9 self+frame forces, 10 vector/CG ops, 11 neighbour build, 12 CG matvec
  * pair-tensor set-up, 13 pair FULL over the topologically scaled rows (FP64), 14 pair FIELD over
- * the scaled rows (FP64), 15 parameter-adjoint pair kernels, 16 bonded terms.  Classes 1 and 2
+ * the scaled rows (FP64), 15 parameter-adjoint pair kernels, 16 bonded terms, 17 the clustered
+ * convolution of the dipole solve (dmffb_set_fused_fft).  Classes 1 and 2
  * hold only the launches over the unscaled rows (kernel precision). */
 int dmffb_set_profiling(dmffb_engine* h, int32_t enabled);
 int dmffb_get_kernel_stats(const dmffb_engine* h, double* ms_out, int64_t* launches_out, int32_t n);
@@ -323,6 +324,52 @@ int dmffb_classical_set_cell_pass(dmffb_engine* h, int32_t enabled);
  * [n_terms*2] = (dE/dk, dE/d(r0 | theta0 | psi)). */
 int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, double* dE_dsig, double* dE_deps,
                                 double* dE_dbond, double* dE_dangle, double* dE_dtorsion);
+
+/* The dipole-solve iterations' reciprocal convolution (forward FFT, influence-function multiply,
+ * inverse FFT) in one thread-block cluster holding the half spectrum in distributed shared memory,
+ * on/off (on by default; FP32 engines with meshes of at most 64 points per axis, else cuFFT).
+ * dmffb_fused_fft_cluster returns the cluster size the last solve used (0: the cuFFT path). */
+int dmffb_set_fused_fft(dmffb_engine* h, int32_t enabled);
+int dmffb_fused_fft_cluster(const dmffb_engine* h);
+/* ---------------------------------------------------------------------------------------
+ * Short-range pairwise terms with per-atom parameters: the built-in kernels of
+ * dmff/admp/pairwise.py evaluated in CUDA (what generate_pairwise_interaction, pairwise.py:47-95,
+ * does for them in the reference), for the short-range generators of dmff/generators/admp.py
+ * (QqTtDampingForce :400-526, SlaterDampingForce :529-669, SlaterExForce and the SlaterSrEs /
+ * SlaterSrPol / SlaterSrDisp / SlaterDhf terms :672-863).  Per-atom parameters, host
+ * [nparam * n] channel-major, in Angstrom units as the generators pass them:
+ *   DMFFB_SR_TT_QQ       (b, q):           -DIELECTRIC e^-br (1 + br) q_i q_j / r, b = sqrt(b_i b_j)
+ *   DMFFB_SR_SLATER_DISP (b, c6, c8, c10): Slater-ISA damped C6/C8/C10 (pairwise.py:131-156)
+ *   DMFFB_SR_SLATER      (a, b):           a_i a_j ((br)^2 / 3 + br + 1) e^-br (pairwise.py:159-171)
+ *   DMFFB_SR_TT_QQ_C6    (a, b, q, c):     TT_damping_qq_c6_kernel (pairwise.py:100-118)
+ * each times mscales[nbond - 1] and the description's sign. */
+enum { DMFFB_SR_TT_QQ = 0, DMFFB_SR_SLATER_DISP = 1, DMFFB_SR_SLATER = 2, DMFFB_SR_TT_QQ_C6 = 3 };
+
+typedef struct {
+    int32_t n_atoms;
+    int32_t kind;             /* DMFFB_SR_* */
+    int32_t precision;        /* DMFFB_FP32 | DMFFB_FP64 */
+    double rc;                /* cutoff of the internal neighbour build, Angstrom */
+    int64_t n_cov;
+    const int32_t* cov_rows;  /* host [n_cov*3] (i, j, nbond), i < j */
+    double mscales[6];        /* nbond-1 indexed, [5] = 1.0 */
+    double sign;              /* overall factor: 1, or -1 for the SlaterSr* / SlaterDhf terms */
+} dmffb_pairwise_desc;
+
+typedef struct {
+    double energy;            /* kJ/mol */
+    double box_grad[9];
+    int64_t n_pairs;
+} dmffb_pairwise_result;
+
+int dmffb_pairwise_create(const dmffb_pairwise_desc* desc, dmffb_engine** out);
+int dmffb_pairwise_set_params(dmffb_engine* h, const double* params);
+int dmffb_pairwise_set_param_grads(dmffb_engine* h, int32_t enabled);
+/* forces_out = -dE/dpos (device [n*3], may be NULL); pairs as in dmffb_admp_compute. */
+int dmffb_pairwise_compute(dmffb_engine* h, void* stream, const double* pos, const double* box, const int32_t* pairs,
+                           int64_t npairs, double* forces_out, dmffb_pairwise_result* result);
+/* dE/dparameter of the last compute (device [nparam*n], channel-major). */
+int dmffb_pairwise_param_grads(dmffb_engine* h, void* stream, double* dE_dparams);
 
 /* CUDA-graph capture of the dipole-solve loop on/off for this engine (on by default). */
 int dmffb_set_graphs(dmffb_engine* h, int32_t enabled);

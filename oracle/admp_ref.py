@@ -931,6 +931,41 @@ def TT_damping_qq_c6_kernel(dr, m, ai, aj, bi, bj, qi, qj, ci, cj):
     return f * m
 
 
+def TT_damping_qq_kernel(dr, m, bi, bj, qi, qj):
+    """pairwise.py:121-128."""
+    b = torch.sqrt(bi * bj)
+    q = qi * qj
+    br = b * dr
+    exp_br = torch.exp(-br)
+    return -DIELECTRIC * exp_br * (1 + br) * q / dr * m
+
+
+def slater_disp_damping_kernel(dr, m, bi, bj, c6i, c6j, c8i, c8j, c10i, c10j):
+    """pairwise.py:131-156."""
+    b = torch.sqrt(bi * bj)
+    c6 = c6i * c6j
+    c8 = c8i * c8j
+    c10 = c10i * c10j
+    br = b * dr
+    br2 = br * br
+    x = br - (2 * br2 + 3 * br) / (br2 + 3 * br + 3)
+    s6 = 1 + x + x ** 2 / 2 + x ** 3 / 6 + x ** 4 / 24 + x ** 5 / 120 + x ** 6 / 720
+    s8 = s6 + x ** 7 / 5040 + x ** 8 / 40320
+    s10 = s8 + x ** 9 / 362880 + x ** 10 / 3628800
+    exp_x = torch.exp(-x)
+    return (exp_x * s6 * c6 / dr ** 6 + exp_x * s8 * c8 / dr ** 8 + exp_x * s10 * c10 / dr ** 10) * m
+
+
+def slater_sr_kernel(dr, m, ai, aj, bi, bj):
+    """pairwise.py:159-171."""
+    b = torch.sqrt(bi * bj)
+    a = ai * aj
+    br = b * dr
+    br2 = br * br
+    P = 1 / 3 * br2 + br + 1
+    return a * P * torch.exp(-br) * m
+
+
 def pairwise_energy(kernel, positions, box, pairs, mScales, *atomic_params):
     """pairwise.py:47-95 (nbond from the pair rows' third column)."""
     pairs = torch.as_tensor(np.asarray(pairs)).long()
