@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--serving-rates", default="50,100,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     p.add_argument("--serving-slots", type=int, default=12)
     p.add_argument("--serving-budget-gb", type=float, default=2.0)
+    p.add_argument("--fused-fft", action="store_true",
+                   help="dipole-solve convolution through the engine's FFT kernels instead of cuFFT")
     return p.parse_args()
 
 
@@ -67,26 +69,59 @@ def workload_config(name, s, world=1):
 
 # ---------------------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock, power and clock-event reasons sampled while the timed region runs: NVML every
+    5 ms (read-only queries; the device matched by PCI bus id), else nvidia-smi every 200 ms."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
-        self.rows = []
+        self.rows = []  # (sm_mhz, max_mhz, [reason names])
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                bus = torch.cuda.get_device_properties(gpu_index).pci_bus_id
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self._nvml = (pynvml, h)
+            self.source = "NVML, 5 ms"
+        except Exception:
+            self.source = "nvidia-smi, 200 ms"
+
+    def _sample_nvml(self):
+        nv, h = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        masks = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        self.rows.append((float(sm), float(mx), [n for n, m in zip(self.NAMES, masks) if bits & m]))
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        for line in out.stdout.strip().splitlines():
+            r = [x.strip() for x in line.split(",")]
+            if len(r) >= 9 and r[1].replace(".", "").isdigit():
+                self.rows.append((float(r[1]), float(r[2]),
+                                  [n for k, n in enumerate(self.NAMES) if r[5 + k] == "Active"]))
 
     def _run(self):
+        period = 0.005 if self._nvml else 0.2
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.rows.append([x.strip() for x in line.split(",")])
+                self._sample_nvml() if self._nvml else self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(period)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -98,12 +133,11 @@ class ClockSampler:
         self._t.join(timeout=10)
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        sm = [r[0] for r in self.rows]
+        mx = [r[1] for r in self.rows]
+        reasons = sorted({n for r in self.rows for n in r[2]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(sm)}
+                "reasons": reasons, "samples": len(sm), "source": self.source}
 
 
 # ---------------------------------------------------------------------------------- roofline
@@ -588,6 +622,7 @@ def main():
                      s["axis_indices"], s["cov_rows"], s["mscales"], s["pscales"], s["dscales"], precision="fp32",
                      solver="cg", cg_tol=1e-6, max_iter=1000, device=dev)
     eng.set_params(s["Q_local"], s.get("pol"), s.get("thole"))
+    eng.set_fused_fft(args.fused_fft)
     if s["lpol"]:
         eng.set_zero_guess(True)  # every step solves from U = 0 (the reference's U_init = None)
     pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
@@ -688,6 +723,8 @@ def main():
                "library_launches": {"cufft_execs": int(launches1["fft_execs"] - launches0["fft_execs"])},
                "result": {"energy_kJmol": res.energy, "cg_iters": n_iter, "converged": int(res.converged),
                           "n_pairs": n_pairs, "n_pairs_scaled": n_scaled}}
+        out["config"]["dipole_convolution"] = ("engine FFT kernels (k_fc_*)" if eng.fused_fft_active()
+                                               else "cuFFT R2C + k_conv + cuFFT C2R")
         if world == 1 and not args.no_cpu_baseline:
             cs, run, cores = cpu_reference_runner()
             run()  # warm-up

@@ -1,23 +1,18 @@
-// Reciprocal convolution of the dipole-solve iterations in one thread-block cluster:
-// real mesh -> forward 3-D FFT -> multiply by the influence function -> inverse 3-D FFT -> real
-// mesh, for meshes of up to 64 points per axis (FP32).
+// Reciprocal convolution of the dipole-solve iterations in three kernels of the engine's own
+// FFT: real mesh -> forward 3-D FFT -> multiply by the influence function -> inverse 3-D FFT ->
+// real mesh, for 7-smooth meshes of up to 64 points per axis (FP32).
 //
 // Each CG iteration of the induced-dipole solve convolves the spread dipole mesh with the
 // Coulomb influence function G(k) = C(k^2) / |theta(k)|^2 (recip.py:440-466; the reference runs a
 // full complex fftn of the mesh inside jax.grad, recip.py:450).  With cuFFT that is an R2C
-// transform (three kernels), a convolution kernel and a C2R transform (three kernels) on a mesh
-// that fits in L2: seven dependent launches of a few microseconds each.  Here one cluster of CL
-// CTAs holds the whole half spectrum in distributed shared memory:
-//   phase A (each CTA, its own x-planes x = c, c + CL, ...): load the plane's real rows, complex
-//           FFT along z of the zero-imaginary rows (keeping kz < K3/2 + 1), FFT along y; the spread
-//           mesh plane is cleared for the next spread;
-//   cluster barrier;
-//   phase B (each CTA, columns (ky, kz) = c, c + CL, ... in chunks): read the column's K1 values
-//           from the CTAs that own them (DSMEM), FFT along x, multiply by G, inverse FFT along x,
-//           write the column back (DSMEM);
-//   cluster barrier;
-//   phase C (each CTA, its planes): inverse FFT along y, Hermitian completion of every row and
-//           inverse complex FFT along z, real part out to the global mesh.
+// transform, a separate convolution kernel and a C2R transform on a mesh that fits in L2, each
+// latency-bound.  Here:
+//   k_fc_fwd_planes (one CTA per x-plane): two real rows packed per complex row, FFT along z,
+//           half spectra separated, FFT along y, half spectrum out; the spread plane is cleared;
+//   k_fc_columns (kFcCols spectrum columns (ky, kz) per CTA): FFT along x, times G, inverse FFT
+//           along x, in place;
+//   k_fc_inv_planes (one CTA per x-plane): inverse FFT along y, Hermitian completion of row pairs
+//           packed as A + i B, inverse FFT along z, the two real rows out.
 // Transforms are unnormalised in both directions (the cuFFT convention the gather expects).
 //
 // Line FFTs: Stockham autosort over the factors of the line length (radices 4, 2, 3, 5, 7; meshes
@@ -26,7 +21,7 @@
 // shared memory, conjugated for the inverse), a hard-coded R-point DFT, outputs to
 // y[(j - k) R + k + u Ns].
 #pragma once
-#include <cooperative_groups.h>
+#include <cmath>
 
 #include "common.cuh"
 
@@ -34,8 +29,10 @@ namespace dmffb {
 
 constexpr int kFcMaxK = 64;      // largest mesh extent per axis
 constexpr int kFcMaxFactors = 8;
-constexpr int kFcThreads = 512;
-constexpr int kFcChunk = 32;      // phase-B columns per round
+constexpr int kFcPlaneThreads = 512;
+constexpr int kFcColThreads = 256;
+constexpr int kFcCols = 8;        // spectrum columns per CTA of the column pass
+constexpr int kFcTw = 2 * kFcMaxK;  // stage twiddles of one line length (sum over stages of Ns R < 2 n)
 
 struct FcPlan {
     int n;                         // line length
@@ -46,11 +43,12 @@ struct FcPlan {
 struct FftConvArgs {
     int K[3];
     int Kh;                        // K[2] / 2 + 1
-    int cl;                        // CTAs in the cluster
-    float* grid_in;                // [K1*K2*K3] spread mesh (cleared by the kernel)
+    float* grid_in;                // [K1*K2*K3] spread mesh (cleared by the forward pass)
     float* grid_out;               // [K1*K2*K3] convolved mesh
+    float2* spec;                  // [K1][K2][Kh] half spectrum between the passes
     const float* G;                // [K1*K2*Kh] influence function over the half spectrum
     FcPlan px, py, pz;
+    float2 tw[3][kFcTw];           // stage twiddles of the x, y and z line lengths
 };
 
 // radices 4, 2, 3, 5, 7 in that order; ok = false when another prime factor remains (such meshes
@@ -70,31 +68,30 @@ __host__ inline FcPlan fc_plan(int n, bool* ok = nullptr) {
     return p;
 }
 
-// twiddles of every stage of a line length: for stage s (span Ns, radix R) the R x Ns table
-// W_{Ns R}^{t k} at off_s + k R + t; total size sum_s Ns R <= 2 n
-__host__ __device__ inline int fc_tw_size(const FcPlan& p) {
-    int ns = 1, tot = 0;
-    for (int s = 0; s < p.nf; ++s) {
-        tot += ns * p.f[s];
-        ns *= p.f[s];
-    }
-    return tot;
-}
-
-__device__ inline void fc_twiddles(float2* tw, const FcPlan& p, int tid, int nth) {
+// stage twiddles of a line length: W_{Ns R}^{t k} of stage s (span Ns, radix R) at off_s + k R + t,
+// off_s the sum of Ns R over the earlier stages (< 2 n in all); FP64 on the host rounded to FP32
+__host__ inline void fc_host_twiddles(const FcPlan& p, float2* tw) {
     int ns = 1, off = 0;
     for (int s = 0; s < p.nf; ++s) {
         const int R = p.f[s];
-        for (int e = tid; e < ns * R; e += nth) {
+        for (int e = 0; e < ns * R; ++e) {
             const int k = e / R, t = e % R;
-            double sn, cs;
-            sincospi(-2.0 * (double)(t * k) / (double)(ns * R), &sn, &cs);
-            tw[off + e] = make_float2((float)cs, (float)sn);
+            const double ang = -2.0 * 3.14159265358979323846 * (double)(t * k) / (double)(ns * R);
+            tw[off + e] = make_float2((float)std::cos(ang), (float)std::sin(ang));
         }
         off += ns * R;
         ns *= R;
     }
 }
+
+// stage twiddles of one line length from the launch arguments into shared memory
+__device__ inline void fc_load_twiddles(float2* dst, const float2* src, int tid, int nth) {
+    for (int e = tid; e < kFcTw; e += nth) dst[e] = src[e];
+}
+
+// a / d for 0 <= a < 2^20 and 1 <= d <= 2^12 through the FP32 reciprocal rcp = 1 / d: (a + 1/2) / d
+// lies at least 1 / (2 d) away from an integer, far above the rounding of the two FP32 operations
+__device__ __forceinline__ int fc_div(int a, float rcp) { return __float2int_rd(((float)a + 0.5f) * rcp); }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -164,19 +161,30 @@ __device__ __forceinline__ void fc_dft(float2 (&v)[R], bool inv) {
     }
 }
 
-// one Stockham stage of radix R over nl lines: butterfly j of a line reads x[j + t N / R], twiddles
-// by W_{Ns R}^{t k} (k = j mod Ns), transforms, and writes y[(j - k) R + k + u Ns]
+// one Stockham stage of radix R over nl lines (line l at l * ls, element stride es, the same
+// layout in and out): butterfly j of a line reads x[j + t N / R], twiddles by W_{Ns R}^{t k}
+// (k = j mod Ns), transforms, and writes y[(j - k) R + k + u Ns].  Consecutive threads take
+// consecutive lines when lines are interleaved (ls < es), else consecutive butterflies of a line.
 template <int R>
-__device__ inline void fc_stage(const float2* in, int lin, int ein, float2* out, int lout, int eout, int nl, int N,
-                                int Ns, const float2* tw, bool inv, int tid, int nth) {
+__device__ inline void fc_stage(const float2* in, float2* out, int ls, int es, int nl, int N, int Ns,
+                                const float2* tw, bool inv, int tid, int nth) {
     const int nb = N / R;
+    const bool line_fast = ls < es;
+    const float rnl = 1.f / (float)nl, rnb = 1.f / (float)nb, rns = 1.f / (float)Ns;
     for (int e = tid; e < nl * nb; e += nth) {
-        const int l = e / nb, j = e - l * nb;
-        const int k = j % Ns;
+        int l, j;
+        if (line_fast) {
+            j = fc_div(e, rnl);
+            l = e - j * nl;
+        } else {
+            l = fc_div(e, rnb);
+            j = e - l * nb;
+        }
+        const int k = j - fc_div(j, rns) * Ns;
         float2 v[R];
 #pragma unroll
         for (int t = 0; t < R; ++t) {
-            v[t] = in[l * lin + (j + t * nb) * ein];
+            v[t] = in[l * ls + (j + t * nb) * es];
             if (t > 0) {
                 float2 w = tw[k * R + t];
                 if (inv) w.y = -w.y;
@@ -186,144 +194,194 @@ __device__ inline void fc_stage(const float2* in, int lin, int ein, float2* out,
         fc_dft<R>(v, inv);
         const int d0 = (j - k) * R + k;
 #pragma unroll
-        for (int u = 0; u < R; ++u) out[l * lout + (d0 + u * Ns) * eout] = v[u];
+        for (int u = 0; u < R; ++u) out[l * ls + (d0 + u * Ns) * es] = v[u];
     }
 }
 
-// nl lines of length p.n, line l at base[l * lstride] with element stride es, transformed in
-// place through the dense scratch scr (>= nl * p.n elements, line-major); inverse = conjugate
-// twiddles, unnormalised
-__device__ inline void fc_lines(const FcPlan& p, float2* base, int nl, int lstride, int es, float2* scr,
+// nl lines of length p.n, line l at base[l * ls] with element stride es, transformed in place
+// through scratch scr of the same layout; inverse = conjugate twiddles, unnormalised.  Ends with
+// a barrier.
+__device__ inline void fc_lines(const FcPlan& p, float2* base, int nl, int ls, int es, float2* scr,
                                 const float2* tw, bool inverse, int tid, int nth) {
     const int N = p.n;
-    if (N == 1) return;
     int Ns = 1, off = 0;
     for (int s = 0; s < p.nf; ++s) {
         const int R = p.f[s];
-        const bool from_lines = (s % 2 == 0);
-        const float2* in = from_lines ? base : scr;
-        float2* out = from_lines ? scr : base;
-        const int lin = from_lines ? lstride : N, ein = from_lines ? es : 1;
-        const int lout = from_lines ? N : lstride, eout = from_lines ? 1 : es;
+        const float2* in = (s % 2 == 0) ? base : scr;
+        float2* out = (s % 2 == 0) ? scr : base;
         switch (R) {
-            case 2: fc_stage<2>(in, lin, ein, out, lout, eout, nl, N, Ns, tw + off, inverse, tid, nth); break;
-            case 3: fc_stage<3>(in, lin, ein, out, lout, eout, nl, N, Ns, tw + off, inverse, tid, nth); break;
-            case 4: fc_stage<4>(in, lin, ein, out, lout, eout, nl, N, Ns, tw + off, inverse, tid, nth); break;
-            case 5: fc_stage<5>(in, lin, ein, out, lout, eout, nl, N, Ns, tw + off, inverse, tid, nth); break;
-            default: fc_stage<7>(in, lin, ein, out, lout, eout, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            case 2: fc_stage<2>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            case 3: fc_stage<3>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            case 4: fc_stage<4>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            case 5: fc_stage<5>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            default: fc_stage<7>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
         }
         __syncthreads();
         off += Ns * R;
         Ns *= R;
     }
     if (p.nf % 2 == 1) {  // the result sits in the scratch: copy it back to the lines
+        const float rnl = 1.f / (float)nl, rn = 1.f / (float)N;
         for (int e = tid; e < nl * N; e += nth) {
-            const int l = e / N, o = e - l * N;
-            base[l * lstride + o * es] = scr[l * N + o];
+            int l, o;
+            if (ls < es) {
+                o = fc_div(e, rnl);
+                l = e - o * nl;
+            } else {
+                l = fc_div(e, rn);
+                o = e - l * N;
+            }
+            base[l * ls + o * es] = scr[l * ls + o * es];
         }
         __syncthreads();
     }
 }
 
-// Shared memory: [planes: P * K2 * Kh float2][work: max(2 * K2 * K3, 2 * chunk * K1) float2]
-// [stage twiddles: 3 * 2 * kFcMaxK float2]
-__host__ inline size_t fc_smem_bytes(const int K[3], int cl) {
-    const int Kh = K[2] / 2 + 1;
-    const int P = (K[0] + cl - 1) / cl;
-    size_t work = (size_t)2 * K[1] * K[2];
-    work = work > (size_t)2 * kFcChunk * K[0] ? work : (size_t)2 * kFcChunk * K[0];
-    return ((size_t)P * K[1] * Kh + work + 3 * 2 * kFcMaxK) * sizeof(float2);
+// shared memory of the plane kernels: rows [ceil(K2/2)][K3] (also the scratch of the y lines) +
+// the z scratch of the same size + the plane [K2][Kh] + stage twiddles of the two line lengths
+__host__ inline size_t fc_plane_smem(const int K[3]) {
+    const int np = (K[1] + 1) / 2, Kh = K[2] / 2 + 1;
+    size_t rows = (size_t)np * K[2];
+    if (rows < (size_t)K[1] * Kh) rows = (size_t)K[1] * Kh;  // the rows region is the y scratch too
+    return (2 * rows + (size_t)K[1] * Kh + 2 * kFcTw) * sizeof(float2);
 }
 
-__global__ void __launch_bounds__(kFcThreads) k_fftconv_cluster(FftConvArgs a) {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cluster = cg::this_cluster();
+// shared memory of the column kernel: kFcCols columns of K1 + scratch + x twiddles
+__host__ inline size_t fc_col_smem(const int K[3]) {
+    return ((size_t)2 * kFcCols * K[0] + kFcTw) * sizeof(float2);
+}
+
+// Forward pass over one x-plane per CTA: rows y = 2p, 2p + 1 of the real plane packed as one
+// complex row (a + i b), FFT along z, the two half spectra separated
+// (A = (C_k + conj C_{-k}) / 2, B = (C_k - conj C_{-k}) / 2i), FFT along y of the [K2][Kh] half
+// plane, written to the spectrum W[x][ky][kz]; the spread mesh plane is cleared for the next spread.
+__global__ void __launch_bounds__(kFcPlaneThreads) k_fc_fwd_planes(FftConvArgs a) {
     extern __shared__ float2 sm[];
-    const int K1 = a.K[0], K2 = a.K[1], K3 = a.K[2], Kh = a.Kh, cl = a.cl;
-    const int c = (int)cluster.block_rank();
-    const int tid = threadIdx.x, nth = blockDim.x;
-    const int P = (K1 + cl - 1) / cl;
-    float2* planes = sm;                                  // [P][K2][Kh]
-    float2* work = planes + (size_t)P * K2 * Kh;
-    size_t wsz = (size_t)2 * K2 * K3;
-    if (wsz < (size_t)2 * kFcChunk * K1) wsz = (size_t)2 * kFcChunk * K1;
-    float2* twx = work + wsz;
-    float2* twy = twx + 2 * kFcMaxK;
-    float2* twz = twy + 2 * kFcMaxK;
-    fc_twiddles(twx, a.px, tid, nth);
-    fc_twiddles(twy, a.py, tid, nth);
-    fc_twiddles(twz, a.pz, tid, nth);
-    __syncthreads();
-    const int my_planes = c < K1 ? (K1 - 1 - c) / cl + 1 : 0;
-    // ---- phase A: z (real rows as complex, keep kz < Kh) then y, per owned plane
-    for (int pl = 0; pl < my_planes; ++pl) {
-        const int x = c + pl * cl;
-        float2* rows = work;                              // [K2][K3]
-        float2* scr = work + (size_t)K2 * K3;
-        float* gin = a.grid_in + (size_t)x * K2 * K3;
-        for (int e = tid; e < K2 * K3; e += nth) {
-            rows[e] = make_float2(gin[e], 0.f);
-            gin[e] = 0.f;                                 // the next spread starts from zero
-        }
-        __syncthreads();
-        fc_lines(a.pz, rows, K2, K3, 1, scr, twz, false, tid, nth);
-        float2* plane = planes + (size_t)pl * K2 * Kh;    // [K2][Kh]
-        for (int e = tid; e < K2 * Kh; e += nth) plane[e] = rows[(e / Kh) * K3 + (e % Kh)];
-        __syncthreads();
-        fc_lines(a.py, plane, Kh, 1, Kh, scr, twy, false, tid, nth);
+    const int K2 = a.K[1], K3 = a.K[2], Kh = a.Kh;
+    const int np = (K2 + 1) / 2;
+    const int x = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    size_t rsz = (size_t)np * K3;
+    if (rsz < (size_t)K2 * Kh) rsz = (size_t)K2 * Kh;
+    float2* rows = sm;
+    float2* scr = rows + rsz;
+    float2* plane = scr + rsz;
+    float2* twy = plane + (size_t)K2 * Kh;
+    float2* twz = twy + kFcTw;
+    fc_load_twiddles(twy, a.tw[1], tid, nth);
+    fc_load_twiddles(twz, a.tw[2], tid, nth);
+    float* gin = a.grid_in + (size_t)x * K2 * K3;
+    const float rk3 = 1.f / (float)K3, rkh = 1.f / (float)Kh;
+#pragma unroll 4
+    for (int e = tid; e < np * K3; e += nth) {
+        const int p = fc_div(e, rk3), z = e - p * K3;
+        const int y1 = 2 * p + 1;
+        const float re = __ldg(gin + (2 * p) * K3 + z);
+        const float im = y1 < K2 ? __ldg(gin + y1 * K3 + z) : 0.f;
+        rows[e] = make_float2(re, im);
     }
-    cluster.sync();
-    // ---- phase B: columns (ky, kz) across the x-planes of the whole cluster
-    const int ncol = K2 * Kh;
-    for (int c0 = c; c0 < ncol; c0 += cl * kFcChunk) {
-        int nc = 0;
-        for (int q = 0; q < kFcChunk; ++q)
-            if (c0 + q * cl < ncol) nc = q + 1;
-        float2* col = work;                               // [nc][K1]
-        float2* scr = work + (size_t)kFcChunk * K1;
-        for (int e = tid; e < nc * K1; e += nth) {
-            const int q = e / K1, x = e % K1;
-            const int cc = c0 + q * cl;
-            float2* remote = cluster.map_shared_rank(planes, x % cl);
-            col[e] = remote[(size_t)(x / cl) * K2 * Kh + cc];
-        }
-        __syncthreads();
-        fc_lines(a.px, col, nc, K1, 1, scr, twx, false, tid, nth);
-        for (int e = tid; e < nc * K1; e += nth) {
-            const int q = e / K1, kx = e % K1;
-            const int cc = c0 + q * cl;
-            const float g = a.G[(size_t)kx * ncol + cc];  // [kx][ky][kz] = kx * K2 * Kh + cc
+    __syncthreads();
+    // the next spread starts from zero (this CTA has read its plane)
+    for (int e = tid; e < K2 * K3; e += nth) gin[e] = 0.f;
+    fc_lines(a.pz, rows, np, K3, 1, scr, twz, false, tid, nth);
+    for (int e = tid; e < K2 * Kh; e += nth) {
+        const int y = fc_div(e, rkh), kz = e - y * Kh;
+        const float2* r = rows + (size_t)(y >> 1) * K3;
+        const float2 c = r[kz], m = r[kz == 0 ? 0 : K3 - kz];  // C_k and C_{-k}
+        // even row: (C_k + conj C_-k) / 2; odd row: (C_k - conj C_-k) / 2i
+        plane[e] = (y & 1) ? make_float2(0.5f * (c.y + m.y), 0.5f * (m.x - c.x))
+                           : make_float2(0.5f * (c.x + m.x), 0.5f * (c.y - m.y));
+    }
+    __syncthreads();
+    fc_lines(a.py, plane, Kh, 1, Kh, rows, twy, false, tid, nth);
+    float2* w = a.spec + (size_t)x * K2 * Kh;
+    for (int e = tid; e < K2 * Kh; e += nth) w[e] = plane[e];
+}
+
+// Columns (ky, kz) of the spectrum, kFcCols per CTA: FFT along x, times the influence function,
+// inverse FFT along x, in place.
+__global__ void __launch_bounds__(kFcColThreads) k_fc_columns(FftConvArgs a) {
+    extern __shared__ float2 sm[];
+    const int K1 = a.K[0], ncol = a.K[1] * a.Kh;
+    const int c0 = blockIdx.x * kFcCols, tid = threadIdx.x, nth = blockDim.x;
+    const int nc = min(kFcCols, ncol - c0);
+    float2* col = sm;  // [K1][kFcCols]: line q at col + q, element stride kFcCols
+    float2* scr = col + (size_t)kFcCols * K1;
+    float2* twx = scr + (size_t)kFcCols * K1;
+    fc_load_twiddles(twx, a.tw[0], tid, nth);
+    const float2* spec = a.spec;
+#pragma unroll 4
+    for (int e = tid; e < K1 * kFcCols; e += nth) {
+        const int x = e / kFcCols, q = e - x * kFcCols;
+        col[e] = q < nc ? __ldg(spec + (size_t)x * ncol + c0 + q) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    fc_lines(a.px, col, nc, 1, kFcCols, scr, twx, false, tid, nth);
+    for (int e = tid; e < K1 * kFcCols; e += nth) {
+        const int kx = e / kFcCols, q = e - kx * kFcCols;
+        if (q < nc) {
+            const float g = __ldg(a.G + (size_t)kx * ncol + c0 + q);
             col[e].x *= g;
             col[e].y *= g;
         }
-        __syncthreads();
-        fc_lines(a.px, col, nc, K1, 1, scr, twx, true, tid, nth);
-        for (int e = tid; e < nc * K1; e += nth) {
-            const int q = e / K1, x = e % K1;
-            const int cc = c0 + q * cl;
-            float2* remote = cluster.map_shared_rank(planes, x % cl);
-            remote[(size_t)(x / cl) * K2 * Kh + cc] = col[e];
-        }
-        __syncthreads();
     }
-    cluster.sync();
-    // ---- phase C: inverse y, then Hermitian rows and inverse z, real part out
-    for (int pl = 0; pl < my_planes; ++pl) {
-        const int x = c + pl * cl;
-        float2* plane = planes + (size_t)pl * K2 * Kh;
-        float2* rows = work;
-        float2* scr = work + (size_t)K2 * K3;
-        fc_lines(a.py, plane, Kh, 1, Kh, scr, twy, true, tid, nth);
-        for (int e = tid; e < K2 * K3; e += nth) {
-            const int y = e / K3, z = e % K3;
-            const float2 v = z < Kh ? plane[y * Kh + z] : plane[y * Kh + (K3 - z)];
-            rows[e] = z < Kh ? v : make_float2(v.x, -v.y);
+    __syncthreads();
+    fc_lines(a.px, col, nc, 1, kFcCols, scr, twx, true, tid, nth);
+    for (int e = tid; e < K1 * kFcCols; e += nth) {
+        const int x = e / kFcCols, q = e - x * kFcCols;
+        if (q < nc) a.spec[(size_t)x * ncol + c0 + q] = col[e];
+    }
+}
+
+// Inverse pass over one x-plane per CTA: inverse FFT along y, the half spectra of rows 2p and
+// 2p + 1 completed Hermitian (imaginary parts of kz = 0 and kz = K3 / 2 dropped, as a complex-to-
+// real transform does) and packed as A + i B, inverse FFT along z, real and imaginary parts out as
+// the two real rows.
+__global__ void __launch_bounds__(kFcPlaneThreads) k_fc_inv_planes(FftConvArgs a) {
+    extern __shared__ float2 sm[];
+    const int K2 = a.K[1], K3 = a.K[2], Kh = a.Kh;
+    const int np = (K2 + 1) / 2;
+    const int x = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
+    size_t rsz = (size_t)np * K3;
+    if (rsz < (size_t)K2 * Kh) rsz = (size_t)K2 * Kh;
+    float2* rows = sm;
+    float2* scr = rows + rsz;
+    float2* plane = scr + rsz;
+    float2* twy = plane + (size_t)K2 * Kh;
+    float2* twz = twy + kFcTw;
+    fc_load_twiddles(twy, a.tw[1], tid, nth);
+    fc_load_twiddles(twz, a.tw[2], tid, nth);
+    const float2* w = a.spec + (size_t)x * K2 * Kh;
+#pragma unroll 4
+    for (int e = tid; e < K2 * Kh; e += nth) plane[e] = __ldg(w + e);
+    __syncthreads();
+    fc_lines(a.py, plane, Kh, 1, Kh, rows, twy, true, tid, nth);
+    const bool even = (K3 % 2) == 0;
+    const float rk3 = 1.f / (float)K3;
+    for (int e = tid; e < np * K3; e += nth) {
+        const int p = fc_div(e, rk3), z = e - p * K3;
+        const int y0 = 2 * p, y1 = 2 * p + 1;
+        const bool lo = z < Kh;
+        const int zz = lo ? z : K3 - z;
+        float2 A = plane[y0 * Kh + zz];
+        float2 B = y1 < K2 ? plane[y1 * Kh + zz] : make_float2(0.f, 0.f);
+        if (z == 0 || (even && z == K3 / 2)) {
+            A.y = 0.f;
+            B.y = 0.f;
         }
-        __syncthreads();
-        fc_lines(a.pz, rows, K2, K3, 1, scr, twz, true, tid, nth);
-        float* gout = a.grid_out + (size_t)x * K2 * K3;
-        for (int e = tid; e < K2 * K3; e += nth) gout[e] = rows[e].x;
-        __syncthreads();
+        if (!lo) {
+            A.y = -A.y;
+            B.y = -B.y;
+        }
+        rows[e] = make_float2(A.x - B.y, A.y + B.x);  // A + i B
+    }
+    __syncthreads();
+    fc_lines(a.pz, rows, np, K3, 1, scr, twz, true, tid, nth);
+    float* gout = a.grid_out + (size_t)x * K2 * K3;
+    for (int e = tid; e < np * K3; e += nth) {
+        const int p = fc_div(e, rk3), z = e - p * K3;
+        const float2 v = rows[e];
+        gout[(2 * p) * K3 + z] = v.x;
+        if (2 * p + 1 < K2) gout[(2 * p + 1) * K3 + z] = v.y;
     }
 }
 

@@ -149,7 +149,8 @@ struct dmffb_engine {
     bool cell_pass = false;  // dmffb_classical_set_cell_pass: pairs from the cell grid, no list
     // dipole-solve convolution in one thread-block cluster (FP32, meshes up to 64 per axis)
     bool fc_enabled = false;  // dmffb_set_fused_fft
-    int fc_cl = -1;          // CTAs per cluster for the current mesh (0: not available, -1: not decided)
+    int fc_ok = -1;          // the engine's FFT convolution serves this mesh (1), not (0), not decided (-1)
+    float2* d_fcW = nullptr;  // [K1][K2][K3/2+1] half spectrum between its passes
     float* d_fcG = nullptr;  // [K1*K2*Kh] influence function of the half spectrum
     int64_t fcG_cap = 0;
     int32_t* d_covrows = nullptr;  // [n_covrows*3] covalent rows (i < j, nbond)
@@ -294,7 +295,7 @@ enum { KC_PREP = 0, KC_PAIR_FULL, KC_PAIR_FIELD, KC_PAIR_MATVEC, KC_SPREAD, KC_F
        KC_GATHER_FIELD, KC_SELF, KC_VEC, KC_NBLIST, KC_MVCOEF,
        // FP64 launches over the topologically scaled rows, parameter-adjoint pair kernels, bonded terms
        KC_PAIR_FULL_SCALED, KC_PAIR_FIELD_SCALED, KC_PGRAD, KC_BONDED,
-       KC_FFTCONV,  // the dipole solve's forward FFT + influence multiply + inverse FFT in one cluster
+       KC_FFTCONV,  // the dipole solve's forward FFT + influence multiply + inverse FFT (engine FFT)
        KC_COUNT };
 static_assert(KC_COUNT <= 32, "kernel-class statistics arrays hold 32 classes");
 
@@ -532,58 +533,43 @@ int lmax_eff(const dmffb_engine* h) { return (h->lmax == 0 && h->lpol) ? 1 : h->
 // reciprocal pass: spread (Qg and/or U) -> FFT -> convolution -> inverse FFT -> gather
 // per-atom wrapped stencil origins and spline weights at these positions, for the cached dipole
 // spread and field gather of the dipole solve
-// Cluster size of the fused dipole-solve convolution for the current mesh: 16 CTAs (non-portable
-// size) or 8, when the kernel's shared memory fits and the device can place such a cluster; 0 when
-// the mesh is larger than 64 points on an axis or no cluster fits (the cuFFT path runs then).
+// Whether the engine's FFT convolution serves the current mesh: FP32, 7-smooth extents of at most
+// 64 points and the kernels' shared memory granted; otherwise the cuFFT path runs.
 int fc_decide(dmffb_engine* h) {
-    if (h->fc_cl >= 0) return h->fc_cl;
-    h->fc_cl = 0;
+    if (h->fc_ok >= 0) return h->fc_ok;
+    h->fc_ok = 0;
     if (h->prec != DMFFB_FP32 || !h->lpme) return 0;
     for (int k = 0; k < 3; ++k) {
         bool smooth = false;
         fc_plan(h->K[k], &smooth);
         if (h->K[k] < 2 || h->K[k] > kFcMaxK || !smooth) return 0;
     }
-    for (int cl : {16, 8}) {
-        const size_t smem = fc_smem_bytes(h->K, cl);
-        if (smem > 227 * 1024) continue;
-        if (cudaFuncSetAttribute(k_fftconv_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            continue;
-        if (cl > 8 && cudaFuncSetAttribute(k_fftconv_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                          cudaSuccess)
-            continue;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(cl);
-        cfg.blockDim = dim3(kFcThreads);
-        cfg.dynamicSmemBytes = smem;
-        cudaLaunchAttribute attr;
-        attr.id = cudaLaunchAttributeClusterDimension;
-        attr.val.clusterDim.x = cl;
-        attr.val.clusterDim.y = 1;
-        attr.val.clusterDim.z = 1;
-        cfg.attrs = &attr;
-        cfg.numAttrs = 1;
-        int nclusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&nclusters, k_fftconv_cluster, &cfg) == cudaSuccess && nclusters > 0) {
-            h->fc_cl = cl;
-            break;
-        }
-        cudaGetLastError();  // clear a refused configuration
+    const size_t sp = fc_plane_smem(h->K), sc = fc_col_smem(h->K);
+    if (sp > 227 * 1024 || sc > 227 * 1024) return 0;
+    if (cudaFuncSetAttribute(k_fc_fwd_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp) != cudaSuccess ||
+        cudaFuncSetAttribute(k_fc_inv_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp) != cudaSuccess ||
+        cudaFuncSetAttribute(k_fc_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
-    return h->fc_cl;
+    h->fc_ok = 1;
+    return 1;
 }
 
-// influence-function table of the fused convolution for this box (once per dipole solve)
+// influence-function table and spectrum buffer of the engine's FFT convolution for this box (once
+// per dipole solve)
 int fc_prepare(dmffb_engine* h, cudaStream_t s, const Box& bx) {
     const int Kh = h->K[2] / 2 + 1;
     const int64_t m = (int64_t)h->K[0] * h->K[1] * Kh;
     int st;
     if (m > h->fcG_cap) {
         if (h->d_fcG) cudaFree(h->d_fcG);
+        if (h->d_fcW) cudaFree(h->d_fcW);
         h->d_fcG = nullptr;
+        h->d_fcW = nullptr;
         h->fcG_cap = m;
         if ((st = dalloc(h, &h->d_fcG, m * sizeof(float)))) return st;
+        if ((st = dalloc(h, &h->d_fcW, m * sizeof(float2)))) return st;
     }
     LAUNCH(h, s, KC_VEC, k_fc_gtable<<<nblk(m, 256), 256, 0, s>>>(h->K[0], h->K[1], h->K[2], Kh, bx, h->d_bmod,
                                                                   h->kappa, fabs(det3(bx.h)), h->d_fcG));
@@ -592,29 +578,26 @@ int fc_prepare(dmffb_engine* h, cudaStream_t s, const Box& bx) {
 }
 
 int fc_launch(dmffb_engine* h, cudaStream_t s, float* in, float* out) {
-    FftConvArgs a;
+    static_assert(sizeof(FftConvArgs) <= 4000, "launch arguments of the FFT convolution");
+    FftConvArgs a = {};
     for (int k = 0; k < 3; ++k) a.K[k] = h->K[k];
     a.Kh = h->K[2] / 2 + 1;
-    a.cl = h->fc_cl;
     a.grid_in = in;
     a.grid_out = out;
+    a.spec = h->d_fcW;
     a.G = h->d_fcG;
     a.px = fc_plan(h->K[0]);
     a.py = fc_plan(h->K[1]);
     a.pz = fc_plan(h->K[2]);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(h->fc_cl);
-    cfg.blockDim = dim3(kFcThreads);
-    cfg.dynamicSmemBytes = fc_smem_bytes(h->K, h->fc_cl);
-    cfg.stream = s;
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeClusterDimension;
-    attr.val.clusterDim.x = h->fc_cl;
-    attr.val.clusterDim.y = 1;
-    attr.val.clusterDim.z = 1;
-    cfg.attrs = &attr;
-    cfg.numAttrs = 1;
-    LAUNCH(h, s, KC_FFTCONV, CK(cudaLaunchKernelEx(&cfg, k_fftconv_cluster, a)));
+    fc_host_twiddles(a.px, a.tw[0]);
+    fc_host_twiddles(a.py, a.tw[1]);
+    fc_host_twiddles(a.pz, a.tw[2]);
+    const size_t sp = fc_plane_smem(h->K), sc = fc_col_smem(h->K);
+    const int ncb = (h->K[1] * a.Kh + kFcCols - 1) / kFcCols;
+    LAUNCH(h, s, KC_FFTCONV, k_fc_fwd_planes<<<h->K[0], kFcPlaneThreads, sp, s>>>(a));
+    LAUNCH(h, s, KC_FFTCONV, k_fc_columns<<<ncb, kFcColThreads, sc, s>>>(a));
+    LAUNCH(h, s, KC_FFTCONV, k_fc_inv_planes<<<h->K[0], kFcPlaneThreads, sp, s>>>(a));
+    CK(cudaGetLastError());
     return DMFFB_OK;
 }
 
@@ -780,7 +763,7 @@ int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, 
         if (fork) CK(cudaEventRecord(h->e_join, h->s2));
     }
     LAUNCH(h, s, KC_SPREAD, k_spread_dip_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(sa, stencil_cache<T>(h)));
-    if (sizeof(T) == 4 && h->fc_enabled && h->fc_cl > 0) {
+    if (sizeof(T) == 4 && h->fc_enabled && h->fc_ok > 0) {
         // forward FFT, influence multiply and inverse FFT in one cluster; it also clears grid2
         int stc = fc_launch(h, s, (float*)h->d_grid2, (float*)h->d_grid);
         if (stc) return stc;
@@ -1049,7 +1032,7 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         std::vector<double> key = {(double)(uintptr_t)pos, (double)(uintptr_t)pairs, (double)npairs,
                                    (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T),
                                    (double)(uintptr_t)h->d_mvcoef, (double)(uintptr_t)h->d_csr_off,
-                                   (double)(h->fc_enabled ? h->fc_cl : 0), (double)(uintptr_t)h->d_fcG};
+                                   (double)(h->fc_enabled ? h->fc_ok : 0), (double)(uintptr_t)h->d_fcG};
         for (int k = 0; k < 9; ++k) key.push_back(bx.h[k]);
         if (!h->cg_exec || key != h->cg_key) {
             if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
@@ -1802,7 +1785,7 @@ int upload_topology(dmffb_engine* h, const dmffb_admp_desc* d) {
 
 // PME mesh of h->K: grids grown to fit, B-spline moduli, cuFFT plans (cached per mesh shape)
 int setup_mesh(dmffb_engine* h) {
-    h->fc_cl = -1;  // the fused convolution's cluster size is decided again for this mesh
+    h->fc_ok = -1;  // whether the engine's FFT convolution serves the mesh is decided again
     const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
     const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
     const int64_t Kc = (int64_t)h->K[0] * h->K[1] * (h->K[2] / 2 + 1);
@@ -1975,7 +1958,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
+                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_fcW, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -3183,9 +3166,9 @@ int dmffb_set_fused_fft(dmffb_engine* h, int32_t enabled) {
     return DMFFB_OK;
 }
 
-int dmffb_fused_fft_cluster(const dmffb_engine* h) {
+int dmffb_fused_fft_active(const dmffb_engine* h) {
     if (!h) return -1;
-    return h->fc_enabled && h->fc_cl > 0 ? h->fc_cl : 0;
+    return h->fc_enabled && h->fc_ok > 0 ? 1 : 0;
 }
 
 int dmffb_set_graphs(dmffb_engine* h, int32_t enabled) {

@@ -319,13 +319,13 @@ class AdmpEngine:
         return buf[: need.value]
 
     def set_fused_fft(self, on=True):
-        """The dipole solve's reciprocal convolution in one thread-block cluster (FP32, meshes up
-        to 64 per axis) or through cuFFT (dmffb_set_fused_fft)."""
+        """The dipole solve's reciprocal convolution through the engine's own FFT kernels (FP32,
+        7-smooth meshes up to 64 per axis) or through cuFFT (dmffb_set_fused_fft)."""
         self._check(self.lib.dmffb_set_fused_fft(self.h, int(bool(on))))
 
-    def fused_fft_cluster(self):
-        """CTAs per cluster of the last solve's convolution (0: cuFFT)."""
-        return int(self.lib.dmffb_fused_fft_cluster(self.h))
+    def fused_fft_active(self):
+        """Whether the last solve's convolution ran through the engine's FFT (else cuFFT)."""
+        return bool(self.lib.dmffb_fused_fft_active(self.h))
 
     def set_timing(self, on=True):
         self.lib.dmffb_set_timing(self.h, int(on))

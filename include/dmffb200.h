@@ -208,7 +208,7 @@ int dmffb_set_timing(dmffb_engine* h, int32_t enabled);
  * 2 pair FIELD, 3 pair MATVEC, 4 spread, 5 FFT (cuFFT), 6 convolution, 7 gather FULL,
  * 8 gather FIELD, 9 self+frame forces, 10 vector/CG ops, 11 neighbour build, 12 CG matvec
  * pair-tensor set-up, 13 pair FULL over the topologically scaled rows (FP64), 14 pair FIELD over
- * the scaled rows (FP64), 15 parameter-adjoint pair kernels, 16 bonded terms, 17 the clustered
+ * the scaled rows (FP64), 15 parameter-adjoint pair kernels, 16 bonded terms, 17 the engine-FFT
  * convolution of the dipole solve (dmffb_set_fused_fft).  Classes 1 and 2
  * hold only the launches over the unscaled rows (kernel precision). */
 int dmffb_set_profiling(dmffb_engine* h, int32_t enabled);
@@ -326,11 +326,12 @@ int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, do
                                 double* dE_dbond, double* dE_dangle, double* dE_dtorsion);
 
 /* The dipole-solve iterations' reciprocal convolution (forward FFT, influence-function multiply,
- * inverse FFT) in one thread-block cluster holding the half spectrum in distributed shared memory,
- * on/off (on by default; FP32 engines with meshes of at most 64 points per axis, else cuFFT).
- * dmffb_fused_fft_cluster returns the cluster size the last solve used (0: the cuFFT path). */
+ * inverse FFT) through the engine's own three-pass FFT (x-planes, spectrum columns with the
+ * multiply, x-planes) instead of cuFFT R2C + convolution + C2R, on/off (off by default; FP32
+ * engines with 7-smooth meshes of at most 64 points per axis, else cuFFT).
+ * dmffb_fused_fft_active returns 1 when the last solve used it, 0 for the cuFFT path. */
 int dmffb_set_fused_fft(dmffb_engine* h, int32_t enabled);
-int dmffb_fused_fft_cluster(const dmffb_engine* h);
+int dmffb_fused_fft_active(const dmffb_engine* h);
 /* ---------------------------------------------------------------------------------------
  * Short-range pairwise terms with per-atom parameters: the built-in kernels of
  * dmff/admp/pairwise.py evaluated in CUDA (what generate_pairwise_interaction, pairwise.py:47-95,

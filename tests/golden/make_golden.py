@@ -107,6 +107,9 @@ def main():
         # XML reader inputs (tests/test_frontend/test_xmlio.py)
         f"{REF}/tests/data/test1.xml": "xmlio_test1.xml",
         f"{REF}/tests/data/test2.xml": "xmlio_test2.xml",
+        # Slater-ISA / short-range inputs (tests/test_admp/test_slater.py)
+        f"{REF}/tests/data/peg.xml": "peg.xml",
+        f"{REF}/tests/data/peg2.pdb": "peg2.pdb",
         f"{wf}/forcefield.xml": "waterbox_forcefield.xml",
         f"{wf}/residues.xml": "waterbox_residues.xml",
         f"{wf}/quadrupole_nonpol/forcefield.xml": "waterbox_quadrupole_nonpol.xml",
@@ -165,6 +168,14 @@ def main():
                 entry.update({"atol": 1e-2} if test == "test_coul_pme" else tol)
                 classical.append(entry)
     energies["classical"] = classical
+    # the nine PEG dimer energies of the short-range test, in the order its potentials are called
+    slater = parametrize_cases(f"{REF}/tests/test_admp/test_slater.py")["test_admp_slater"][0]
+    energies["peg2_slater"] = {
+        "pdb": os.path.basename(slater["pdb"]), "xml": os.path.basename(slater["prm"]), "rc_nm": 1.49,
+        "ethresh": 1e-4, "decimal": 4, "source": "tests/test_admp/test_slater.py:17-27",
+        "forces": ["ADMPPmeForce", "ADMPDispPmeForce", "SlaterExForce", "SlaterSrEsForce", "SlaterSrPolForce",
+                   "SlaterSrDispForce", "SlaterDhfForce", "QqTtDampingForce", "SlaterDampingForce"],
+        "values": [float(v) for v in slater["values"]]}
     with open(os.path.join(HERE, "energies.json"), "w") as f:
         json.dump(energies, f, indent=1)
 
