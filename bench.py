@@ -23,7 +23,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 
 import numpy as np
@@ -50,6 +49,9 @@ def parse():
     p.add_argument("--serving-rates", default="50,100,200,500,1000,2000", help="Poisson arrival rates (req/s)")
     p.add_argument("--serving-slots", type=int, default=12)
     p.add_argument("--serving-budget-gb", type=float, default=2.0)
+    p.add_argument("--cg", default="auto", choices=["auto", "persistent", "per-pass"],
+                   help="dipole solve: persistent CG kernel, graph-replayed per-pass solve, or the "
+                        "engine's size rule (persistent up to 4096 atoms)")
     p.add_argument("--fused-fft", action="store_true",
                    help="dipole-solve convolution through the engine's FFT kernels instead of cuFFT")
     return p.parse_args()
@@ -69,75 +71,51 @@ def workload_config(name, s, world=1):
 
 # ---------------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """SM clock, power and clock-event reasons sampled while the timed region runs: NVML every
-    5 ms (read-only queries; the device matched by PCI bus id), else nvidia-smi every 200 ms."""
+    """SM clock, power and clock-event reasons sampled while the timed region runs: one
+    ``nvidia-smi --query-gpu ... -lms 20`` process (read-only queries, a sample every 20 ms) from
+    entry to exit, its CSV parsed afterwards."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    PERIOD_MS = 20
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.rows = []  # (sm_mhz, max_mhz, [reason names])
-        self._stop = threading.Event()
-        self._t = None
-        self._nvml = None
+        self._p = None
+
+    def __enter__(self):
         try:
-            import pynvml
-            import torch
-            pynvml.nvmlInit()
-            try:
-                bus = torch.cuda.get_device_properties(gpu_index).pci_bus_id
-                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
-            except Exception:
-                h = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
-            self._nvml = (pynvml, h)
-            self.source = "NVML, 5 ms"
+            self._p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                        "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
-            self.source = "nvidia-smi, 200 ms"
+            self._p = None
+        return self
 
-    def _sample_nvml(self):
-        nv, h = self._nvml
-        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-        masks = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
-                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
-        self.rows.append((float(sm), float(mx), [n for n, m in zip(self.NAMES, masks) if bits & m]))
-
-    def _sample_smi(self):
-        out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-        for line in out.stdout.strip().splitlines():
+    def __exit__(self, *a):
+        if self._p is None:
+            return
+        time.sleep(2 * self.PERIOD_MS / 1000.0)  # at least one sample after the timed region
+        self._p.terminate()
+        try:
+            out, _ = self._p.communicate(timeout=10)
+        except Exception:
+            self._p.kill()
+            out, _ = self._p.communicate()
+        for line in out.strip().splitlines():
             r = [x.strip() for x in line.split(",")]
             if len(r) >= 9 and r[1].replace(".", "").isdigit():
                 self.rows.append((float(r[1]), float(r[2]),
                                   [n for k, n in enumerate(self.NAMES) if r[5 + k] == "Active"]))
-
-    def _run(self):
-        period = 0.005 if self._nvml else 0.2
-        while not self._stop.is_set():
-            try:
-                self._sample_nvml() if self._nvml else self._sample_smi()
-            except Exception:
-                pass
-            self._stop.wait(period)
-
-    def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
-        return self
-
-    def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
 
     def summary(self):
         sm = [r[0] for r in self.rows]
         mx = [r[1] for r in self.rows]
         reasons = sorted({n for r in self.rows for n in r[2]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(sm), "source": self.source}
+                "reasons": reasons, "samples": len(sm), "source": f"nvidia-smi -lms {self.PERIOD_MS}"}
 
 
 # ---------------------------------------------------------------------------------- roofline
@@ -202,7 +180,21 @@ def class_rooflines(stats, steps, work, fp32_peak, hbm_peak):
     return out
 
 
-def admp_work(s, n_pairs, n_scaled):
+def cg_solve_bytes(s, n_pairs, iters):
+    """Algorithmic bytes of one persistent CG solve (k_cg_solve) of ``iters`` iterations, per
+    iteration: the matvec's 12 B per CSR entry (24 B per pair), the dipole spread and field gather
+    (N(12 + 16) + 4K^3 and 4K^3 + N(12 + 16 + 24)), the three FFT passes (mesh read, spectrum
+    written, spectrum read and written by the column pass, spectrum read, mesh written: 24 K^3 in
+    FP32 complex half-spectrum units counted as 4 B per real mesh point), and the CG vectors (the
+    direction update reads z, p and writes p; the update reads p, Ap, fmv, r, x, pol and writes x,
+    r, z: 24 + 80 B per atom component)."""
+    n = s["n_atoms"]
+    K3 = float(np.prod(s["K"]))
+    per_iter = 24.0 * n_pairs + n * (12 + 16) + 4 * K3 + 4 * K3 + n * (12 + 16 + 24) + 24 * K3 + 3 * n * (24 + 80)
+    return iters * per_iter
+
+
+def admp_work(s, n_pairs, n_scaled, iters=0):
     """Algorithmic work per launch of each class for a polarizable ADMP step (fixed convention:
     FMA = 2 flop, exp / erf / erfc / sqrt / div = 1 flop): pair FULL polarizable 1900 flop/pair,
     FIELD 600 flop/pair, the CG matvec 12 B per CSR entry (two entries per pair: packed j + two
@@ -217,7 +209,7 @@ def admp_work(s, n_pairs, n_scaled):
             "pair_full_scaled": ("fp64", 1900.0 * n_scaled), "pair_field_scaled": ("fp64", 600.0 * n_scaled),
             "pair_matvec": ("hbm", 12.0 * 2 * n_pairs), "matvec_coef": ("fp32", 200.0 * n_pairs),
             "spread": ("hbm", n * (12 + 4 * 4) + 4 * K3), "gather_field": ("hbm", 4 * K3 + n * (12 + 16 + 24)),
-            "conv": ("hbm", 16 * K3)}
+            "conv": ("hbm", 16 * K3), "cg_persistent": ("hbm", cg_solve_bytes(s, n_pairs, iters))}
 
 
 def headline_roofline(classes, per_launch_bytes, traffic, peak, peak_src, kernel, cls):
@@ -338,6 +330,40 @@ def serving_ideal_seconds(systems, iters, peaks, fp32_peak):
     return flops / (fp32_peak * 1e12) + byts / (peaks["hbm_gbs"] * 1e9)
 
 
+def serving_ceiling(systems, fp32_seq, plain, offline_wall_s):
+    """Where the plain path's time goes and what cross-request batching could at most gain: per
+    size bucket (waters) the requests, their share of the atoms, and the per-request service times
+    of the FP32 engine and of the plain FP64 path, each run one request at a time; then two bounds
+    on the whole-stream speedup over the plain path: (1) every request at the largest bucket's FP32
+    rate (atom-evals/s), (2) every request below the largest bucket free (perfect batching of the
+    small, launch-bound boxes) and the largest bucket as measured."""
+    edges = [100, 300, 1000, 3000, 10001]
+    waters = np.array([s["n_atoms"] // 3 for s in systems])
+    atoms = np.array([s["n_atoms"] for s in systems], dtype=np.float64)
+    t32 = np.array([r.c.t_done - r.c.t_start for r in fp32_seq])
+    t64 = np.array([r.c.t_done - r.c.t_start for r in plain])
+    buckets = []
+    for lo, hi in zip(edges[:-1], edges[1:]):
+        m = (waters >= lo) & (waters < hi)
+        if not m.any():
+            continue
+        buckets.append({"waters": f"{lo}-{hi - 1}", "requests": int(m.sum()),
+                        "atom_share": round(float(atoms[m].sum() / atoms.sum()), 4),
+                        "fp32_ms_median": round(float(np.median(t32[m])) * 1e3, 3),
+                        "fp64_plain_ms_median": round(float(np.median(t64[m])) * 1e3, 3),
+                        "fp32_s": round(float(t32[m].sum()), 4), "fp64_plain_s": round(float(t64[m].sum()), 4),
+                        "fp32_atom_evals_per_s": float(atoms[m].sum() / t32[m].sum()),
+                        "fp64_plain_atom_evals_per_s": float(atoms[m].sum() / t64[m].sum())})
+    top = buckets[-1]
+    T64 = float(t64.sum())
+    t_all_top = float(atoms.sum()) / top["fp32_atom_evals_per_s"]
+    return {"buckets": buckets, "plain_fp64_service_s": round(T64, 4),
+            "fp32_sequential_service_s": round(float(t32.sum()), 4), "offline_fp32_wall_s": round(offline_wall_s, 4),
+            "bound_all_at_largest_bucket_rate": round(T64 / t_all_top, 3),
+            "bound_small_requests_free": round(T64 / top["fp32_s"], 3),
+            "measured_offline_speedup": round(T64 / offline_wall_s, 3)}
+
+
 def bench_serving(args, systems, dev, peaks, fp32_peak):
     """The serving stream: continuous-batching FP32 server (saturation and Poisson arrivals) and the
     plain FP64 path (one request at a time, no graphs) on the same requests; latency = completion -
@@ -389,6 +415,14 @@ def bench_serving(args, systems, dev, peaks, fp32_peak):
     out["plain_fp64_reference_solver"] = dict(rst, sample="every request of the stream, one at a time",
                                               solver="fixed-point dipole iteration, POL_CONV 1.0, MAX_N_POL 30")
     out["speedup_vs_plain_reference_solver"] = out["offline_fp32"]["atom_evals_per_s"] / rst["atom_evals_per_s"]
+    # the same FP32 engine one request at a time (graphs on): per-request service times for the
+    # ceiling breakdown
+    seq = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp32", device=dev)
+    seq.prewarm([ServingRequest(s) for s in warm])
+    sreqs, sst = seq.run_stream(systems, np.zeros(len(systems)))
+    seq.close()
+    out["sequential_fp32"] = dict(sst, sample="every request of the stream, one at a time, graphs on")
+    out["ceiling"] = serving_ceiling(systems, sreqs, preqs, out["offline_fp32"]["wall_s"])
     errs_e, errs_f = [], []
     for q, p in zip(fp32, preqs):
         errs_e.append(abs(q.energy - p.energy) / abs(p.energy))
@@ -623,6 +657,7 @@ def main():
                      solver="cg", cg_tol=1e-6, max_iter=1000, device=dev)
     eng.set_params(s["Q_local"], s.get("pol"), s.get("thole"))
     eng.set_fused_fft(args.fused_fft)
+    eng.set_persistent_cg({"auto": "auto", "persistent": 1, "per-pass": 0}[args.cg])
     if s["lpol"]:
         eng.set_zero_guess(True)  # every step solves from U = 0 (the reference's U_init = None)
     pos = torch.tensor(s["pos"], dtype=torch.float64, device=dev)
@@ -693,10 +728,20 @@ def main():
     eng.set_profiling(False)
     n_pairs = int(res.n_pairs)
     n_scaled = int((eng.internal_pairs()[:, 2] != 0).sum().item())
-    classes = class_rooflines(stats, args.steps, admp_work(s, n_pairs, n_scaled), fp32_peak, peaks["hbm_gbs"])
-    # the kernel with the largest share of the step's launches: the CG matvec, 12 B per CSR entry
-    roof = headline_roofline(classes, 12.0 * 2 * n_pairs, None, peaks["hbm_gbs"], src, "k_matvec_apply (CG matvec)",
-                             "pair_matvec")
+    n_iter_med = int(statistics.median(iters)) if s["lpol"] else 0
+    classes = class_rooflines(stats, args.steps, admp_work(s, n_pairs, n_scaled, n_iter_med), fp32_peak,
+                              peaks["hbm_gbs"])
+    if "cg_persistent" in classes:
+        # the kernel with the largest share of the step: the persistent CG solve; its passes
+        # timed on the device clock inside the kernel (CTA 0, barrier waits included)
+        classes["cg_persistent"]["passes_ms_per_step"] = {k: round(v / args.steps, 4)
+                                                          for k, v in eng.cg_phase_times().items()}
+        roof = headline_roofline(classes, cg_solve_bytes(s, n_pairs, n_iter_med), None, peaks["hbm_gbs"], src,
+                                 "k_cg_solve (persistent CG dipole solve)", "cg_persistent")
+    else:
+        # the per-pass solve: the CG matvec, 12 B per CSR entry
+        roof = headline_roofline(classes, 12.0 * 2 * n_pairs, None, peaks["hbm_gbs"], src,
+                                 "k_matvec_apply (CG matvec)", "pair_matvec")
 
     c4 = None
     if world == 1 and not args.no_c4 and args.workload == "c1":
@@ -723,7 +768,11 @@ def main():
                "library_launches": {"cufft_execs": int(launches1["fft_execs"] - launches0["fft_execs"])},
                "result": {"energy_kJmol": res.energy, "cg_iters": n_iter, "converged": int(res.converged),
                           "n_pairs": n_pairs, "n_pairs_scaled": n_scaled}}
-        out["config"]["dipole_convolution"] = ("engine FFT kernels (k_fc_*)" if eng.fused_fft_active()
+        pcg = eng.persistent_cg_blocks() > 0
+        out["config"]["dipole_solve"] = (f"persistent CG kernel k_cg_solve ({eng.persistent_cg_blocks()} co-resident CTAs)"
+                                         if pcg else "graph-replayed per-pass CG")
+        out["config"]["dipole_convolution"] = ("engine FFT passes inside k_cg_solve" if pcg else
+                                               "engine FFT kernels (k_fc_*)" if eng.fused_fft_active()
                                                else "cuFFT R2C + k_conv + cuFFT C2R")
         if world == 1 and not args.no_cpu_baseline:
             cs, run, cores = cpu_reference_runner()

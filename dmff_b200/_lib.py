@@ -18,6 +18,7 @@ DMFFB_NEIGHBOR_OVERFLOW = 5
 DMFFB_NONFINITE = 6
 DMFFB_CUFFT_ERROR = 7
 DMFFB_SCRATCH_TOO_SMALL = 8
+DMFFB_TIMEOUT = 9
 NOALLOC_MAX_ATOMS = 65536
 
 DMFFB_FP32 = 0
@@ -35,7 +36,7 @@ EXPORTED = [
     "dmffb_classical_create", "dmffb_classical_set_params", "dmffb_classical_set_terms",
     "dmffb_classical_set_param_grads", "dmffb_classical_compute", "dmffb_classical_param_grads",
     "dmffb_classical_set_cell_pass",
-    "dmffb_set_graphs", "dmffb_set_fused_fft", "dmffb_fused_fft_active", "dmffb_admp_backward", "dmffb_admp_param_grads_host", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
+    "dmffb_set_graphs", "dmffb_set_fused_fft", "dmffb_fused_fft_active", "dmffb_set_persistent_cg", "dmffb_persistent_cg_blocks", "dmffb_set_cg_wait_limit", "dmffb_get_cg_phase_times", "dmffb_admp_backward", "dmffb_admp_param_grads_host", "dmffb_admp_set_param_grads", "dmffb_admp_set_zero_guess", "dmffb_admp_param_grads", "dmffb_server_create", "dmffb_server_submit", "dmffb_server_wait", "dmffb_server_clock",
     "dmffb_request_footprint", "dmffb_server_prewarm", "dmffb_server_destroy", "dmffb_md_force_create",
     "dmffb_md_force_execute", "dmffb_md_force_last_result", "dmffb_md_force_dipoles", "dmffb_md_force_destroy",
     "dmffb_pairwise_create", "dmffb_pairwise_set_params", "dmffb_pairwise_set_param_grads", "dmffb_pairwise_compute",
@@ -54,7 +55,7 @@ DMFFB_TERM_TORSION = 2
 
 KERNEL_CLASSES = ["prepare", "pair_full", "pair_field", "pair_matvec", "spread", "fft", "conv", "gather_full",
                   "gather_field", "self_frames", "vector", "neighbors", "matvec_coef", "pair_full_scaled",
-                  "pair_field_scaled", "param_grads", "bonded", "fft_conv"]
+                  "pair_field_scaled", "param_grads", "bonded", "fft_conv", "cg_persistent"]
 
 
 class AdmpDesc(ctypes.Structure):
@@ -323,6 +324,10 @@ def load():
     lib.dmffb_set_graphs.argtypes = [vp, i32]
     lib.dmffb_set_fused_fft.argtypes = [vp, i32]
     lib.dmffb_fused_fft_active.argtypes = [vp]
+    lib.dmffb_set_persistent_cg.argtypes = [vp, i32]
+    lib.dmffb_persistent_cg_blocks.argtypes = [vp]
+    lib.dmffb_set_cg_wait_limit.argtypes = [vp, ctypes.c_double, i32]
+    lib.dmffb_get_cg_phase_times.argtypes = [vp, vp, i32]
     lib.dmffb_server_create.argtypes = [P(ServerDesc), P(vp)]
     lib.dmffb_server_submit.argtypes = [vp, P(Request)]
     lib.dmffb_server_wait.argtypes = [vp, dbl]

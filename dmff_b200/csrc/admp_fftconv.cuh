@@ -1,6 +1,6 @@
 // Reciprocal convolution of the dipole-solve iterations in three kernels of the engine's own
 // FFT: real mesh -> forward 3-D FFT -> multiply by the influence function -> inverse 3-D FFT ->
-// real mesh, for 7-smooth meshes of up to 64 points per axis (FP32).
+// real mesh, for meshes of up to 64 points per axis (FP32).
 //
 // Each CG iteration of the induced-dipole solve convolves the spread dipole mesh with the
 // Coulomb influence function G(k) = C(k^2) / |theta(k)|^2 (recip.py:440-466; the reference runs a
@@ -15,8 +15,9 @@
 //           packed as A + i B, inverse FFT along z, the two real rows out.
 // Transforms are unnormalised in both directions (the cuFFT convention the gather expects).
 //
-// Line FFTs: Stockham autosort over the factors of the line length (radices 4, 2, 3, 5, 7; meshes
-// with another prime factor take cuFFT), one radix-R butterfly per thread and stage: inputs
+// Line FFTs: Stockham autosort over the factors of the line length (radices 4, 2, 3, 5, 7, then a
+// remaining prime as one generic stage of O(R) work per output), one radix-R butterfly per thread
+// and stage for the hard-coded radices: inputs
 // x[j + t N / R] times the stage twiddles W_{Ns R}^{t k} (k = j mod Ns, precomputed per stage in
 // shared memory, conjugated for the inverse), a hard-coded R-point DFT, outputs to
 // y[(j - k) R + k + u Ns].
@@ -51,32 +52,37 @@ struct FftConvArgs {
     float2 tw[3][kFcTw];           // stage twiddles of the x, y and z line lengths
 };
 
-// radices 4, 2, 3, 5, 7 in that order; ok = false when another prime factor remains (such meshes
-// take the cuFFT path)
+// radices 4, 2, 3, 5, 7 in that order, then the remaining factor (a prime above 7, n <= 64) as one
+// generic stage; ok = false when n is out of range
 __host__ inline FcPlan fc_plan(int n, bool* ok = nullptr) {
     FcPlan p;
     p.n = n;
     p.nf = 0;
     int m = n;
     for (int r : {4, 2, 3, 5, 7}) {
-        while (m % r == 0 && p.nf < kFcMaxFactors) {
+        while (m % r == 0 && p.nf < kFcMaxFactors - 1) {
             p.f[p.nf++] = r;
             m /= r;
         }
     }
-    if (ok) *ok = (m == 1);
+    if (m > 1) p.f[p.nf++] = m;
+    if (ok) *ok = n >= 2 && n <= kFcMaxK;
     return p;
 }
 
-// stage twiddles of a line length: W_{Ns R}^{t k} of stage s (span Ns, radix R) at off_s + k R + t,
-// off_s the sum of Ns R over the earlier stages (< 2 n in all); FP64 on the host rounded to FP32
+__host__ __device__ inline bool fc_hardcoded(int R) { return R == 2 || R == 3 || R == 4 || R == 5 || R == 7; }
+
+// stage twiddles of a line length, Ns R entries per stage (span Ns, radix R) at off_s (the sum of
+// Ns R over the earlier stages, < 2 n in all): W_{Ns R}^{t k} at off_s + k R + t for a hard-coded
+// radix, W_{Ns R}^m at off_s + m for the generic stage; FP64 on the host rounded to FP32
 __host__ inline void fc_host_twiddles(const FcPlan& p, float2* tw) {
     int ns = 1, off = 0;
     for (int s = 0; s < p.nf; ++s) {
         const int R = p.f[s];
         for (int e = 0; e < ns * R; ++e) {
             const int k = e / R, t = e % R;
-            const double ang = -2.0 * 3.14159265358979323846 * (double)(t * k) / (double)(ns * R);
+            const int m = fc_hardcoded(R) ? t * k : e;
+            const double ang = -2.0 * 3.14159265358979323846 * (double)m / (double)(ns * R);
             tw[off + e] = make_float2((float)std::cos(ang), (float)std::sin(ang));
         }
         off += ns * R;
@@ -198,6 +204,41 @@ __device__ inline void fc_stage(const float2* in, float2* out, int ls, int es, i
     }
 }
 
+// the generic stage (radix R not hard-coded, a prime above 7): one output per thread,
+//     y[(j - k) R + k + u Ns] = sum_t x[j + t N / R] W_{Ns R}^{t (k + u Ns)},  k = j mod Ns,
+// with W_{Ns R}^m read from the stage's table (conjugated for the inverse)
+__device__ inline void fc_stage_generic(const float2* in, float2* out, int ls, int es, int nl, int N, int Ns, int R,
+                                        const float2* tw, bool inv, int tid, int nth) {
+    const int nb = N / R, span = Ns * R;
+    const bool line_fast = ls < es;
+    const float rnl = 1.f / (float)nl, rn = 1.f / (float)N, rnb = 1.f / (float)nb, rns = 1.f / (float)Ns;
+    for (int e = tid; e < nl * N; e += nth) {
+        int l, o;
+        if (line_fast) {
+            o = fc_div(e, rnl);
+            l = e - o * nl;
+        } else {
+            l = fc_div(e, rn);
+            o = e - l * N;
+        }
+        const int u = fc_div(o, rnb), j = o - u * nb;
+        const int k = j - fc_div(j, rns) * Ns;
+        const int m = k + u * Ns;
+        float2 acc = make_float2(0.f, 0.f);
+        int idx = 0;
+        for (int t = 0; t < R; ++t) {
+            const float2 v = in[l * ls + (j + t * nb) * es];
+            float2 w = tw[idx];
+            if (inv) w.y = -w.y;
+            acc.x += v.x * w.x - v.y * w.y;
+            acc.y += v.x * w.y + v.y * w.x;
+            idx += m;
+            if (idx >= span) idx -= span;
+        }
+        out[l * ls + ((j - k) * R + k + u * Ns) * es] = acc;
+    }
+}
+
 // nl lines of length p.n, line l at base[l * ls] with element stride es, transformed in place
 // through scratch scr of the same layout; inverse = conjugate twiddles, unnormalised.  Ends with
 // a barrier.
@@ -214,7 +255,8 @@ __device__ inline void fc_lines(const FcPlan& p, float2* base, int nl, int ls, i
             case 3: fc_stage<3>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
             case 4: fc_stage<4>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
             case 5: fc_stage<5>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
-            default: fc_stage<7>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            case 7: fc_stage<7>(in, out, ls, es, nl, N, Ns, tw + off, inverse, tid, nth); break;
+            default: fc_stage_generic(in, out, ls, es, nl, N, Ns, R, tw + off, inverse, tid, nth); break;
         }
         __syncthreads();
         off += Ns * R;
@@ -237,82 +279,75 @@ __device__ inline void fc_lines(const FcPlan& p, float2* base, int nl, int ls, i
     }
 }
 
-// shared memory of the plane kernels: rows [ceil(K2/2)][K3] (also the scratch of the y lines) +
-// the z scratch of the same size + the plane [K2][Kh] + stage twiddles of the two line lengths
-__host__ inline size_t fc_plane_smem(const int K[3]) {
-    const int np = (K[1] + 1) / 2, Kh = K[2] / 2 + 1;
-    size_t rows = (size_t)np * K[2];
-    if (rows < (size_t)K[1] * Kh) rows = (size_t)K[1] * Kh;  // the rows region is the y scratch too
-    return (2 * rows + (size_t)K[1] * Kh + 2 * kFcTw) * sizeof(float2);
+// Shared memory of one plane pass (plane_smem_layout): rows [ceil(K2/2)][K3] (also the scratch of the
+// y lines), the z scratch of the same size and the plane [K2][Kh].
+struct FcPlaneSmem {
+    float2 *rows, *scr, *plane;
+};
+
+__device__ inline FcPlaneSmem fc_plane_layout(const FftConvArgs& a, float2* sm) {
+    const int K2 = a.K[1], K3 = a.K[2], Kh = a.Kh;
+    size_t rsz = (size_t)((K2 + 1) / 2) * K3;
+    if (rsz < (size_t)K2 * Kh) rsz = (size_t)K2 * Kh;
+    FcPlaneSmem m;
+    m.rows = sm;
+    m.scr = sm + rsz;
+    m.plane = sm + 2 * rsz;
+    return m;
 }
 
-// shared memory of the column kernel: kFcCols columns of K1 + scratch + x twiddles
-__host__ inline size_t fc_col_smem(const int K[3]) {
-    return ((size_t)2 * kFcCols * K[0] + kFcTw) * sizeof(float2);
-}
-
-// Forward pass over one x-plane per CTA: rows y = 2p, 2p + 1 of the real plane packed as one
+// Forward pass of x-plane x by one CTA: rows y = 2p, 2p + 1 of the real plane packed as one
 // complex row (a + i b), FFT along z, the two half spectra separated
 // (A = (C_k + conj C_{-k}) / 2, B = (C_k - conj C_{-k}) / 2i), FFT along y of the [K2][Kh] half
-// plane, written to the spectrum W[x][ky][kz]; the spread mesh plane is cleared for the next spread.
-__global__ void __launch_bounds__(kFcPlaneThreads) k_fc_fwd_planes(FftConvArgs a) {
-    extern __shared__ float2 sm[];
+// plane, written to the spectrum W[x][ky][kz]; the spread mesh plane is cleared for the next
+// spread.  Mesh and spectrum are read with coherent loads (a persistent caller writes them in the
+// same launch).  Ends with a barrier of the CTA.
+__device__ inline void fc_fwd_plane(const FftConvArgs& a, int x, float2* sm, const float2* twy, const float2* twz) {
     const int K2 = a.K[1], K3 = a.K[2], Kh = a.Kh;
     const int np = (K2 + 1) / 2;
-    const int x = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
-    size_t rsz = (size_t)np * K3;
-    if (rsz < (size_t)K2 * Kh) rsz = (size_t)K2 * Kh;
-    float2* rows = sm;
-    float2* scr = rows + rsz;
-    float2* plane = scr + rsz;
-    float2* twy = plane + (size_t)K2 * Kh;
-    float2* twz = twy + kFcTw;
-    fc_load_twiddles(twy, a.tw[1], tid, nth);
-    fc_load_twiddles(twz, a.tw[2], tid, nth);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const FcPlaneSmem m = fc_plane_layout(a, sm);
     float* gin = a.grid_in + (size_t)x * K2 * K3;
     const float rk3 = 1.f / (float)K3, rkh = 1.f / (float)Kh;
 #pragma unroll 4
     for (int e = tid; e < np * K3; e += nth) {
         const int p = fc_div(e, rk3), z = e - p * K3;
         const int y1 = 2 * p + 1;
-        const float re = __ldg(gin + (2 * p) * K3 + z);
-        const float im = y1 < K2 ? __ldg(gin + y1 * K3 + z) : 0.f;
-        rows[e] = make_float2(re, im);
+        const float re = gin[(2 * p) * K3 + z];
+        const float im = y1 < K2 ? gin[y1 * K3 + z] : 0.f;
+        m.rows[e] = make_float2(re, im);
     }
     __syncthreads();
     // the next spread starts from zero (this CTA has read its plane)
     for (int e = tid; e < K2 * K3; e += nth) gin[e] = 0.f;
-    fc_lines(a.pz, rows, np, K3, 1, scr, twz, false, tid, nth);
+    fc_lines(a.pz, m.rows, np, K3, 1, m.scr, twz, false, tid, nth);
     for (int e = tid; e < K2 * Kh; e += nth) {
         const int y = fc_div(e, rkh), kz = e - y * Kh;
-        const float2* r = rows + (size_t)(y >> 1) * K3;
-        const float2 c = r[kz], m = r[kz == 0 ? 0 : K3 - kz];  // C_k and C_{-k}
+        const float2* r = m.rows + (size_t)(y >> 1) * K3;
+        const float2 c = r[kz], mm = r[kz == 0 ? 0 : K3 - kz];  // C_k and C_{-k}
         // even row: (C_k + conj C_-k) / 2; odd row: (C_k - conj C_-k) / 2i
-        plane[e] = (y & 1) ? make_float2(0.5f * (c.y + m.y), 0.5f * (m.x - c.x))
-                           : make_float2(0.5f * (c.x + m.x), 0.5f * (c.y - m.y));
+        m.plane[e] = (y & 1) ? make_float2(0.5f * (c.y + mm.y), 0.5f * (mm.x - c.x))
+                             : make_float2(0.5f * (c.x + mm.x), 0.5f * (c.y - mm.y));
     }
     __syncthreads();
-    fc_lines(a.py, plane, Kh, 1, Kh, rows, twy, false, tid, nth);
+    fc_lines(a.py, m.plane, Kh, 1, Kh, m.rows, twy, false, tid, nth);
     float2* w = a.spec + (size_t)x * K2 * Kh;
-    for (int e = tid; e < K2 * Kh; e += nth) w[e] = plane[e];
+    for (int e = tid; e < K2 * Kh; e += nth) w[e] = m.plane[e];
+    __syncthreads();
 }
 
-// Columns (ky, kz) of the spectrum, kFcCols per CTA: FFT along x, times the influence function,
-// inverse FFT along x, in place.
-__global__ void __launch_bounds__(kFcColThreads) k_fc_columns(FftConvArgs a) {
-    extern __shared__ float2 sm[];
+// Columns (ky, kz) = c0 .. c0 + kFcCols - 1 of the spectrum by one CTA: FFT along x, times the
+// influence function, inverse FFT along x, in place.  Ends with a barrier of the CTA.
+__device__ inline void fc_column_block(const FftConvArgs& a, int c0, float2* sm, const float2* twx) {
     const int K1 = a.K[0], ncol = a.K[1] * a.Kh;
-    const int c0 = blockIdx.x * kFcCols, tid = threadIdx.x, nth = blockDim.x;
+    const int tid = threadIdx.x, nth = blockDim.x;
     const int nc = min(kFcCols, ncol - c0);
     float2* col = sm;  // [K1][kFcCols]: line q at col + q, element stride kFcCols
     float2* scr = col + (size_t)kFcCols * K1;
-    float2* twx = scr + (size_t)kFcCols * K1;
-    fc_load_twiddles(twx, a.tw[0], tid, nth);
-    const float2* spec = a.spec;
 #pragma unroll 4
     for (int e = tid; e < K1 * kFcCols; e += nth) {
         const int x = e / kFcCols, q = e - x * kFcCols;
-        col[e] = q < nc ? __ldg(spec + (size_t)x * ncol + c0 + q) : make_float2(0.f, 0.f);
+        col[e] = q < nc ? a.spec[(size_t)x * ncol + c0 + q] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     fc_lines(a.px, col, nc, 1, kFcCols, scr, twx, false, tid, nth);
@@ -330,31 +365,23 @@ __global__ void __launch_bounds__(kFcColThreads) k_fc_columns(FftConvArgs a) {
         const int x = e / kFcCols, q = e - x * kFcCols;
         if (q < nc) a.spec[(size_t)x * ncol + c0 + q] = col[e];
     }
+    __syncthreads();
 }
 
-// Inverse pass over one x-plane per CTA: inverse FFT along y, the half spectra of rows 2p and
+// Inverse pass of x-plane x by one CTA: inverse FFT along y, the half spectra of rows 2p and
 // 2p + 1 completed Hermitian (imaginary parts of kz = 0 and kz = K3 / 2 dropped, as a complex-to-
 // real transform does) and packed as A + i B, inverse FFT along z, real and imaginary parts out as
-// the two real rows.
-__global__ void __launch_bounds__(kFcPlaneThreads) k_fc_inv_planes(FftConvArgs a) {
-    extern __shared__ float2 sm[];
+// the two real rows.  Ends with a barrier of the CTA.
+__device__ inline void fc_inv_plane(const FftConvArgs& a, int x, float2* sm, const float2* twy, const float2* twz) {
     const int K2 = a.K[1], K3 = a.K[2], Kh = a.Kh;
     const int np = (K2 + 1) / 2;
-    const int x = blockIdx.x, tid = threadIdx.x, nth = blockDim.x;
-    size_t rsz = (size_t)np * K3;
-    if (rsz < (size_t)K2 * Kh) rsz = (size_t)K2 * Kh;
-    float2* rows = sm;
-    float2* scr = rows + rsz;
-    float2* plane = scr + rsz;
-    float2* twy = plane + (size_t)K2 * Kh;
-    float2* twz = twy + kFcTw;
-    fc_load_twiddles(twy, a.tw[1], tid, nth);
-    fc_load_twiddles(twz, a.tw[2], tid, nth);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const FcPlaneSmem m = fc_plane_layout(a, sm);
     const float2* w = a.spec + (size_t)x * K2 * Kh;
 #pragma unroll 4
-    for (int e = tid; e < K2 * Kh; e += nth) plane[e] = __ldg(w + e);
+    for (int e = tid; e < K2 * Kh; e += nth) m.plane[e] = w[e];
     __syncthreads();
-    fc_lines(a.py, plane, Kh, 1, Kh, rows, twy, true, tid, nth);
+    fc_lines(a.py, m.plane, Kh, 1, Kh, m.rows, twy, true, tid, nth);
     const bool even = (K3 % 2) == 0;
     const float rk3 = 1.f / (float)K3;
     for (int e = tid; e < np * K3; e += nth) {
@@ -362,8 +389,8 @@ __global__ void __launch_bounds__(kFcPlaneThreads) k_fc_inv_planes(FftConvArgs a
         const int y0 = 2 * p, y1 = 2 * p + 1;
         const bool lo = z < Kh;
         const int zz = lo ? z : K3 - z;
-        float2 A = plane[y0 * Kh + zz];
-        float2 B = y1 < K2 ? plane[y1 * Kh + zz] : make_float2(0.f, 0.f);
+        float2 A = m.plane[y0 * Kh + zz];
+        float2 B = y1 < K2 ? m.plane[y1 * Kh + zz] : make_float2(0.f, 0.f);
         if (z == 0 || (even && z == K3 / 2)) {
             A.y = 0.f;
             B.y = 0.f;
@@ -372,17 +399,61 @@ __global__ void __launch_bounds__(kFcPlaneThreads) k_fc_inv_planes(FftConvArgs a
             A.y = -A.y;
             B.y = -B.y;
         }
-        rows[e] = make_float2(A.x - B.y, A.y + B.x);  // A + i B
+        m.rows[e] = make_float2(A.x - B.y, A.y + B.x);  // A + i B
     }
     __syncthreads();
-    fc_lines(a.pz, rows, np, K3, 1, scr, twz, true, tid, nth);
+    fc_lines(a.pz, m.rows, np, K3, 1, m.scr, twz, true, tid, nth);
     float* gout = a.grid_out + (size_t)x * K2 * K3;
     for (int e = tid; e < np * K3; e += nth) {
         const int p = fc_div(e, rk3), z = e - p * K3;
-        const float2 v = rows[e];
+        const float2 v = m.rows[e];
         gout[(2 * p) * K3 + z] = v.x;
         if (2 * p + 1 < K2) gout[(2 * p + 1) * K3 + z] = v.y;
     }
+    __syncthreads();
+}
+
+// bytes of the plane-pass working area (fc_plane_layout)
+__host__ __device__ inline size_t fc_plane_work(const int K[3]) {
+    const int np = (K[1] + 1) / 2, Kh = K[2] / 2 + 1;
+    size_t rows = (size_t)np * K[2];
+    if (rows < (size_t)K[1] * Kh) rows = (size_t)K[1] * Kh;
+    return (2 * rows + (size_t)K[1] * Kh) * sizeof(float2);
+}
+
+// bytes of the column-pass working area
+__host__ __device__ inline size_t fc_col_work(const int K[3]) { return (size_t)2 * kFcCols * K[0] * sizeof(float2); }
+
+// shared memory of the stand-alone kernels: working area + the stage twiddles they use
+__host__ inline size_t fc_plane_smem(const int K[3]) { return fc_plane_work(K) + 2 * kFcTw * sizeof(float2); }
+__host__ inline size_t fc_col_smem(const int K[3]) { return fc_col_work(K) + kFcTw * sizeof(float2); }
+
+__global__ void __launch_bounds__(kFcPlaneThreads) k_fc_fwd_planes(FftConvArgs a) {
+    extern __shared__ float2 sm[];
+    float2* twy = sm + fc_plane_work(a.K) / sizeof(float2);
+    float2* twz = twy + kFcTw;
+    fc_load_twiddles(twy, a.tw[1], threadIdx.x, blockDim.x);
+    fc_load_twiddles(twz, a.tw[2], threadIdx.x, blockDim.x);
+    __syncthreads();
+    fc_fwd_plane(a, blockIdx.x, sm, twy, twz);
+}
+
+__global__ void __launch_bounds__(kFcColThreads) k_fc_columns(FftConvArgs a) {
+    extern __shared__ float2 sm[];
+    float2* twx = sm + fc_col_work(a.K) / sizeof(float2);
+    fc_load_twiddles(twx, a.tw[0], threadIdx.x, blockDim.x);
+    __syncthreads();
+    fc_column_block(a, blockIdx.x * kFcCols, sm, twx);
+}
+
+__global__ void __launch_bounds__(kFcPlaneThreads) k_fc_inv_planes(FftConvArgs a) {
+    extern __shared__ float2 sm[];
+    float2* twy = sm + fc_plane_work(a.K) / sizeof(float2);
+    float2* twz = twy + kFcTw;
+    fc_load_twiddles(twy, a.tw[1], threadIdx.x, blockDim.x);
+    fc_load_twiddles(twz, a.tw[2], threadIdx.x, blockDim.x);
+    __syncthreads();
+    fc_inv_plane(a, blockIdx.x, sm, twy, twz);
 }
 
 // influence function table over the half spectrum (the multiplier of k_conv for Coulomb, k = 0

@@ -876,19 +876,14 @@ __global__ void __launch_bounds__(256) k_matvec_coef(PairArgs<T> a, CsrArgs c, M
 }
 
 // The CG matvec streams 12 bytes per CSR entry (packed j + two coefficients); the pair
-// direction z is recomputed from the positions, which like U stay cache-resident.  With dot_out,
-// sum_i U_i . out_i is reduced into *dot_out.
+// direction z is recomputed from the positions, which like U stay cache-resident.  One warp per
+// atom i: out_i = sum_j A_ij U_j; returns U_i . out_i in lane 0 (0 elsewhere).
 template <typename T>
-__global__ void __launch_bounds__(256) k_matvec_apply(CsrArgs c, const MvCoef<T>* coef, const T* pos4, BoxT<T> bx,
-                                                      const double* U, double* out, double* dot_out = nullptr) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const bool active = w < c.n;
-    if (!active && !dot_out) return;
-    const int i = active ? w : 0;
+__device__ __forceinline__ double matvec_atom(const CsrArgs& c, const MvCoef<T>* coef, const T* pos4,
+                                              const BoxT<T>& bx, const double* U, double* out, int i, int lane) {
     const T xi = pos4[4 * i], yi = pos4[4 * i + 1], zi = pos4[4 * i + 2];
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    const int64_t beg = active ? c.off[i] : 0, end = active ? c.off[i + 1] : 0;
+    const int64_t beg = c.off[i], end = c.off[i + 1];
     for (int64_t k = beg + lane; k < end; k += 32) {
         const int j = c.ent[k] & 0x0FFFFFFF;
         const MvCoef<T> cf = coef[k];
@@ -906,13 +901,23 @@ __global__ void __launch_bounds__(256) k_matvec_apply(CsrArgs c, const MvCoef<T>
     acc0 = warp_sum(acc0);
     acc1 = warp_sum(acc1);
     acc2 = warp_sum(acc2);
+    if (lane != 0) return 0.0;
+    out[3 * i] = acc0;
+    out[3 * i + 1] = acc1;
+    out[3 * i + 2] = acc2;
+    return U[3 * i] * acc0 + U[3 * i + 1] * acc1 + U[3 * i + 2] * acc2;
+}
+
+// With dot_out, sum_i U_i . out_i is reduced into *dot_out.
+template <typename T>
+__global__ void __launch_bounds__(256) k_matvec_apply(CsrArgs c, const MvCoef<T>* coef, const T* pos4, BoxT<T> bx,
+                                                      const double* U, double* out, double* dot_out = nullptr) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const bool active = w < c.n;
+    if (!active && !dot_out) return;
     double d[1] = {0.0};
-    if (active && lane == 0) {
-        out[3 * i] = acc0;
-        out[3 * i + 1] = acc1;
-        out[3 * i + 2] = acc2;
-        if (dot_out) d[0] = U[3 * i] * acc0 + U[3 * i + 1] * acc1 + U[3 * i + 2] * acc2;
-    }
+    if (active) d[0] = matvec_atom<T>(c, coef, pos4, bx, U, out, w, lane);
     if (dot_out) block_reduce_add<1>(d, dot_out);
 }
 

@@ -644,11 +644,8 @@ __global__ void __launch_bounds__(256) k_stencil_prep(int n, const double* pos, 
 // passes, so a warp's atomics of one pass touch five runs of six consecutive floats (coalesced in
 // L2) instead of 32 scattered addresses.
 template <typename T>
-__global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, StencilCache<T> st) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
-    if (warp >= a.n) return;  // whole warps: every lane below takes part in the shuffles
+__device__ __forceinline__ void spread_dip_atom(const SpreadArgs<T>& a, const StencilCache<T>& st, int warp,
+                                                int lane) {
     const int at = (int)(((int64_t)warp * a.perm_mul) % a.n);
     const T mu0 = (T)a.U[3 * at], mu1 = (T)a.U[3 * at + 1], mu2 = (T)a.U[3 * at + 2];
     const int grp = lane / 6, iz = lane - 6 * grp;
@@ -687,6 +684,15 @@ __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, Sten
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, StencilCache<T> st) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
+    if (warp >= a.n) return;  // whole warps: every lane takes part in the shuffles
+    spread_dip_atom<T>(a, st, warp, lane);
+}
+
 // Field terms folded into the gather: out = recip [+ mv] [+ (1/pol + self1) U]; with dot_out,
 // sum U . out is reduced into *dot_out; *zero1 is cleared by thread 0 of block 0.
 struct FieldCombine {
@@ -700,72 +706,75 @@ struct FieldCombine {
 
 // k_gather_field with the cached stencil: lanes own whole (x, y) columns (lanes 0..31, then
 // lanes 0..3) and read the column's six z points in sequence (one or two sectors, L1 hits after
-// the first), contracting them with the warp-uniform z weights.
+// the first), contracting them with the warp-uniform z weights.  One warp per atom; returns
+// U_at . out_at in lane 0 when cmb.dot_out is set (0 elsewhere).
+template <typename T>
+__device__ __forceinline__ double gather_field_atom(const StencilCache<T>& st, const MeshGeom& g, const T* phi,
+                                                    double scale, double* out, const FieldCombine& cmb, int at,
+                                                    int lane) {
+    T p1 = T(0), p2 = T(0), p3 = T(0);
+    const int4 o = st.org[at];
+    const T* w = st.w + 36 * (size_t)at;
+    const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
+    T mz0[6], mz1[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        mz0[t] = __ldg(w + 24 + t);
+        mz1[t] = __ldg(w + 30 + t);
+    }
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+        const int L = lane + 32 * pass;
+        if (L < 36) {
+            const int ix = L / 6, iy = L - 6 * ix;
+            const int gx = wrap_up(o.x + ix, K0), gy = wrap_up(o.y + iy, K1);
+            const T* line = phi + ((size_t)gx * K1 + gy) * K2;
+            int gz = o.z;
+            T s0 = T(0), s1 = T(0);
+#pragma unroll
+            for (int t = 0; t < 6; ++t) {
+                const T v = line[gz];
+                s0 += v * mz0[t];
+                s1 += v * mz1[t];
+                gz = (gz + 1 == K2) ? 0 : gz + 1;
+            }
+            const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy), my1 = __ldg(w + 18 + iy);
+            p1 += mx1 * my0 * s0;
+            p2 += mx0 * my1 * s0;
+            p3 += mx0 * my0 * s1;
+        }
+    }
+    p1 = warp_sum(p1);
+    p2 = warp_sum(p2);
+    p3 = warp_sum(p3);
+    if (lane != 0) return 0.0;
+    const double* B = g.B;
+    const double P1 = scale * (double)p1, P2 = scale * (double)p2, P3 = scale * (double)p3;
+    double pp = 0.0, d = 0.0;
+    if (cmb.U) {
+        pp = cmb.pol[at];
+        pp = pp < 1e-8 ? 1e-8 : pp;
+        pp = DMFFB_DIELECTRIC / pp + cmb.self1;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double v = -(P1 * B[c] + P2 * B[3 + c] + P3 * B[6 + c]);
+        if (cmb.mv) v += cmb.mv[3 * at + c];
+        if (cmb.U) v += pp * cmb.U[3 * at + c];
+        out[3 * at + c] = v;
+        if (cmb.dot_out) d += cmb.U[3 * at + c] * v;
+    }
+    return d;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache<T> st, MeshGeom g, const T* phi,
                                                              double scale, double* out, FieldCombine cmb) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x == 0 && cmb.zero1) *cmb.zero1 = 0.0;
-    const bool active = warp < n;
-    const int at = active ? warp : 0;
-    T p1 = T(0), p2 = T(0), p3 = T(0);
-    if (active) {
-        const int4 o = st.org[at];
-        const T* w = st.w + 36 * (size_t)at;
-        const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
-        T mz0[6], mz1[6];
-#pragma unroll
-        for (int t = 0; t < 6; ++t) {
-            mz0[t] = __ldg(w + 24 + t);
-            mz1[t] = __ldg(w + 30 + t);
-        }
-#pragma unroll
-        for (int pass = 0; pass < 2; ++pass) {
-            const int L = lane + 32 * pass;
-            if (L < 36) {
-                const int ix = L / 6, iy = L - 6 * ix;
-                const int gx = wrap_up(o.x + ix, K0), gy = wrap_up(o.y + iy, K1);
-                const T* line = phi + ((size_t)gx * K1 + gy) * K2;
-                int gz = o.z;
-                T s0 = T(0), s1 = T(0);
-#pragma unroll
-                for (int t = 0; t < 6; ++t) {
-                    const T v = __ldg(line + gz);
-                    s0 += v * mz0[t];
-                    s1 += v * mz1[t];
-                    gz = (gz + 1 == K2) ? 0 : gz + 1;
-                }
-                const T mx0 = __ldg(w + ix), mx1 = __ldg(w + 6 + ix), my0 = __ldg(w + 12 + iy),
-                        my1 = __ldg(w + 18 + iy);
-                p1 += mx1 * my0 * s0;
-                p2 += mx0 * my1 * s0;
-                p3 += mx0 * my0 * s1;
-            }
-        }
-    }
-    p1 = warp_sum(p1);
-    p2 = warp_sum(p2);
-    p3 = warp_sum(p3);
     double d[1] = {0.0};
-    if (active && lane == 0) {
-        const double* B = g.B;
-        const double P1 = scale * (double)p1, P2 = scale * (double)p2, P3 = scale * (double)p3;
-        double pp = 0.0;
-        if (cmb.U) {
-            pp = cmb.pol[at];
-            pp = pp < 1e-8 ? 1e-8 : pp;
-            pp = DMFFB_DIELECTRIC / pp + cmb.self1;
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            double v = -(P1 * B[c] + P2 * B[3 + c] + P3 * B[6 + c]);
-            if (cmb.mv) v += cmb.mv[3 * at + c];
-            if (cmb.U) v += pp * cmb.U[3 * at + c];
-            out[3 * at + c] = v;
-            if (cmb.dot_out) d[0] += cmb.U[3 * at + c] * v;
-        }
-    }
+    if (warp < n) d[0] = gather_field_atom<T>(st, g, phi, scale, out, cmb, warp, lane);
     if (cmb.dot_out) block_reduce_add<1>(d, cmb.dot_out);
 }
 

@@ -24,6 +24,7 @@
 #include "classical.cuh"
 #include "nbcells.cuh"
 #include "admp_fftconv.cuh"
+#include "admp_cgsolve.cuh"
 #include "pairwise.cuh"
 
 using namespace dmffb;
@@ -151,6 +152,13 @@ struct dmffb_engine {
     bool fc_enabled = false;  // dmffb_set_fused_fft
     int fc_ok = -1;          // the engine's FFT convolution serves this mesh (1), not (0), not decided (-1)
     float2* d_fcW = nullptr;  // [K1][K2][K3/2+1] half spectrum between its passes
+    int pcg_mode = 2;         // dmffb_set_persistent_cg: 0 off, 1 on, 2 for systems of at most pcg_auto_atoms
+    int pcg_auto_atoms = 4096;
+    int pcg_max_blocks = -1;  // co-resident k_cg_solve CTAs for the current mesh (0: unavailable, -1: not decided)
+    void* d_pcg = nullptr;    // persistent solve scalars, barrier words and status
+    double pcg_wait_s = 2.0;  // limit of one grid-barrier wait
+    int pcg_phantom = 0;      // arrivals the next persistent solve's barrier waits for beyond its CTAs (tests)
+    double pcg_phase_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // pass times of the persistent solves run while profiling
     float* d_fcG = nullptr;  // [K1*K2*Kh] influence function of the half spectrum
     int64_t fcG_cap = 0;
     int32_t* d_covrows = nullptr;  // [n_covrows*3] covalent rows (i < j, nbond)
@@ -296,6 +304,7 @@ enum { KC_PREP = 0, KC_PAIR_FULL, KC_PAIR_FIELD, KC_PAIR_MATVEC, KC_SPREAD, KC_F
        // FP64 launches over the topologically scaled rows, parameter-adjoint pair kernels, bonded terms
        KC_PAIR_FULL_SCALED, KC_PAIR_FIELD_SCALED, KC_PGRAD, KC_BONDED,
        KC_FFTCONV,  // the dipole solve's forward FFT + influence multiply + inverse FFT (engine FFT)
+       KC_CGSOLVE,  // the whole CG solve in one persistent cooperative launch
        KC_COUNT };
 static_assert(KC_COUNT <= 32, "kernel-class statistics arrays hold 32 classes");
 
@@ -533,22 +542,35 @@ int lmax_eff(const dmffb_engine* h) { return (h->lmax == 0 && h->lpol) ? 1 : h->
 // reciprocal pass: spread (Qg and/or U) -> FFT -> convolution -> inverse FFT -> gather
 // per-atom wrapped stencil origins and spline weights at these positions, for the cached dipole
 // spread and field gather of the dipole solve
-// Whether the engine's FFT convolution serves the current mesh: FP32, 7-smooth extents of at most
-// 64 points and the kernels' shared memory granted; otherwise the cuFFT path runs.
+// The dynamic shared memory limit of a kernel is a property of the function, shared by every
+// engine of the process (and by the server's slot threads): it is set to what the largest mesh
+// served (64 points per axis) needs, the same value from every caller, never to one engine's own
+// need, which another engine's smaller setting would undercut at its next launch.
+const int kFcMaxMesh[3] = {kFcMaxK, kFcMaxK, kFcMaxK};
+
+bool fc_grant_smem() {
+    return cudaFuncSetAttribute(k_fc_fwd_planes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fc_plane_smem(kFcMaxMesh)) == cudaSuccess &&
+           cudaFuncSetAttribute(k_fc_inv_planes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fc_plane_smem(kFcMaxMesh)) == cudaSuccess &&
+           cudaFuncSetAttribute(k_fc_columns, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fc_col_smem(kFcMaxMesh)) == cudaSuccess &&
+           cudaFuncSetAttribute(k_cg_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)cg_solve_smem(kFcMaxMesh)) == cudaSuccess;
+}
+
+// Whether the engine's FFT convolution serves the current mesh: FP32, extents of at most 64 points
+// and the kernels' shared memory granted; otherwise the cuFFT path runs.
 int fc_decide(dmffb_engine* h) {
     if (h->fc_ok >= 0) return h->fc_ok;
     h->fc_ok = 0;
     if (h->prec != DMFFB_FP32 || !h->lpme) return 0;
     for (int k = 0; k < 3; ++k) {
-        bool smooth = false;
-        fc_plan(h->K[k], &smooth);
-        if (h->K[k] < 2 || h->K[k] > kFcMaxK || !smooth) return 0;
+        bool ok = false;
+        fc_plan(h->K[k], &ok);
+        if (!ok) return 0;
     }
-    const size_t sp = fc_plane_smem(h->K), sc = fc_col_smem(h->K);
-    if (sp > 227 * 1024 || sc > 227 * 1024) return 0;
-    if (cudaFuncSetAttribute(k_fc_fwd_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp) != cudaSuccess ||
-        cudaFuncSetAttribute(k_fc_inv_planes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sp) != cudaSuccess ||
-        cudaFuncSetAttribute(k_fc_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc) != cudaSuccess) {
+    if (!fc_grant_smem()) {
         cudaGetLastError();
         return 0;
     }
@@ -577,8 +599,7 @@ int fc_prepare(dmffb_engine* h, cudaStream_t s, const Box& bx) {
     return DMFFB_OK;
 }
 
-int fc_launch(dmffb_engine* h, cudaStream_t s, float* in, float* out) {
-    static_assert(sizeof(FftConvArgs) <= 4000, "launch arguments of the FFT convolution");
+FftConvArgs fc_args(dmffb_engine* h, float* in, float* out) {
     FftConvArgs a = {};
     for (int k = 0; k < 3; ++k) a.K[k] = h->K[k];
     a.Kh = h->K[2] / 2 + 1;
@@ -592,6 +613,12 @@ int fc_launch(dmffb_engine* h, cudaStream_t s, float* in, float* out) {
     fc_host_twiddles(a.px, a.tw[0]);
     fc_host_twiddles(a.py, a.tw[1]);
     fc_host_twiddles(a.pz, a.tw[2]);
+    return a;
+}
+
+int fc_launch(dmffb_engine* h, cudaStream_t s, float* in, float* out) {
+    static_assert(sizeof(FftConvArgs) <= 4000, "launch arguments of the FFT convolution");
+    FftConvArgs a = fc_args(h, in, out);
     const size_t sp = fc_plane_smem(h->K), sc = fc_col_smem(h->K);
     const int ncb = (h->K[1] * a.Kh + kFcCols - 1) / kFcCols;
     LAUNCH(h, s, KC_FFTCONV, k_fc_fwd_planes<<<h->K[0], kFcPlaneThreads, sp, s>>>(a));
@@ -600,6 +627,34 @@ int fc_launch(dmffb_engine* h, cudaStream_t s, float* in, float* out) {
     CK(cudaGetLastError());
     return DMFFB_OK;
 }
+
+// Co-resident CTAs of the persistent CG solve for the current mesh (0: the graph-replayed solve
+// runs instead): needs the engine-FFT convolution for the mesh, the kernel's shared memory and a
+// device that takes cooperative launches.
+bool pcg_wanted(const dmffb_engine* h) {
+    return h->pcg_mode == 1 || (h->pcg_mode == 2 && h->n <= h->pcg_auto_atoms);
+}
+
+int pcg_decide(dmffb_engine* h) {
+    if (h->pcg_max_blocks >= 0) return h->pcg_max_blocks;
+    h->pcg_max_blocks = 0;
+    if (fc_decide(h) <= 0) return 0;
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const size_t smem = cg_solve_smem(h->K);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cg_solve, kCgThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    h->pcg_max_blocks = per_sm * nsm;
+    return h->pcg_max_blocks;
+}
+
 
 template <typename T>
 int stencil_prep(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx) {
@@ -616,7 +671,9 @@ int stencil_prep(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& 
     }
     LAUNCH(h, s, KC_VEC, k_stencil_prep<T><<<nblk(n, 128), 128, 0, s>>>(n, pos, mesh_geom(bx, h->K), h->d_stc_org,
                                                                         (T*)h->d_stc_w));
-    if (sizeof(T) == 4 && h->fc_enabled && fc_decide(h) > 0 && (st = fc_prepare(h, s, bx))) return st;
+    if (sizeof(T) == 4 && (h->fc_enabled || (pcg_wanted(h) && pcg_decide(h) > 0)) && fc_decide(h) > 0 &&
+        (st = fc_prepare(h, s, bx)))
+        return st;
     h->stencils_ready = true;
     return DMFFB_OK;
 }
@@ -938,6 +995,84 @@ int field_eval(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
 
 // Solves A U = -b for the induced dipoles, b the permanent field (dE/dU at U = 0), A = d2E/dU2.
 // With rhs (the second-order pass) it solves A U = -rhs from U = 0 by CG instead.
+// layout of d_pcg: acc[4][4] doubles, barrier words {count, gen, status, pad}, CgStatus
+constexpr size_t kPcgAcc = 0, kPcgBar = 16 * sizeof(double), kPcgOut = kPcgBar + 4 * sizeof(unsigned);
+constexpr size_t kPcgPhase = kPcgOut + 32;  // CgStatus padded to 32 B, then 8 pass timers
+constexpr size_t kPcgBytes = kPcgPhase + 8 * sizeof(unsigned long long);
+
+// The CG iterations after k_cg_init (sc[0] = r.z, sc[3] = r.r, sc[4] = b.b on the device) in one
+// cooperative launch of k_cg_solve; convergence is decided on the device and read back once.
+int cg_persistent(dmffb_engine* h, cudaStream_t s, const Box& bx, double* U, const double* sc,
+                  dmffb_admp_result* res) {
+    int st;
+    if (!h->d_pcg && (st = dalloc(h, (char**)&h->d_pcg, kPcgBytes))) return st;
+    char* base = (char*)h->d_pcg;
+    CK(cudaMemsetAsync(base, 0, kPcgBytes, s));
+    CgSolveArgs a = {};
+    a.n = h->n;
+    a.x = U;
+    a.r = h->d_r;
+    a.z = h->d_z;
+    a.p = h->d_p;
+    a.Ap = h->d_Ap;
+    a.fmv = h->d_fmv;
+    a.pol = h->d_pol;
+    a.csr.n = h->n;
+    a.csr.off = h->d_csr_off;
+    a.csr.ent = h->d_csr_ent;
+    a.coef = (const MvCoef<float>*)h->d_mvcoef;
+    a.pos4 = (const float*)h->d_posT;
+    a.bxT = boxT<float>(bx);
+    a.st = stencil_cache<float>(h);
+    a.g = mesh_geom(bx, h->K);
+    a.perm_mul = h->perm_mul;
+    a.gscale = 2.0 * DMFFB_DIELECTRIC;
+    const double k = h->kappa;
+    a.self1 = -2.0 * DMFFB_DIELECTRIC * (k / 1.7724538509055159) * 2.0 * k * k / 3.0;
+    a.fc = fc_args(h, (float*)h->d_grid2, (float*)h->d_grid);
+    a.acc = (double*)(base + kPcgAcc);
+    a.init = sc;
+    a.tol = h->cg_tol;
+    a.max_iter = h->max_iter;
+    unsigned* bw = (unsigned*)(base + kPcgBar);
+    a.bar.count = bw;
+    a.bar.gen = bw + 1;
+    a.bar.status = (int*)(bw + 2);
+    a.bar.wait_ns = (long long)(h->pcg_wait_s * 1e9);
+    a.bar.phantom = (unsigned)h->pcg_phantom;
+    h->pcg_phantom = 0;
+    a.out = (CgStatus*)(base + kPcgOut);
+    a.phase_ns = h->prof ? (unsigned long long*)(base + kPcgPhase) : nullptr;
+    // CTAs: enough warps for the matvec + spread pass (two warps per atom), the x-planes and the
+    // spectrum column blocks, within what the device holds at once
+    const int ncb = (h->K[1] * (h->K[2] / 2 + 1) + kFcCols - 1) / kFcCols;
+    int grid = (int)((2 * (int64_t)h->n + kCgThreads / 32 - 1) / (kCgThreads / 32));
+    grid = std::max(grid, std::max(h->K[0], ncb));
+    grid = std::min(grid, h->pcg_max_blocks);
+    void* args[] = {&a};
+    LAUNCH(h, s, KC_CGSOLVE, CK(cudaLaunchCooperativeKernel((const void*)k_cg_solve, dim3(grid), dim3(kCgThreads),
+                                                            args, cg_solve_smem(h->K), s)));
+    static_assert(sizeof(CgStatus) <= 32, "status block of the persistent solve");
+    CK(cudaMemcpyAsync(h->h_scal, a.out, a.phase_ns ? kPcgBytes - kPcgOut : sizeof(CgStatus),
+                       cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CgStatus cs;
+    memcpy(&cs, h->h_scal, sizeof(cs));
+    if (a.phase_ns) {
+        unsigned long long ph[8];
+        memcpy(ph, (char*)h->h_scal + (kPcgPhase - kPcgOut), sizeof(ph));
+        for (int k = 0; k < 8; ++k) h->pcg_phase_ms[k] += ph[k] * 1e-6;
+    }
+    const int n3 = 3 * h->n;
+    res->n_iter = cs.iters;
+    res->converged = cs.converged;
+    res->residual_rms = sqrt(cs.rr / n3);
+    if (cs.status == DMFFB_CG_TIMEOUT)
+        return fail(h, DMFFB_TIMEOUT, "dipole solve: a grid barrier wait of the persistent CG kernel ran out");
+    if (cs.status == DMFFB_CG_NONFINITE) return fail(h, DMFFB_NONFINITE, "non-finite residual in the dipole solve");
+    return DMFFB_OK;
+}
+
 template <typename T>
 int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx, const int32_t* pairs,
                   int64_t npairs, double* U, dmffb_admp_result* res, const double* rhs = nullptr) {
@@ -1002,11 +1137,13 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     CK(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
     LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_r, h->d_z, h->d_r, h->d_r, sc + 0, sc + 3));
     LAUNCH(h, s, KC_VEC, k_dot2<<<nb3, 256, 0, s>>>(3 * n, h->d_b, h->d_b, nullptr, nullptr, sc + 4, nullptr));
+    const bool fused = h->lpme && h->have_plans && h->stencils_ready;
+    if (sizeof(T) == 4 && fused && pcg_wanted(h) && h->d_fcW && pcg_decide(h) > 0)
+        return cg_persistent(h, s, bx, U, sc, res);
     int it = 0;
     bool conv = false;
     double rms = 0.0, rms_b = 0.0;
     // one CG iteration; slot = parity of the r.z scalar it reads
-    const bool fused = h->lpme && h->have_plans && h->stencils_ready;
     auto iteration = [&](int slot) -> int {
         int st2;
         if (fused) {
@@ -1786,6 +1923,7 @@ int upload_topology(dmffb_engine* h, const dmffb_admp_desc* d) {
 // PME mesh of h->K: grids grown to fit, B-spline moduli, cuFFT plans (cached per mesh shape)
 int setup_mesh(dmffb_engine* h) {
     h->fc_ok = -1;  // whether the engine's FFT convolution serves the mesh is decided again
+    h->pcg_max_blocks = -1;
     const size_t ts = h->prec == DMFFB_FP32 ? 4 : 8;
     const int64_t K3 = (int64_t)h->K[0] * h->K[1] * h->K[2];
     const int64_t Kc = (int64_t)h->K[0] * h->K[1] * (h->K[2] / 2 + 1);
@@ -1958,7 +2096,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_fcW, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
+                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_fcW, h->d_pcg, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -3163,6 +3301,30 @@ int dmffb_set_timing(dmffb_engine* h, int32_t enabled) {
 int dmffb_set_fused_fft(dmffb_engine* h, int32_t enabled) {
     if (!h) return DMFFB_BAD_ARG;
     h->fc_enabled = enabled != 0;
+    return DMFFB_OK;
+}
+
+int dmffb_set_persistent_cg(dmffb_engine* h, int32_t mode) {
+    if (!h || mode < 0 || mode > 2) return DMFFB_BAD_ARG;
+    h->pcg_mode = mode;
+    return DMFFB_OK;
+}
+
+int dmffb_persistent_cg_blocks(const dmffb_engine* h) {
+    if (!h) return -1;
+    return pcg_wanted(h) && h->pcg_max_blocks > 0 ? h->pcg_max_blocks : 0;
+}
+
+int dmffb_get_cg_phase_times(const dmffb_engine* h, double* ms_out, int32_t n) {
+    if (!h || !ms_out || n < 0) return DMFFB_BAD_ARG;
+    for (int k = 0; k < n && k < 8; ++k) ms_out[k] = h->pcg_phase_ms[k];
+    return DMFFB_OK;
+}
+
+int dmffb_set_cg_wait_limit(dmffb_engine* h, double seconds, int32_t phantom_arrivals) {
+    if (!h || !(seconds > 0) || phantom_arrivals < 0) return DMFFB_BAD_ARG;
+    h->pcg_wait_s = seconds;
+    h->pcg_phantom = phantom_arrivals;
     return DMFFB_OK;
 }
 

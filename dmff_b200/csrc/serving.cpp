@@ -6,7 +6,9 @@
 // arrival time has passed and the device footprint of everything in flight plus its own fits
 // the budget.  Workers run their requests through dmffb_admp_compute_host on their own streams,
 // so the GPU interleaves the kernels of all admitted requests: many small, launch-bound boxes
-// overlap, while the footprint budget keeps only a few large ones in flight.
+// overlap, while the footprint budget keeps only a few large ones in flight.  With several slots
+// the engines run the per-pass dipole solve (short kernels that interleave); a single slot uses
+// the persistent solve for small requests.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -174,6 +176,10 @@ int dmffb_server_create(const dmffb_server_desc* d, dmffb_server** out) {
             return st;
         }
         dmffb_set_graphs(h, d->use_graphs);
+        // several slots: the per-pass solve, whose short kernels interleave with the other slots'
+        // (a persistent solve holds its SMs for the whole solve, mostly waiting at barriers);
+        // one slot: the engine's size rule, which shortens each small request
+        dmffb_set_persistent_cg(h, d->n_slots > 1 ? 0 : 2);
         s->eng.push_back(h);
     }
     for (int k = 0; k < d->n_slots; ++k) s->workers.emplace_back(worker, s, k);

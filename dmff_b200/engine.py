@@ -320,8 +320,33 @@ class AdmpEngine:
 
     def set_fused_fft(self, on=True):
         """The dipole solve's reciprocal convolution through the engine's own FFT kernels (FP32,
-        7-smooth meshes up to 64 per axis) or through cuFFT (dmffb_set_fused_fft)."""
+        meshes up to 64 per axis) or through cuFFT (dmffb_set_fused_fft)."""
         self._check(self.lib.dmffb_set_fused_fft(self.h, int(bool(on))))
+
+    def set_persistent_cg(self, mode=True):
+        """The whole CG dipole solve in one persistent cooperative launch (FP32, meshes up to 64
+        per axis; dmffb_set_persistent_cg): True / 1 always, False / 0 never (the graph-replayed
+        per-pass solve), "auto" / 2 (the default) for systems of at most 4096 atoms."""
+        m = 2 if mode == "auto" else int(mode)
+        self._check(self.lib.dmffb_set_persistent_cg(self.h, m))
+
+    def persistent_cg_blocks(self):
+        """Co-resident CTAs of the persistent solve for the current mesh (0: not used)."""
+        return int(self.lib.dmffb_persistent_cg_blocks(self.h))
+
+    def set_cg_wait_limit(self, seconds, phantom_arrivals=0):
+        """Bound of each grid-barrier wait of the persistent solve; phantom_arrivals > 0 makes the
+        next solve's barrier wait for arrivals that never come (it returns DMFFB_TIMEOUT)."""
+        self._check(self.lib.dmffb_set_cg_wait_limit(self.h, float(seconds), int(phantom_arrivals)))
+
+    CG_PHASES = ["direction", "matvec_spread", "fft_planes_fwd", "fft_columns", "fft_planes_inv", "gather",
+                 "update"]
+
+    def cg_phase_times(self):
+        """{pass: ms} of the persistent solves run while profiling was on (device clock, CTA 0)."""
+        arr = (ctypes.c_double * 8)()
+        self.lib.dmffb_get_cg_phase_times(self.h, arr, 8)
+        return {k: arr[i] for i, k in enumerate(self.CG_PHASES)}
 
     def fused_fft_active(self):
         """Whether the last solve's convolution ran through the engine's FFT (else cuFFT)."""

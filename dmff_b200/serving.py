@@ -159,10 +159,14 @@ def stream_stats(reqs):
     atoms = sum(r.n_atoms for r in reqs)
     t_first = min(r.c.t_arrival for r in reqs)
     t_last = max(r.c.t_done for r in reqs)
-    bad = sum(1 for r in reqs if r.status not in (L.DMFFB_OK, L.DMFFB_NOT_CONVERGED))
+    bad = [r.status for r in reqs if r.status not in (L.DMFFB_OK, L.DMFFB_NOT_CONVERGED)]
+    codes = {}
+    for c in bad:
+        codes[str(int(c))] = codes.get(str(int(c)), 0) + 1
     return {"requests": len(reqs), "atoms": int(atoms), "wall_s": t_last - t_first,
             "atom_evals_per_s": atoms / (t_last - t_first), "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3), "failed": bad,
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3), "failed": len(bad),
+            "failed_status": codes,
             "not_converged": sum(1 for r in reqs if r.status == L.DMFFB_NOT_CONVERGED)}
 
 

@@ -26,7 +26,8 @@ enum {
     DMFFB_NEIGHBOR_OVERFLOW = 5,  /* pair capacity too small; *npairs_out holds the count needed */
     DMFFB_NONFINITE = 6,
     DMFFB_CUFFT_ERROR = 7,
-    DMFFB_SCRATCH_TOO_SMALL = 8   /* request exceeds a fixed-size scratch limit (see the _noalloc entry) */
+    DMFFB_SCRATCH_TOO_SMALL = 8,  /* request exceeds a fixed-size scratch limit (see the _noalloc entry) */
+    DMFFB_TIMEOUT = 9             /* a bounded device-side wait ran out; the context stays usable */
 };
 
 /* local-axis types, dmff/admp/spatial.py:59-65 */
@@ -209,7 +210,8 @@ int dmffb_set_timing(dmffb_engine* h, int32_t enabled);
  * 8 gather FIELD, 9 self+frame forces, 10 vector/CG ops, 11 neighbour build, 12 CG matvec
  * pair-tensor set-up, 13 pair FULL over the topologically scaled rows (FP64), 14 pair FIELD over
  * the scaled rows (FP64), 15 parameter-adjoint pair kernels, 16 bonded terms, 17 the engine-FFT
- * convolution of the dipole solve (dmffb_set_fused_fft).  Classes 1 and 2
+ * convolution of the dipole solve (dmffb_set_fused_fft), 18 the persistent CG solve
+ * (dmffb_set_persistent_cg).  Classes 1 and 2
  * hold only the launches over the unscaled rows (kernel precision). */
 int dmffb_set_profiling(dmffb_engine* h, int32_t enabled);
 int dmffb_get_kernel_stats(const dmffb_engine* h, double* ms_out, int64_t* launches_out, int32_t n);
@@ -328,9 +330,27 @@ int dmffb_classical_param_grads(dmffb_engine* h, void* stream, double* dE_dq, do
 /* The dipole-solve iterations' reciprocal convolution (forward FFT, influence-function multiply,
  * inverse FFT) through the engine's own three-pass FFT (x-planes, spectrum columns with the
  * multiply, x-planes) instead of cuFFT R2C + convolution + C2R, on/off (off by default; FP32
- * engines with 7-smooth meshes of at most 64 points per axis, else cuFFT).
+ * engines with meshes of at most 64 points per axis, else cuFFT).
  * dmffb_fused_fft_active returns 1 when the last solve used it, 0 for the cuFFT path. */
 int dmffb_set_fused_fft(dmffb_engine* h, int32_t enabled);
+/* The whole CG dipole solve in one persistent cooperative launch (k_cg_solve: direction update,
+ * real-space matvec and dipole spread, the engine-FFT convolution, field gather and CG update per
+ * iteration, separated by grid barriers; convergence decided on the device, one read-back per
+ * solve).  mode 0: off (the graph-replayed per-pass solve), 1: on, 2 (default): on for systems of
+ * at most 4096 atoms, where the launch chain of the per-pass solve dominates.  FP32 engines with
+ * meshes of at most 64 points per axis on devices with cooperative launch only.
+ * dmffb_persistent_cg_blocks returns the co-resident CTAs available to it for the current mesh
+ * (0: not used).
+ * dmffb_set_cg_wait_limit bounds every grid-barrier wait of the kernel (default 2 s): past it the
+ * solve returns DMFFB_TIMEOUT with the context usable; phantom_arrivals > 0 makes the next solve's
+ * first barrier wait for arrivals that never come (for tests of that path). */
+int dmffb_set_persistent_cg(dmffb_engine* h, int32_t mode);
+int dmffb_persistent_cg_blocks(const dmffb_engine* h);
+int dmffb_set_cg_wait_limit(dmffb_engine* h, double seconds, int32_t phantom_arrivals);
+/* Device-clock time of each pass of the persistent solve (0 direction update, 1 matvec + spread,
+ * 2 forward planes, 3 spectrum columns, 4 inverse planes, 5 field gather, 6 CG update; barrier
+ * waits included, measured on CTA 0), summed over the solves run while profiling was on. */
+int dmffb_get_cg_phase_times(const dmffb_engine* h, double* ms_out, int32_t n);
 int dmffb_fused_fft_active(const dmffb_engine* h);
 /* ---------------------------------------------------------------------------------------
  * Short-range pairwise terms with per-atom parameters: the built-in kernels of
@@ -384,7 +404,9 @@ int dmffb_set_graphs(dmffb_engine* h, int32_t enabled);
  * the head request is admitted when its arrival time has passed, a slot is idle and the summed
  * device footprint of the requests in flight plus its own stays within hbm_budget_bytes.
  * Admitted requests run concurrently on their slots' streams, so small requests overlap on the
- * GPU while large ones limit how many run at once. */
+ * GPU while large ones limit how many run at once.  With n_slots > 1 the slots run the per-pass
+ * dipole solve (its short kernels interleave across slots); with one slot the persistent solve
+ * serves small requests (dmffb_set_persistent_cg mode 2). */
 typedef struct dmffb_server dmffb_server;
 
 typedef struct {

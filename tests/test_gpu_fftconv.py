@@ -13,6 +13,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _solve(eng, s, fused):
+    eng.set_persistent_cg(False)  # the per-pass solve: cuFFT or the engine FFT kernels
     eng.set_fused_fft(fused)
     eng.set_zero_guess(True)
     pos = torch.tensor(s["pos"], dtype=torch.float64, device="cuda")
@@ -22,23 +23,15 @@ def _solve(eng, s, fused):
     return res, F.cpu().numpy().copy(), U.cpu().numpy().copy(), eng.fused_fft_active()
 
 
-def _smooth(k):
-    for r in (2, 3, 5, 7):
-        while k % r == 0:
-            k //= r
-    return k == 1
-
-
-@pytest.mark.parametrize("n_waters", [150, 300, 700, 2300, 3900])
+@pytest.mark.parametrize("n_waters", [150, 300, 700, 2300, 3900, 9000])
 def test_fused_convolution_matches_cufft(n_waters):
-    """Serving-stream boxes: meshes 17^3 (prime: cuFFT), 21^3, 28^3, 41^3 (prime: cuFFT), 50^3 and
-    beyond."""
+    """Serving-stream boxes: meshes 17^3 (prime), 21^3, 28^3, 41^3 (prime), 50^3 and beyond."""
     s = serving_system(n_waters, 500 + n_waters)
     eng = make_engine(s, precision="fp32", cg_tol=1e-7)
     r0, F0, U0, cl0 = _solve(eng, s, False)
     r1, F1, U1, cl1 = _solve(eng, s, True)
     assert not cl0
-    assert cl1 == (max(s["K"]) <= 64 and all(_smooth(k) for k in s["K"])), (s["K"], cl1)
+    assert cl1 == (max(s["K"]) <= 64), (s["K"], cl1)
     assert abs(r1.energy - r0.energy) <= 2e-6 * abs(r0.energy), (s["K"], r1.energy, r0.energy)
     assert rel_force_rms(F1, F0) < 1e-5
     assert np.abs(U1 - U0).max() <= 1e-5 * np.abs(U0).max()

@@ -148,14 +148,16 @@ def _peg_case():
     gold = json.load(open(os.path.join(HERE, "golden", "energies.json")))["peg2_slater"]
     pdb = PDBFile(os.path.join(DATA, gold["pdb"]))
     H = Hamiltonian(os.path.join(DATA, gold["xml"]))
+    # FP64 and the reference's own dipole iteration (fixed-point steps to POL_CONV), as the values were made
     pots = H.createPotential(pdb.topology, nonbondedCutoff=gold["rc_nm"], nonbondedMethod="CutoffPeriodic",
-                             ethresh=gold["ethresh"])
+                             ethresh=gold["ethresh"], precision="fp64", pol_solver="reference")
     cov = pdb.topology.buildCovMat()
     pos = np.asarray(pdb.positions, dtype=np.float64)
     box = np.asarray(pdb.topology.getPeriodicBoxVectors(), dtype=np.float64)
     nbl = NeighborList(box, gold["rc_nm"], cov)
     nbl.allocate(pos)
-    pairs = np.asarray(nbl.pairs)
+    pairs = nbl.pairs
+    pairs = pairs.cpu().numpy() if torch.is_tensor(pairs) else np.asarray(pairs)
     pairs = pairs[pairs[:, 0] < pairs[:, 1]]
     return gold, H, pots, pos, box, pairs
 

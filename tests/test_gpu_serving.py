@@ -126,3 +126,21 @@ def test_large_requests_same_alone_and_in_the_mix_and_fp64():
         assert rel_force_rms(b.forces, a.forces) < 1e-4
         assert abs(a.energy - p.energy) <= 1e-5 * abs(p.energy)
         assert rel_force_rms(a.forces, p.forces) < 1e-4
+
+
+def test_many_mesh_shapes_in_flight():
+    """48 requests alternating small and large meshes (17^3 .. 49^3) on 12 slots: engines of
+    different meshes launch the persistent solve and the FFT kernels side by side, every request
+    succeeds and matches its result alone."""
+    sizes = [100, 1500, 150, 1200, 200, 2300, 300, 900, 120, 3900, 450, 700] * 4
+    syss = [serving_system(n, 300 + k) for k, n in enumerate(sizes)]
+    cap = 3 * max(sizes)
+    one = AdmpServer(n_slots=1, capacity_atoms=cap, precision="fp32")
+    ref, _ = _run(one, syss)
+    one.close()
+    srv = AdmpServer(n_slots=12, capacity_atoms=cap, precision="fp32")
+    reqs, stats = _run(srv, syss)
+    srv.close()
+    for a, b in zip(reqs, ref):
+        assert abs(a.energy - b.energy) <= 2e-6 * abs(b.energy)
+        assert rel_force_rms(a.forces, b.forces) < 2e-5
