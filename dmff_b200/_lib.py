@@ -43,7 +43,8 @@ EXPORTED = [
     "dmffb_pairwise_param_grads",
 ]
 DMFFB_SR_TT_QQ, DMFFB_SR_SLATER_DISP, DMFFB_SR_SLATER, DMFFB_SR_TT_QQ_C6 = 0, 1, 2, 3
-SR_NPARAM = {0: 2, 1: 4, 2: 2, 3: 4}
+DMFFB_SR_QEQ_GAUSS3, DMFFB_SR_QEQ_GAUSS2 = 4, 5
+SR_NPARAM = {0: 2, 1: 4, 2: 2, 3: 4, 4: 2, 5: 2}
 
 DMFFB_COUL_NONE = 0
 DMFFB_COUL_PME = 1

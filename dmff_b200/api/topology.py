@@ -187,10 +187,12 @@ class DMFFTopology:
                 a = by_name.get(p["name"])
                 if a is None:
                     continue
-                for k, v in p.items():  # type plus per-atom attributes such as charge
+                # type plus per-atom attributes such as charge; what the caller already set on
+                # the atom (as the reference's tests set charges and types by hand) stays
+                for k, v in p.items():
                     if k != "name":
-                        a.meta[k] = v
-                a.meta["class"] = type2class.get(p["type"])
+                        a.meta.setdefault(k, v)
+                a.meta.setdefault("class", type2class.get(a.meta.get("type", p["type"])))
             if not any(have_bond[a.index] for a in res._atoms):
                 for b in tpl["bonds"]:
                     if "atomName1" in b:

@@ -2999,6 +2999,8 @@ int pairwise_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, co
             case SR_TT_QQ: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_TT_QQ><<<nbk, 128, 0, s>>>(a)); break;
             case SR_SLATER_DISP: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_SLATER_DISP><<<nbk, 128, 0, s>>>(a)); break;
             case SR_SLATER: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_SLATER><<<nbk, 128, 0, s>>>(a)); break;
+            case SR_QEQ_GAUSS3: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_QEQ_GAUSS3><<<nbk, 128, 0, s>>>(a)); break;
+            case SR_QEQ_GAUSS2: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_QEQ_GAUSS2><<<nbk, 128, 0, s>>>(a)); break;
             default: LAUNCH(h, s, KC_PAIR_FULL, k_sr_pair<T, SR_TT_QQ_C6><<<nbk, 128, 0, s>>>(a)); break;
         }
         CK(cudaGetLastError());
@@ -3019,7 +3021,7 @@ extern "C" {
 int dmffb_pairwise_create(const dmffb_pairwise_desc* d, dmffb_engine** out) {
     if (!d || !out) return DMFFB_BAD_ARG;
     *out = nullptr;
-    if (d->n_atoms <= 0 || d->kind < DMFFB_SR_TT_QQ || d->kind > DMFFB_SR_TT_QQ_C6 || !(d->rc > 0)) return DMFFB_BAD_ARG;
+    if (d->n_atoms <= 0 || d->kind < DMFFB_SR_TT_QQ || d->kind > DMFFB_SR_QEQ_GAUSS2 || !(d->rc > 0)) return DMFFB_BAD_ARG;
     dmffb_admp_desc a;
     memset(&a, 0, sizeof(a));
     a.n_atoms = d->n_atoms;

@@ -12,6 +12,9 @@
 //   SR_TT_QQ_C6  (pairwise.py:100-118, generate_pairwise_interaction(TT_damping_qq_c6_kernel)):
 //                E = 2625.5 a e^-x - 2625.5 e^-x (1 + x) q / r_b + e^-x P6(x) c / r^6,
 //                r_b = 1.889726878 r,  x = b r_b,  a = sqrt(a_i a_j), q = q_i q_j, c = c_i c_j
+//   SR_QEQ_GAUSS3 (qeq.py:98-112, the Gaussian-charge short range of ADMPQeqForce, DampMod 3):
+//                E = -D erfc(r / s) q / r,  s = sqrt(eta_i^2 + eta_j^2),  q = q_i q_j (0 when s <= 1e-4)
+//   SR_QEQ_GAUSS2 (qeq.py:85-95, DampMod 2): the same with s = sqrt(2 (eta_i^2 + eta_j^2))
 // each times m.  One thread per pair row (the layout of the classical pair kernel: minimum image
 // in FP64, i-side warp segmented sums, j-side atomics, FP64 block reduction of the energy and box
 // gradient); dE/dr and every per-atom parameter partial come from the closed forms, using
@@ -22,11 +25,11 @@
 
 namespace dmffb {
 
-enum { SR_TT_QQ = 0, SR_SLATER_DISP = 1, SR_SLATER = 2, SR_TT_QQ_C6 = 3 };
+enum { SR_TT_QQ = 0, SR_SLATER_DISP = 1, SR_SLATER = 2, SR_TT_QQ_C6 = 3, SR_QEQ_GAUSS3 = 4, SR_QEQ_GAUSS2 = 5 };
 
 // parameters per atom of each kind
 __host__ __device__ constexpr int sr_nparam(int kind) {
-    return kind == SR_TT_QQ ? 2 : (kind == SR_SLATER_DISP ? 4 : (kind == SR_SLATER ? 2 : 4));
+    return kind == SR_SLATER_DISP || kind == SR_TT_QQ_C6 ? 4 : 2;
 }
 
 template <typename T>
@@ -57,8 +60,8 @@ __device__ __forceinline__ void exp_series(TC x, int K, TC& s, TC& last) {
 }
 
 // E(r) and dE/dr of one pair, with dE/d(pair parameter) in gp[0..3]: the pair parameters are
-// (b, q) for TT_QQ, (b, c6, c8, c10) for SLATER_DISP, (a, b) for SLATER, (a, b, q, c) for TT_QQ_C6
-// where a, b (and the Slater a) are the combined values above
+// (b, q) for TT_QQ, (b, c6, c8, c10) for SLATER_DISP, (a, b) for SLATER, (a, b, q, c) for TT_QQ_C6,
+// (q, s) for the QEQ_GAUSS kinds, where a, b, s (and the Slater a) are the combined values above
 template <int KIND, typename TC>
 __device__ __forceinline__ void sr_eval(TC r, const TC pp[4], TC& e, TC& de, TC gp[4]) {
     const TC D = TC(DMFFB_DIELECTRIC);
@@ -109,6 +112,21 @@ __device__ __forceinline__ void sr_eval(TC r, const TC pp[4], TC& e, TC& de, TC 
         gp[0] = P * ey;
         gp[1] = dEdy * r;
         gp[2] = gp[3] = TC(0);
+    } else if (KIND == SR_QEQ_GAUSS3 || KIND == SR_QEQ_GAUSS2) {
+        const TC q = pp[0], sw = pp[1];
+        gp[2] = gp[3] = TC(0);
+        if (!(sw > TC(1e-4))) {
+            e = de = gp[0] = gp[1] = TC(0);
+        } else {
+            const TC rinv = TC(1) / r;
+            const TC x = r / sw;
+            const TC ec = d_erfc(x);
+            const TC g = TC(DMFFB_TWO_OVER_SQRTPI) * d_exp(-x * x);  // -d erfc / dx
+            e = -D * q * ec * rinv;
+            de = -D * q * (-g / sw * rinv - ec * rinv * rinv);
+            gp[0] = -D * ec * rinv;
+            gp[1] = -D * q * g / (sw * sw);  // d erfc(r / s) / ds = g r / s^2
+        }
     } else {  // SR_TT_QQ_C6
         const TC a = pp[0], b = pp[1], q = pp[2], c = pp[3];
         const TC kb = TC(1.889726878);
@@ -181,6 +199,10 @@ __global__ void __launch_bounds__(128) k_sr_pair(SrArgs<T> a) {
         } else if (KIND == SR_SLATER) {
             pp[0] = vi[0] * vj[0];
             pp[1] = sqrt(vi[1] * vj[1]);
+        } else if (KIND == SR_QEQ_GAUSS3 || KIND == SR_QEQ_GAUSS2) {
+            pp[0] = vi[0] * vj[0];
+            const T c2 = KIND == SR_QEQ_GAUSS2 ? T(2) : T(1);
+            pp[1] = sqrt(c2 * (vi[1] * vi[1] + vj[1] * vj[1]));
         } else {
             pp[0] = sqrt(vi[0] * vj[0]);
             pp[1] = sqrt(vi[1] * vj[1]);
@@ -213,6 +235,12 @@ __global__ void __launch_bounds__(128) k_sr_pair(SrArgs<T> a) {
             } else if (KIND == SR_SLATER) {
                 gi[0] = gp[0] * vj[0]; gj[0] = gp[0] * vi[0];
                 gi[1] = gp[1] * sq(vi[1], vj[1], pp[1]); gj[1] = gp[1] * sq(vj[1], vi[1], pp[1]);
+            } else if (KIND == SR_QEQ_GAUSS3 || KIND == SR_QEQ_GAUSS2) {
+                // s^2 = c2 (eta_i^2 + eta_j^2): ds / deta_i = c2 eta_i / s
+                const T c2 = KIND == SR_QEQ_GAUSS2 ? T(2) : T(1);
+                gi[0] = gp[0] * vj[0]; gj[0] = gp[0] * vi[0];
+                const T sinv = pp[1] > T(0) ? T(1) / pp[1] : T(0);
+                gi[1] = gp[1] * c2 * vi[1] * sinv; gj[1] = gp[1] * c2 * vj[1] * sinv;
             } else {
                 gi[0] = gp[0] * sq(vi[0], vj[0], pp[0]); gj[0] = gp[0] * sq(vj[0], vi[0], pp[0]);
                 gi[1] = gp[1] * sq(vi[1], vj[1], pp[1]); gj[1] = gp[1] * sq(vj[1], vi[1], pp[1]);

@@ -363,8 +363,13 @@ int dmffb_fused_fft_active(const dmffb_engine* h);
  *   DMFFB_SR_SLATER_DISP (b, c6, c8, c10): Slater-ISA damped C6/C8/C10 (pairwise.py:131-156)
  *   DMFFB_SR_SLATER      (a, b):           a_i a_j ((br)^2 / 3 + br + 1) e^-br (pairwise.py:159-171)
  *   DMFFB_SR_TT_QQ_C6    (a, b, q, c):     TT_damping_qq_c6_kernel (pairwise.py:100-118)
- * each times mscales[nbond - 1] and the description's sign. */
-enum { DMFFB_SR_TT_QQ = 0, DMFFB_SR_SLATER_DISP = 1, DMFFB_SR_SLATER = 2, DMFFB_SR_TT_QQ_C6 = 3 };
+ *   DMFFB_SR_QEQ_GAUSS3  (q, eta):         -DIELECTRIC erfc(r / s) q_i q_j / r, s = sqrt(eta_i^2 + eta_j^2),
+ *                                          0 for s <= 1e-4 (ADMPQeqForce DampMod 3, dmff/admp/qeq.py:98-112)
+ *   DMFFB_SR_QEQ_GAUSS2  (q, eta):         the same with s = sqrt(2 (eta_i^2 + eta_j^2)) (DampMod 2, :85-95)
+ * each times mscales[nbond - 1] and the description's sign.  The parameter adjoints of the QEq
+ * kinds with respect to q are the short-range part of the charge Hessian times q. */
+enum { DMFFB_SR_TT_QQ = 0, DMFFB_SR_SLATER_DISP = 1, DMFFB_SR_SLATER = 2, DMFFB_SR_TT_QQ_C6 = 3,
+       DMFFB_SR_QEQ_GAUSS3 = 4, DMFFB_SR_QEQ_GAUSS2 = 5 };
 
 typedef struct {
     int32_t n_atoms;

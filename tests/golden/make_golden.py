@@ -110,6 +110,11 @@ def main():
         # Slater-ISA / short-range inputs (tests/test_admp/test_slater.py)
         f"{REF}/tests/data/peg.xml": "peg.xml",
         f"{REF}/tests/data/peg2.pdb": "peg2.pdb",
+        # charge-equilibration inputs (tests/test_admp/test_qeq.py)
+        f"{REF}/tests/data/qeq.xml": "qeq.xml",
+        f"{REF}/tests/data/qeq.pdb": "qeq.pdb",
+        f"{REF}/tests/data/qeq2.xml": "qeq2.xml",
+        f"{REF}/tests/data/qeq2.pdb": "qeq2.pdb",
         f"{wf}/forcefield.xml": "waterbox_forcefield.xml",
         f"{wf}/residues.xml": "waterbox_residues.xml",
         f"{wf}/quadrupole_nonpol/forcefield.xml": "waterbox_quadrupole_nonpol.xml",
@@ -176,6 +181,16 @@ def main():
         "forces": ["ADMPPmeForce", "ADMPDispPmeForce", "SlaterExForce", "SlaterSrEsForce", "SlaterSrPolForce",
                    "SlaterSrDispForce", "SlaterDhfForce", "QqTtDampingForce", "SlaterDampingForce"],
         "values": [float(v) for v in slater["values"]]}
+    # the two charge-equilibration energies of tests/test_admp/test_qeq.py
+    qeq_src = open(f"{REF}/tests/test_admp/test_qeq.py").read()
+    qm = re.findall(r"assert_almost_equal\(energy, (-?[\d.]+), decimal=(\d)", qeq_src)
+    qv = [float(v) for v, _ in qm]
+    qd = [int(d) for _, d in qm]
+    energies["qeq"] = {"xml": "qeq.xml", "pdb": "qeq.pdb", "rc_nm": 0.6, "ethresh": 1e-3, "value": qv[0],
+                       "decimal": qd[0], "source": "tests/test_admp/test_qeq.py:12-40"}
+    energies["qeq2"] = {"xml": "qeq2.xml", "pdb": "qeq2.pdb", "rc_nm": 0.6, "ethresh": 1e-3, "value": qv[1],
+                        "decimal": qd[1], "source": "tests/test_admp/test_qeq.py:43-89",
+                        "groups": [[0, 144], [144, 147]], "group_vals": [0.0, 0.0], "lagmt0": [1.0, 1.0]}
     with open(os.path.join(HERE, "energies.json"), "w") as f:
         json.dump(energies, f, indent=1)
 
