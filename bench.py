@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--cg", default="auto", choices=["auto", "persistent", "per-pass"],
                    help="dipole solve: persistent CG kernel, graph-replayed per-pass solve, or the "
                         "engine's size rule (persistent up to 4096 atoms)")
+    p.add_argument("--size-sweep", action="store_true",
+                   help="per-request latency of single serving boxes (150-9000 waters) with the per-pass and "
+                        "the persistent dipole solve, one JSON line, then exit")
     p.add_argument("--fused-fft", action="store_true",
                    help="dipole-solve convolution through the engine's FFT kernels instead of cuFFT")
     return p.parse_args()
@@ -626,6 +629,43 @@ def classical_cpu_reference(s, cfg, args):
 
 
 # ---------------------------------------------------------------------------------- GPU side
+def size_sweep(dev):
+    """One engine re-pointed at serving boxes of 150-9000 waters (three boxes per size, four passes
+    each, the first dropped): median host time of reconfigure + set_params + compute_host and the
+    engine's device time of the dipole solve, per-pass vs persistent CG."""
+    import torch
+    from dmff_b200.engine import AdmpEngine
+    from dmff_b200.synthetic import serving_system
+    sizes = [150, 300, 600, 1200, 2500, 5000, 9000]
+    systems = {n: [serving_system(n, 100 * n + k) for k in range(3)] for n in sizes}
+    s0 = systems[sizes[-1]][0]
+    eng = AdmpEngine(3 * max(sizes), 2, True, True, s0["rc"], s0["kappa"], s0["K"], s0["axis_types"],
+                     s0["axis_indices"], s0["cov_rows"], s0["mscales"], s0["pscales"], s0["dscales"],
+                     precision="fp32", solver="cg", cg_tol=1e-6, max_iter=500, device=dev)
+    out = {}
+    for mode, name in ((0, "per_pass"), (1, "persistent")):
+        eng.set_persistent_cg(mode)
+        for n in sizes:
+            rows = []
+            for rep in range(4):
+                for s in systems[n]:
+                    t0 = time.perf_counter()
+                    eng.reconfigure(s["n_atoms"], s["rc"], s["kappa"], s["K"], s["axis_types"], s["axis_indices"],
+                                    s["cov_rows"], s["mscales"], s["pscales"], s["dscales"])
+                    eng.set_params(s["Q_local"], s["pol"], s["thole"])
+                    eng.set_timing(True)
+                    res, _, _ = eng.compute_host(s["pos"], s["box"])
+                    t1 = time.perf_counter()
+                    solve_ms = eng.timings()[1]
+                    eng.set_timing(False)
+                    if rep > 0:
+                        rows.append((t1 - t0, solve_ms, res.n_iter))
+            r = np.median(np.array(rows), axis=0)
+            out.setdefault(str(n), {"K": int(systems[n][0]["K"][0])})[name] = {
+                "request_ms": round(float(r[0]) * 1e3, 3), "solve_ms": round(float(r[1]), 3), "cg_iters": int(r[2])}
+    print(json.dumps({"size_sweep": out, "unit": "ms, median of 9", "waters": sizes}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -633,6 +673,11 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "c4":
         run_classical(args, rank, world, local)
+        return
+    if args.size_sweep:
+        import torch
+        torch.cuda.set_device(local)
+        size_sweep(torch.device("cuda", local))
         return
     from dmff_b200.synthetic import workload
     s = workload(args.workload)
