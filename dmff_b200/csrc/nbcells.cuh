@@ -5,10 +5,13 @@
 // written once per step and read once by the pair kernel: at 100 000 atoms and rc 10 A that is
 // 61 M rows, 0.74 GB out and back, plus j-side force atomics.  This pass evaluates the same pair
 // set straight from the cell binning of the step's positions:
-//   * one warp per atom i walks the 5^3 stencil of half-width cells as one concatenated
-//     candidate list (the layout of k_pairs_warp3), 32 candidates per batch, reading a cell-ordered
-//     float4 copy of the positions (contiguous runs per cell, the atom index in the w slot);
-//     atoms are taken in cell order, so the warps of a block share their candidates through L1;
+//   * one warp per atom i walks the forward half of the 5^3 stencil of half-width cells (the 62
+//     offsets after (0, 0, 0) in lexicographic order, and in its own cell the atoms after it in
+//     cell order), so every unordered pair is met once, as one concatenated candidate list, 32
+//     candidates per batch, reading a cell-ordered float4 copy of the positions (contiguous runs
+//     per cell, the atom index in the w slot); atoms are taken in cell order, so the warps of a
+//     block share their candidates through L1 (with at least 5 cells per axis the 5 offsets of an
+//     axis are distinct cells, and a box of at least 2.5 rc has one image of a pair within rc);
 //   * FP32 prefilter on float positions, the exact FP64 test of the list build (within_rc on the
 //     lower/higher orientation) inside a 2e-3 A band around rc, so the kept set is the list's
 //     set bit for bit;
@@ -16,11 +19,11 @@
 //     atom's [cov_lo, cov_hi] range) are skipped here: an FP64 pass over the covalent rows
 //     within rc evaluates them (k_nb_pair with a cut-off test);
 //   * every other kept pair is queued in shared memory and evaluated 32 at a time (every lane
-//     busy) from both of its atoms: nb_eval in kernel precision on the FP64 minimum-image vector
-//     and distance of k_nb_pair, the force added to atom i only (lane registers, one warp sum and one store per atom: no atomics), half of the energy
-//     and of the box gradient per visit;
-//   * the count of kept pairs with j > i (scaled ones included) is the list's row count.
-// Energies and the box gradient accumulate per lane (about 40 pairs each) and meet in an FP64 block
+//     busy): nb_eval in kernel precision on the FP64 minimum-image vector and distance of
+//     k_nb_pair; the force on i accumulates in lane registers (one warp sum and one atomic per
+//     atom), the force on j goes out as an atomic;
+//   * the count of kept pairs (scaled ones included) is the list's row count.
+// Energies and the box gradient accumulate per lane (about 20 pairs each) and meet in an FP64 block
 // reduction.
 #pragma once
 #include "classical.cuh"
@@ -52,7 +55,7 @@ struct NbCellArgs {
     double* scal;             // [0] E_coul, [1] E_lj, [2..10] box gradient, [11] pairs i < j within rc
 };
 
-// One kept pair (i, j) seen from atom i: energy halves, box-gradient halves and the force on i.
+// One kept pair (i, j), met once: energy, box gradient, the force on i (registers) and on j (atomics).
 template <typename T>
 __device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int j, const double* pi,
                                              const BoxT<double>& bxd, bool lj, int ti, T qi, T& g0, T& g1, T& g2,
@@ -78,17 +81,20 @@ __device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int 
     g0 -= s * e[0];
     g1 -= s * e[1];
     g2 -= s * e[2];
-    acc[0] += T(0.5) * ec;
-    acc[1] += T(0.5) * el;
+    atomicAdd(a.grad + 3 * j, s * e[0]);
+    atomicAdd(a.grad + 3 * j + 1, s * e[1]);
+    atomicAdd(a.grad + 3 * j + 2, s * e[2]);
+    acc[0] += ec;
+    acc[1] += el;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[2 + 3 * k + c] -= T(0.5) * nn[k] * s * e[c];
+        for (int c = 0; c < 3; ++c) acc[2 + 3 * k + c] -= nn[k] * s * e[c];
 }
 
 template <typename T>
 __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
-    constexpr int S = 2, W = 2 * S + 1, NQ = W * W * W;
+    constexpr int S = 2, W = 2 * S + 1, NQ = (W * W * W + 1) / 2;  // offsets q0 = 62 .. 124 of the 5^3 stencil
     __shared__ int s_beg[kNbWarps][NQ];
     __shared__ int s_off[kNbWarps][NQ + 1];
     __shared__ int s_q[kNbWarps][64];  // kept candidates waiting for a full 32-lane batch
@@ -122,13 +128,16 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
             const int q = q0 + lane;
             int cnt = 0;
             if (q < NQ) {
-                const int dx = q / (W * W) - S, dy = (q / W) % W - S, dz = q % W - S;
+                const int qq = q + NQ - 1;  // (0, 0, 0) and the offsets after it
+                const int dx = qq / (W * W) - S, dy = (qq / W) % W - S, dz = qq % W - S;
                 const int cx = (c3[0] + dx + a.nc[0]) % a.nc[0];
                 const int cy = (c3[1] + dy + a.nc[1]) % a.nc[1];
                 const int cz = (c3[2] + dz + a.nc[2]) % a.nc[2];
                 const int cc = (cx * a.nc[1] + cy) * a.nc[2] + cz;
-                const int cs = a.cell_start[cc];
-                cnt = a.cell_start[cc + 1] - cs;
+                int cs = a.cell_start[cc];
+                const int ce = a.cell_start[cc + 1];
+                if (q == 0) cs = max(cs, ks + 1);  // own cell: the atoms after i in cell order
+                cnt = max(ce - cs, 0);
                 s_beg[wl][q] = cs;
             }
             int incl = cnt;
@@ -181,7 +190,7 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
                                       : within_rc(a.boxd, a.pos + 3 * j, pi, a.rc);
                 }
             }
-            if (keep && j > i) red[11] += 1.0;
+            if (keep) red[11] += 1.0;
             // topologically scaled pairs belong to the FP64 covalent pass
             if (keep && j >= lo && j <= hi) {
                 const int nbd = j > i ? lookup_nbond(a.cov, i, j) : lookup_nbond(a.cov, j, i);
@@ -208,9 +217,9 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
         g1 = warp_sum(g1);
         g2 = warp_sum(g2);
         if (lane == 0) {
-            a.grad[3 * i] = g0;
-            a.grad[3 * i + 1] = g1;
-            a.grad[3 * i + 2] = g2;
+            atomicAdd(a.grad + 3 * i, g0);
+            atomicAdd(a.grad + 3 * i + 1, g1);
+            atomicAdd(a.grad + 3 * i + 2, g2);
         }
     }
     block_reduce_add<12>(red, a.scal);
