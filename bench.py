@@ -47,8 +47,8 @@ def parse():
     p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the serving stream measured beside the step (0: skip)")
     p.add_argument("--serving-rates", default="50,100,200,500,1000,2000", help="Poisson arrival rates (req/s)")
-    p.add_argument("--serving-slots", type=int, default=12)
-    p.add_argument("--serving-budget-gb", type=float, default=2.0)
+    p.add_argument("--serving-slots", type=int, default=8)
+    p.add_argument("--serving-budget-gb", type=float, default=8.0)
     p.add_argument("--cg", default="auto", choices=["auto", "persistent", "per-pass"],
                    help="dipole solve: persistent CG kernel, graph-replayed per-pass solve, or the "
                         "engine's size rule (persistent up to 4096 atoms)")
@@ -396,7 +396,11 @@ def bench_serving(args, systems, dev, peaks, fp32_peak):
                        "t_ideal_s": round(t_ideal, 4), "t_measured_s": round(st["wall_s"], 4),
                        "frac": round(t_ideal / st["wall_s"], 4)}
     for rate in [float(x) for x in args.serving_rates.split(",") if x]:
-        _, st = srv.run_stream(systems, serving_arrivals(len(systems), rate, seed=33))
+        preq, st = srv.run_stream(systems, serving_arrivals(len(systems), rate, seed=33))
+        # the five slowest requests: queue wait (arrival to admission) and service time
+        worst = sorted(preq, key=lambda r: -r.latency)[:5]
+        st["slowest"] = [{"waters": r.n_atoms // 3, "wait_ms": round((r.c.t_start - r.c.t_arrival) * 1e3, 2),
+                          "service_ms": round((r.c.t_done - r.c.t_start) * 1e3, 2)} for r in worst]
         out[f"poisson_{int(rate)}_per_s"] = st
     srv.close()
     # plain path: FP64, one slot, graphs off, every request back to back

@@ -146,9 +146,12 @@ class AdmpServer:
     def run_stream(self, systems, arrivals, timeout=1800.0):
         """Submit ``systems`` (dicts as built by ``synthetic.serving_system``) with ``arrivals``
         (seconds from now, non-decreasing); returns (requests, stats)."""
+        # the requests (host arrays, C structs) are built before the clock starts, so that the
+        # arrival times are not already past when they are submitted
+        reqs = [ServingRequest(s) for s in systems]
         t0 = self.clock() + 0.05  # a short head start so that submission runs ahead of arrivals
-        reqs = [ServingRequest(s, t0 + float(a)) for s, a in zip(systems, arrivals)]
-        for r in reqs:
+        for r, a in zip(reqs, arrivals):
+            r.c.t_arrival = t0 + float(a)
             self.submit(r)
         self.wait(timeout)
         return reqs, stream_stats(reqs)
