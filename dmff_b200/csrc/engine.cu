@@ -124,7 +124,8 @@ struct dmffb_engine {
     cudaEvent_t e_fork = nullptr, e_join = nullptr, e_in = nullptr, e_out = nullptr;
     cudaEvent_t e_build = nullptr;  // end of the last neighbour build on its stream (no host wait)
     cudaGraphExec_t cg_exec = nullptr;
-    std::vector<double> cg_key;
+    std::vector<double> cg_key;       // what the instantiated graph bakes in
+    std::vector<double> cg_seen_key;  // the previous solve's key
     bool use_graphs = true;
     // ---- dispersion PME / TT damping (engines made by dmffb_disp_create)
     int kind = 0;  // 0 ADMP multipolar PME, 1 dispersion
@@ -1163,14 +1164,22 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
         return DMFFB_OK;
     };
     // two iterations (slot 0 then 1) are captured once into a CUDA graph and replayed; the graph
-    // is recaptured when any pointer or the box it bakes in changes
-    const bool graphs = h->use_graphs && !h->prof;
+    // bakes in pointers and the box, so it is captured on the second solve in a row with the same
+    // ones (a one-off solve, such as a serving request of a new size, runs its launches directly
+    // and pays no capture and instantiation) and replayed while they stay the same
+    bool graphs = h->use_graphs && !h->prof;
     if (graphs) {
         std::vector<double> key = {(double)(uintptr_t)pos, (double)(uintptr_t)pairs, (double)npairs,
                                    (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T),
                                    (double)(uintptr_t)h->d_mvcoef, (double)(uintptr_t)h->d_csr_off,
                                    (double)(h->fc_enabled ? h->fc_ok : 0), (double)(uintptr_t)h->d_fcG};
         for (int k = 0; k < 9; ++k) key.push_back(bx.h[k]);
+        const bool repeat = key == h->cg_seen_key;
+        h->cg_seen_key = key;
+        if ((!h->cg_exec || key != h->cg_key) && !repeat) graphs = false;
+    }
+    if (graphs) {
+        const std::vector<double>& key = h->cg_seen_key;
         if (!h->cg_exec || key != h->cg_key) {
             if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
             cudaGraph_t g;
@@ -2080,6 +2089,7 @@ int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* d) {
         h->cg_exec = nullptr;
     }
     h->cg_key.clear();
+    h->cg_seen_key.clear();
     h->params_set = false;
     h->have_last = false;
     return DMFFB_OK;
