@@ -389,9 +389,20 @@ def bench_serving(args, systems, dev, peaks, fp32_peak):
            "slots": args.serving_slots, "hbm_budget_GB": args.serving_budget_gb,
            "slots_budget_choice": "best of a sweep of 8-32 slots x 2 / 8 GB on this stream (8 slots, 8 GB)",
            "cg_tol_rel": 1e-6, "step": "polarizable ADMP energy + forces + virial, host buffers in and out"}
+    import torch
+    torch.cuda.synchronize(dev)
+    free0 = torch.cuda.mem_get_info(dev)[0]
     srv = AdmpServer(n_slots=args.serving_slots, capacity_atoms=cap, precision="fp32",
                      hbm_budget_bytes=int(args.serving_budget_gb * (1 << 30)), device=dev)
     srv.prewarm([ServingRequest(s) for s in warm])
+    torch.cuda.synchronize(dev)
+    # device memory the slots really hold once every mesh shape has run on each (engines at the
+    # largest request, grown pair and mesh buffers, cached cuFFT plans)
+    used = free0 - torch.cuda.mem_get_info(dev)[0]
+    out["server_device_bytes"] = {"all_slots": int(used), "per_slot": int(used // args.serving_slots),
+                                  "admission": "analytical per-request footprint against the budget "
+                                               "(dmffb_request_footprint); it limits how many large "
+                                               "requests run at once"}
     reqs, st = srv.run_stream(systems, np.zeros(len(systems)))
     out["offline_fp32"] = st
     fp32 = reqs
