@@ -114,6 +114,7 @@ struct SpreadArgs {
     T* grid;
     int perm_mul;  // warps visit atoms in the order (w * perm_mul) mod n, gcd(perm_mul, n) = 1
     double* zero_scal[3] = {nullptr, nullptr, nullptr};  // scalars thread 0 of block 0 sets to 0 (may be null)
+    unsigned long long* ctr_inc = nullptr;                // counter thread 0 of block 0 advances (may be null)
 };
 
 template <typename T>
@@ -689,6 +690,7 @@ __global__ void __launch_bounds__(256) k_spread_dip_cached(SpreadArgs<T> a, Sten
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x < 3 && a.zero_scal[threadIdx.x]) *a.zero_scal[threadIdx.x] = 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && a.ctr_inc) *a.ctr_inc += 1ull;
     if (warp >= a.n) return;  // whole warps: every lane takes part in the shuffles
     spread_dip_atom<T>(a, st, warp, lane);
 }
@@ -702,6 +704,10 @@ struct FieldCombine {
     double self1 = 0.0;
     double* dot_out = nullptr;
     double* zero1 = nullptr;
+    // with ctr: zero_pair[1 - ((*ctr - 1) & 1)] is cleared as well (the r.z slot of the CG step
+    // whose counter the spread has just advanced)
+    double* zero_pair = nullptr;
+    const unsigned long long* ctr = nullptr;
 };
 
 // k_gather_field with the cached stencil: lanes own whole (x, y) columns (lanes 0..31, then
@@ -773,6 +779,7 @@ __global__ void __launch_bounds__(256) k_gather_field_cached(int n, StencilCache
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (blockIdx.x == 0 && threadIdx.x == 0 && cmb.zero1) *cmb.zero1 = 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && cmb.zero_pair) cmb.zero_pair[1 - (int)((*cmb.ctr - 1ull) & 1ull)] = 0.0;
     double d[1] = {0.0};
     if (warp < n) d[0] = gather_field_atom<T>(st, g, phi, scale, out, cmb, warp, lane);
     if (cmb.dot_out) block_reduce_add<1>(d, cmb.dot_out);

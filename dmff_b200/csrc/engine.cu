@@ -123,7 +123,9 @@ struct dmffb_engine {
     cudaStream_t s1 = nullptr, s2 = nullptr;  // engine work stream (capturable) and matvec side stream
     cudaEvent_t e_fork = nullptr, e_join = nullptr, e_in = nullptr, e_out = nullptr;
     cudaEvent_t e_build = nullptr;  // end of the last neighbour build on its stream (no host wait)
-    cudaGraphExec_t cg_exec = nullptr;
+    cudaGraphExec_t cg_exec = nullptr;   // two CG steps
+    cudaGraphExec_t cg_exec1 = nullptr;  // one CG step (fused path: an odd last segment)
+    int64_t cg_graph1_launches = 0, cg_graph1_ffts = 0;
     std::vector<double> cg_key;       // what the instantiated graph bakes in
     std::vector<double> cg_seen_key;  // the previous solve's key
     bool use_graphs = true;
@@ -403,11 +405,17 @@ __global__ void k_cg_init(int n, const double* b, const double* Ax, const double
     p[k] = z[k];
 }
 
-// Ap may come in two parts (Ap + Ap2, p.Ap = s[2] + s[5]); s[5] stays 0 when Ap2 is null
+// Ap may come in two parts (Ap + Ap2, p.Ap = s[2] + s[5]); s[5] stays 0 when Ap2 is null.
+// With ctr (the CG step counter, already advanced for this step), slot = (*ctr - 1) mod 2 and
+// rz_new points at the slot pair s[0..1], this step's r.z going to rz_new[1 - slot].
 __global__ void k_cg_update(int n, const double* s, int slot, double* x, double* r, double* z, const double* p,
                             const double* Ap, const double* pol, double* rz_new, double* rr,
-                            const double* Ap2 = nullptr) {
+                            const double* Ap2 = nullptr, const unsigned long long* ctr = nullptr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ctr) {
+        slot = (int)((*ctr - 1ull) & 1ull);
+        rz_new += 1 - slot;
+    }
     const double pAp = s[2] + s[5];
     const double alpha = pAp != 0.0 ? s[slot] / pAp : 0.0;
     double v[1] = {0.0}, w[1] = {0.0};
@@ -427,9 +435,14 @@ __global__ void k_cg_update(int n, const double* s, int slot, double* x, double*
     block_reduce_add<1>(w, rr);
 }
 
+// with ctr (the CG step counter, not yet advanced for this step), slot_new = *ctr mod 2
 __global__ void k_cg_p(int n, const double* s, int slot_old, int slot_new, const double* z, double* p,
-                       double* zero = nullptr) {
+                       double* zero = nullptr, const unsigned long long* ctr = nullptr) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ctr) {
+        slot_new = (int)(*ctr & 1ull);
+        slot_old = 1 - slot_new;
+    }
     if (k == 0 && zero) *zero = 0.0;
     if (k >= 3 * n) return;
     const double beta = s[slot_old] != 0.0 ? s[slot_new] / s[slot_old] : 0.0;
@@ -780,15 +793,18 @@ int recip_pass(dmffb_engine* h, cudaStream_t s, const double* pos, const Box& bx
     return DMFFB_OK;
 }
 
-// One CG step's direction update and matvec A p on the PME path with the stencil cache: k_cg_p
-// forms p = z + beta p (beta from the previous step's r.z) and clears sc[5]; the real-space
-// matvec forks onto the side stream, writes d_fmv and reduces p.fmv into sc[5], overlapping the
-// whole reciprocal pass; the dipole spread clears sc[2] and sc[3] (rr); the gather writes
-// d_Ap = recip + diagonal p, reduces p.d_Ap into sc[2] and clears sc[1 - slot], the r.z slot
-// this step's update writes.  A p = d_Ap + d_fmv; the caller joins the side stream
-// (h->e_join) before the update reads them.
+// One CG step's direction update and matvec A p on the PME path with the stencil cache.  The
+// step's r.z slot comes from the step counter in sc[7] (zero at the start of the solve), so a
+// captured step runs right whatever the parity of the step it is replayed as: k_cg_p reads the
+// counter (slot = count mod 2), forms p = z + beta p (beta from the previous step's r.z) and
+// clears sc[5]; the real-space matvec forks onto the side stream, writes d_fmv and reduces p.fmv
+// into sc[5], overlapping the whole reciprocal pass; the dipole spread clears sc[2] and sc[3]
+// (rr) and advances the counter; the gather writes d_Ap = recip + diagonal p, reduces p.d_Ap into
+// sc[2] and clears sc[1 - slot], the r.z slot this step's update writes.  A p = d_Ap + d_fmv; the
+// caller joins the side stream (h->e_join) before the update reads them.
 template <typename T>
-int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, int slot) {
+int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc) {
+    unsigned long long* ctr = (unsigned long long*)(sc + 7);
     const MeshGeom g = mesh_geom(bx, h->K);
     SpreadArgs<T> sa;
     sa.n = h->n;
@@ -802,7 +818,8 @@ int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, 
     sa.perm_mul = h->perm_mul;
     sa.zero_scal[0] = sc + 2;
     sa.zero_scal[1] = sc + 3;
-    LAUNCH(h, s, KC_VEC, k_cg_p<<<nblk(3 * h->n, 256), 256, 0, s>>>(h->n, sc, 1 - slot, slot, h->d_z, h->d_p, sc + 5));
+    sa.ctr_inc = ctr;
+    LAUNCH(h, s, KC_VEC, k_cg_p<<<nblk(3 * h->n, 256), 256, 0, s>>>(h->n, sc, 1, 0, h->d_z, h->d_p, sc + 5, ctr));
     const bool fork = h->s2 && !h->prof;
     {
         CsrArgs c;
@@ -860,7 +877,8 @@ int cg_matvec_fused(dmffb_engine* h, cudaStream_t s, const Box& bx, double* sc, 
     cmb.pol = h->d_pol;
     cmb.self1 = -2.0 * DMFFB_DIELECTRIC * (k / 1.7724538509055159) * 2.0 * k * k / 3.0;
     cmb.dot_out = sc + 2;
-    cmb.zero1 = sc + (1 - slot);
+    cmb.zero_pair = sc;
+    cmb.ctr = ctr;
     LAUNCH(h, s, KC_GATHER_FIELD, k_gather_field_cached<T><<<nblk((int64_t)h->n * 32, 256), 256, 0, s>>>(
                                       h->n, stencil_cache<T>(h), g, (const T*)h->d_grid, 2.0 * DMFFB_DIELECTRIC, h->d_Ap,
                                       cmb));
@@ -1148,10 +1166,11 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     auto iteration = [&](int slot) -> int {
         int st2;
         if (fused) {
-            if ((st2 = cg_matvec_fused<T>(h, s, bx, sc, slot))) return st2;
+            if ((st2 = cg_matvec_fused<T>(h, s, bx, sc))) return st2;
             if (h->s2 && !h->prof) CK(cudaStreamWaitEvent(s, h->e_join, 0));
-            LAUNCH(h, s, KC_VEC, k_cg_update<<<nb3, 256, 0, s>>>(n, sc, slot, U, h->d_r, h->d_z, h->d_p, h->d_Ap,
-                                                               h->d_pol, sc + (1 - slot), sc + 3, h->d_fmv));
+            LAUNCH(h, s, KC_VEC, k_cg_update<<<nb3, 256, 0, s>>>(n, sc, 0, U, h->d_r, h->d_z, h->d_p, h->d_Ap,
+                                                               h->d_pol, sc, sc + 3, h->d_fmv,
+                                                               (const unsigned long long*)(sc + 7)));
             return DMFFB_OK;
         }
         // Ap = A p with p.Ap reduced into sc[2]; pAp, rr and the r.z slot this step writes are
@@ -1166,42 +1185,79 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
     // two iterations (slot 0 then 1) are captured once into a CUDA graph and replayed; the graph
     // bakes in pointers and the box, so it is captured on the second solve in a row with the same
     // ones (a one-off solve, such as a serving request of a new size, runs its launches directly
-    // and pays no capture and instantiation) and replayed while they stay the same
+    // and pays no capture and instantiation) and replayed while they stay the same.  The fused
+    // step takes its parity from the device step counter, so a one-step graph is captured beside
+    // it for a last segment of odd length.
     bool graphs = h->use_graphs && !h->prof;
     if (graphs) {
         std::vector<double> key = {(double)(uintptr_t)pos, (double)(uintptr_t)pairs, (double)npairs,
                                    (double)(uintptr_t)U, (double)(uintptr_t)h->d_csr_ent, (double)sizeof(T),
                                    (double)(uintptr_t)h->d_mvcoef, (double)(uintptr_t)h->d_csr_off,
-                                   (double)(h->fc_enabled ? h->fc_ok : 0), (double)(uintptr_t)h->d_fcG};
+                                   (double)(h->fc_enabled ? h->fc_ok : 0), (double)(uintptr_t)h->d_fcG,
+                                   (double)fused};
         for (int k = 0; k < 9; ++k) key.push_back(bx.h[k]);
         const bool repeat = key == h->cg_seen_key;
         h->cg_seen_key = key;
         if ((!h->cg_exec || key != h->cg_key) && !repeat) graphs = false;
     }
+    auto capture = [&](int steps, cudaGraphExec_t* exec, int64_t* launches, int64_t* ffts) -> int {
+        if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
+        cudaGraph_t g;
+        const int64_t l0 = h->n_launch, f0 = h->n_fft;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        int st0 = iteration(0);
+        if (!st0 && steps == 2) st0 = iteration(1);
+        cudaError_t ce = cudaStreamEndCapture(s, &g);
+        // captured launches run on replay: count them there
+        *launches = h->n_launch - l0;
+        *ffts = h->n_fft - f0;
+        h->n_launch = l0;
+        h->n_fft = f0;
+        if (st0) return st0;
+        if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        return DMFFB_OK;
+    };
     if (graphs) {
         const std::vector<double>& key = h->cg_seen_key;
         if (!h->cg_exec || key != h->cg_key) {
-            if (h->cg_exec) { cudaGraphExecDestroy(h->cg_exec); h->cg_exec = nullptr; }
-            cudaGraph_t g;
-            const int64_t l0 = h->n_launch, f0 = h->n_fft;
-            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            int st0 = iteration(0);
-            int st1 = st0 ? st0 : iteration(1);
-            cudaError_t ce = cudaStreamEndCapture(s, &g);
-            // captured launches run on replay: count them there
-            h->cg_graph_launches = h->n_launch - l0;
-            h->cg_graph_ffts = h->n_fft - f0;
-            h->n_launch = l0;
-            h->n_fft = f0;
-            if (st1) return st1;
-            if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(ce));
-            ce = cudaGraphInstantiate(&h->cg_exec, g, 0);
-            cudaGraphDestroy(g);
-            if (ce != cudaSuccess) return fail(h, DMFFB_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+            if ((st = capture(2, &h->cg_exec, &h->cg_graph_launches, &h->cg_graph_ffts))) return st;
+            if (h->cg_exec1) { cudaGraphExecDestroy(h->cg_exec1); h->cg_exec1 = nullptr; }
+            if (fused && (st = capture(1, &h->cg_exec1, &h->cg_graph1_launches, &h->cg_graph1_ffts))) return st;
             h->cg_key = key;
         }
     }
-    const int check_every = 4;  // host reads the residual every few iterations (no per-iteration sync)
+    // The host reads the residual every few steps (no per-step sync).  On the fused path, from the
+    // second read on, the residual's decay over the last segment predicts the steps still needed:
+    // a segment shorter than check_every then ends at the first step expected to converge.
+    const int check_every = 4;
+    double r_prev = -1.0;
+    int it_prev = 0;
+    auto run_steps = [&](int k) -> int {
+        int st2;
+        for (; k >= 2; k -= 2) {
+            if (graphs) {
+                CK(cudaGraphLaunch(h->cg_exec, s));
+                h->n_launch += h->cg_graph_launches;
+                h->n_fft += h->cg_graph_ffts;
+            } else {
+                if ((st2 = iteration(0))) return st2;
+                if ((st2 = iteration(1))) return st2;
+            }
+        }
+        if (k == 1) {
+            if (graphs) {
+                CK(cudaGraphLaunch(h->cg_exec1, s));
+                h->n_launch += h->cg_graph1_launches;
+                h->n_fft += h->cg_graph1_ffts;
+            } else if ((st2 = iteration(0))) {
+                return st2;
+            }
+        }
+        return DMFFB_OK;
+    };
     while (true) {
         CK(cudaMemcpyAsync(h->h_scal, sc + 3, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
@@ -1214,17 +1270,16 @@ int solve_dipoles(dmffb_engine* h, cudaStream_t s, const double* pos, const Box&
             break;
         }
         if (it >= h->max_iter) break;
-        for (int k = 0; k < check_every; k += 2) {
-            if (graphs) {
-                CK(cudaGraphLaunch(h->cg_exec, s));
-                h->n_launch += h->cg_graph_launches;
-                h->n_fft += h->cg_graph_ffts;
-            } else {
-                if ((st = iteration(0))) return st;
-                if ((st = iteration(1))) return st;
-            }
-            it += 2;
+        int k = check_every;
+        if (fused && r_prev > 0.0 && rms < r_prev && it > it_prev) {
+            const double rate = std::pow(rms / r_prev, 1.0 / (double)(it - it_prev));
+            const double need = std::log(h->cg_tol * rms_b / rms) / std::log(rate);
+            if (need > 0.0 && need < (double)check_every) k = std::max(1, (int)std::ceil(need));
         }
+        r_prev = rms;
+        it_prev = it;
+        if ((st = run_steps(k))) return st;
+        it += k;
     }
     res->n_iter = it;
     res->converged = conv ? 1 : 0;
@@ -2088,6 +2143,10 @@ int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* d) {
         cudaGraphExecDestroy(h->cg_exec);
         h->cg_exec = nullptr;
     }
+    if (h->cg_exec1) {
+        cudaGraphExecDestroy(h->cg_exec1);
+        h->cg_exec1 = nullptr;
+    }
     h->cg_key.clear();
     h->cg_seen_key.clear();
     h->params_set = false;
@@ -2118,6 +2177,7 @@ void dmffb_destroy(dmffb_engine* h) {
     for (int k = 0; k < 8; ++k) cudaEventDestroy(h->ev[k]);
     for (auto e : h->ev_pool) cudaEventDestroy(e);
     if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
+    if (h->cg_exec1) cudaGraphExecDestroy(h->cg_exec1);
     if (h->s2) cudaStreamDestroy(h->s2);
     if (h->s1) cudaStreamDestroy(h->s1);
     if (h->e_in) cudaEventDestroy(h->e_in);
