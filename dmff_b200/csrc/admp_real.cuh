@@ -553,7 +553,7 @@ enum { ROWS_ALL = 0, ROWS_UNSCALED = 1, ROWS_SCALED = 2 };
 // arithmetic) or only nbond != 0 rows (always FP64); the FP32 engine launches the last two so
 // that no warp mixes the two arithmetic paths.
 template <typename T, bool POL, int MODE, int ROWS = ROWS_ALL>
-__global__ void __launch_bounds__(128) k_admp_pair(PairArgs<T> a) {
+__global__ void __launch_bounds__(128, (sizeof(T) == 4 && ROWS == ROWS_UNSCALED && MODE == PAIR_FULL) ? 6 : 0) k_admp_pair(PairArgs<T> a) {
     const int64_t row = launch_row<ROWS>(a);
     int i = -1, j = -1, nb = 0;
     if (row < a.npairs) {
