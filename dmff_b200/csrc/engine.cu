@@ -1806,6 +1806,16 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
         c.coul = h->coul;
         c.grad = (T*)h->d_glr;
         c.scal = h->d_scal;
+        {
+            const double* m = bx.h;
+            const double V = fabs(det3(m));
+            for (int k = 0; k < 3; ++k) {
+                const double* u = m + 3 * ((k + 1) % 3);
+                const double* w = m + 3 * ((k + 2) % 3);
+                const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+                c.width[k] = V / sqrt(cx * cx + cy * cy + cz * cz);
+            }
+        }
         LAUNCH(h, s, KC_PAIR_FULL, k_nb_cells<T><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(c));
         CK(cudaGetLastError());
         // rows with a topological scale: the covalent rows within rc, FP64 for FP32 engines

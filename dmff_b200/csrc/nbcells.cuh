@@ -12,6 +12,8 @@
 //     per cell, the atom index in the w slot); atoms are taken in cell order, so the warps of a
 //     block share their candidates through L1 (with at least 5 cells per axis the 5 offsets of an
 //     axis are distinct cells, and a box of at least 2.5 rc has one image of a pair within rc);
+//   * stencil cells with no point within rc of the atom are skipped (per atom, from its position
+//     in its cell);
 //   * FP32 prefilter on float positions, the exact FP64 test of the list build (within_rc on the
 //     lower/higher orientation) inside a 2e-3 A band around rc, so the kept set is the list's
 //     set bit for bit;
@@ -39,6 +41,8 @@ struct NbCellArgs {
     Box boxd;
     double rc;
     int nc[3];                // half-width cells per axis (>= 5)
+    double width[3];          // perpendicular widths of the box (the distance between the faces
+                              // of constant fractional coordinate k)
     const int32_t* cell_start;
     NbArgs cov;               // covalent-map lookup (cov_ptr / cov_j / cov_nb over i < j)
     const int32_t* cov_lo;    // [n] smallest / largest covalent partner index (lo > hi: none)
@@ -122,6 +126,21 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
         const float rlo2 = rlo * rlo, rhi2 = rhi * rhi;
         int c3[3];
         cell_of(a.boxd, a.nc, pi, c3);
+        // the atom's fractional coordinates (as cell_of takes them): a stencil cell none of whose
+        // points lies within rc + 0.01 A of the atom is skipped (about a third of the forward half
+        // for half-width cells).  Orthorhombic boxes: the exact distance to the cell's box; others
+        // the lower bound max_k gap_k width_k (gap_k the fractional gap along k).  The margin
+        // covers the FP32 prefilter band (rc +- 2e-3 A) and the rounding of the binning, so the
+        // kept pairs are unchanged.
+        double sfr[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double v = pi[0] * a.boxd.hinv[k] + pi[1] * a.boxd.hinv[3 + k] + pi[2] * a.boxd.hinv[6 + k];
+            sfr[k] = v - floor(v);
+        }
+        const bool ortho = a.boxd.h[1] == 0.0 && a.boxd.h[2] == 0.0 && a.boxd.h[3] == 0.0 && a.boxd.h[5] == 0.0 &&
+                           a.boxd.h[6] == 0.0 && a.boxd.h[7] == 0.0;
+        const double rprune = a.rc + 0.01;
         int carry = 0;
         if (lane == 0) s_off[wl][0] = 0;
         for (int q0 = 0; q0 < NQ; q0 += 32) {
@@ -138,6 +157,18 @@ __global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
                 const int ce = a.cell_start[cc + 1];
                 if (q == 0) cs = max(cs, ks + 1);  // own cell: the atoms after i in cell order
                 cnt = max(ce - cs, 0);
+                if (q > 0) {
+                    const int dd[3] = {dx, dy, dz};
+                    double d2 = 0.0, dmax = 0.0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const double lo = (double)(c3[k] + dd[k]) / a.nc[k], hi = (double)(c3[k] + dd[k] + 1) / a.nc[k];
+                        const double gap = fmax(0.0, fmax(lo - sfr[k], sfr[k] - hi)) * a.width[k];
+                        d2 += gap * gap;
+                        dmax = fmax(dmax, gap);
+                    }
+                    if (ortho ? d2 > rprune * rprune : dmax > rprune) cnt = 0;
+                }
                 s_beg[wl][q] = cs;
             }
             int incl = cnt;

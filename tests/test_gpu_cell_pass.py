@@ -60,3 +60,26 @@ def test_cell_pass_matches_list_path_at_classical_box_density(precision):
         b1, b2 = np.array(r1.box_grad), np.array(r2.box_grad)
         assert np.abs(b2 - b1).max() <= (1e-10 if precision == "fp64" else 1e-5) * np.abs(b1).max()
         pos = pos + torch.tensor(rng.normal(0.0, 0.05, size=s["pos"].shape), device="cuda")
+
+
+def test_cell_pass_matches_list_path_triclinic():
+    """The same comparison in a sheared box (the cell pass's triclinic stencil bounds): 32 A block
+    at the classical box's density, box rows (32, 0, 0), (5, 32, 0), (-4, 6, 32)."""
+    scale = (32.0 / 70.0) ** 3
+    s = polymer_water_box(int(round(200 * scale)), 50, int(round(30000 * scale)), 32.0, seed=9, rc=10.0, ethresh=1e-5)
+    frac = s["pos"] @ np.linalg.inv(s["box"])
+    box = np.array([[32.0, 0.0, 0.0], [5.0, 32.0, 0.0], [-4.0, 6.0, 32.0]])
+    pos = torch.tensor(frac @ box, device="cuda")
+    s = dict(s, box=box)
+    lst = _engine(s, "fp32")
+    cel = _engine(s, "fp32")
+    cel.set_cell_pass(True)
+    lst.rebuild_internal_pairs(pos, box)
+    r1, F1 = lst.compute(pos, box)
+    F1 = F1.cpu().numpy().copy()
+    r2, F2 = cel.compute(pos, box)
+    F2 = F2.cpu().numpy().copy()
+    assert r2.n_pairs == r1.n_pairs > 1_000_000
+    for k in ("e_coul_real", "e_lj", "energy"):
+        assert abs(getattr(r2, k) - getattr(r1, k)) <= 2e-6 * abs(getattr(r1, k)), k
+    assert rel_force_rms(F2, F1) < 1e-5
