@@ -97,7 +97,7 @@ __device__ __forceinline__ void nb_cell_pair(const NbCellArgs<T>& a, int i, int 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(32 * kNbWarps) k_nb_cells(NbCellArgs<T> a) {
+__global__ void __launch_bounds__(32 * kNbWarps, sizeof(T) == 4 ? 4 : 0) k_nb_cells(NbCellArgs<T> a) {
     constexpr int S = 2, W = 2 * S + 1, NQ = (W * W * W + 1) / 2;  // offsets q0 = 62 .. 124 of the 5^3 stencil
     __shared__ int s_beg[kNbWarps][NQ];
     __shared__ int s_off[kNbWarps][NQ + 1];
