@@ -170,69 +170,75 @@ struct SelfArgs {
 };
 
 // self energy (pme.py:1183-1222), polarization penalty (pme.py:1225-1240), torque -> forces
+// One thread per (atom, frame slot s, component c): 12 per atom.  Thread (at, 0, 0) also adds the
+// Ewald self energy and the polarization penalty and writes tau_out; every thread forms the
+// atom's torque (permanent + self term) and maps it onto the force on the slot's atom along c
+// through the derivative of the local frame (build_frame's forward mode), so the twelve frame
+// derivatives of an atom run in parallel instead of in one thread.
+constexpr int kSelfTasks = 12;
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_self_frames(SelfArgs<T> a) {
-    const int at = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t task = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int at = (int)(task / kSelfTasks), sc = (int)(task - (int64_t)at * kSelfTasks);
+    const int s = sc / 3, c = sc - 3 * (sc / 3);
     double red[11];
 #pragma unroll
     for (int k = 0; k < 11; ++k) red[k] = 0.0;
     if (at < a.f.n) {
         const double D = DMFFB_DIELECTRIC;
-        double Qt[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Qt[k] = a.Qg[9 * at + k];
         double Ux = 0, Uy = 0, Uz = 0;
         if (a.U) { Ux = a.U[3 * at]; Uy = a.U[3 * at + 1]; Uz = a.U[3 * at + 2]; }
-        Qt[1] += Uz; Qt[2] += Ux; Qt[3] += Uy;
         double tau[3] = {(double)a.torque[3 * at], (double)a.torque[3 * at + 1], (double)a.torque[3 * at + 2]};
         if (a.lpme) {
             const double k = a.kappa;
             const double f0 = k / 1.7724538509055159;
             const double f1 = f0 * 2.0 * k * k / 3.0;
             const double f2 = f0 * 4.0 * k * k * k * k / 15.0;
-            double e = f0 * Qt[0] * Qt[0];
-            if (a.lmax_eff >= 1) e += f1 * (Qt[1] * Qt[1] + Qt[2] * Qt[2] + Qt[3] * Qt[3]);
-            if (a.lmax_eff >= 2) e += f2 * (Qt[4] * Qt[4] + Qt[5] * Qt[5] + Qt[6] * Qt[6] + Qt[7] * Qt[7] + Qt[8] * Qt[8]);
-            red[0] = -D * e;
+            if (sc == 0) {
+                double Qt[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) Qt[q] = a.Qg[9 * at + q];
+                Qt[1] += Uz; Qt[2] += Ux; Qt[3] += Uy;
+                double e = f0 * Qt[0] * Qt[0];
+                if (a.lmax_eff >= 1) e += f1 * (Qt[1] * Qt[1] + Qt[2] * Qt[2] + Qt[3] * Qt[3]);
+                if (a.lmax_eff >= 2) e += f2 * (Qt[4] * Qt[4] + Qt[5] * Qt[5] + Qt[6] * Qt[6] + Qt[7] * Qt[7] + Qt[8] * Qt[8]);
+                red[0] = -D * e;
+            }
             // torque of the self term: mu_perm x (-2 D f1 (mu_perm + U))  = -2 D f1 mu_perm x U
             const double mx = a.Qg[9 * at + 2], my = a.Qg[9 * at + 3], mz = a.Qg[9 * at + 1];
-            const double s = -2.0 * D * f1;
-            tau[0] += s * (my * Uz - mz * Uy);
-            tau[1] += s * (mz * Ux - mx * Uz);
-            tau[2] += s * (mx * Uy - my * Ux);
+            const double sf = -2.0 * D * f1;
+            tau[0] += sf * (my * Uz - mz * Uy);
+            tau[1] += sf * (mz * Ux - mx * Uz);
+            tau[2] += sf * (mx * Uy - my * Ux);
         }
-        if (a.U && a.pol) {
-            double p = a.pol[at];
-            p = p < 1e-8 ? 1e-8 : p;
-            red[1] = D * 0.5 / p * (Ux * Ux + Uy * Uy + Uz * Uz);
+        if (sc == 0) {
+            if (a.U && a.pol) {
+                double p = a.pol[at];
+                p = p < 1e-8 ? 1e-8 : p;
+                red[1] = D * 0.5 / p * (Ux * Ux + Uy * Uy + Uz * Uz);
+            }
+            if (a.tau_out) { a.tau_out[3 * at] = tau[0]; a.tau_out[3 * at + 1] = tau[1]; a.tau_out[3 * at + 2] = tau[2]; }
         }
-        if (a.tau_out) { a.tau_out[3 * at] = tau[0]; a.tau_out[3 * at + 1] = tau[1]; a.tau_out[3 * at + 2] = tau[2]; }
         if (a.lmax_eff >= 1 && a.f.axis_type[at] != 5 && a.f.axis_idx) {
             const int type = a.f.axis_type[at];
             const int nslot = (type == 2 || type == 3) ? 4 : (type == 4 ? 2 : 3);
-            for (int s = 0; s < nslot; ++s) {
+            if (s < nslot) {
                 const int atom = s == 0 ? at : a.f.axis_idx[3 * at + s - 1];
-                double g[3];
                 double nimg[3][3];
-                for (int c = 0; c < 3; ++c) {
-                    V3D X, Y, Z;
-                    build_frame(a.f, at, s, c, X, Y, Z, nimg);
-                    // omega = z x dz + (y . dx) z
-                    const double zx = Z.x.v, zy = Z.y.v, zz = Z.z.v;
-                    const double dzx = Z.x.d, dzy = Z.y.d, dzz = Z.z.d;
-                    const double ydx = Y.x.v * X.x.d + Y.y.v * X.y.d + Y.z.v * X.z.d;
-                    const double om0 = zy * dzz - zz * dzy + ydx * zx;
-                    const double om1 = zz * dzx - zx * dzz + ydx * zy;
-                    const double om2 = zx * dzy - zy * dzx + ydx * zz;
-                    g[c] = tau[0] * om0 + tau[1] * om1 + tau[2] * om2;
-                }
-                atomicAdd(a.grad + 3 * atom, g[0]);
-                atomicAdd(a.grad + 3 * atom + 1, g[1]);
-                atomicAdd(a.grad + 3 * atom + 2, g[2]);
-                if (a.want_box && s > 0) {
-                    for (int k = 0; k < 3; ++k)
-                        for (int c = 0; c < 3; ++c) red[2 + 3 * k + c] += -nimg[s - 1][k] * g[c];
-                }
+                V3D X, Y, Z;
+                build_frame(a.f, at, s, c, X, Y, Z, nimg);
+                // omega = z x dz + (y . dx) z
+                const double zx = Z.x.v, zy = Z.y.v, zz = Z.z.v;
+                const double dzx = Z.x.d, dzy = Z.y.d, dzz = Z.z.d;
+                const double ydx = Y.x.v * X.x.d + Y.y.v * X.y.d + Y.z.v * X.z.d;
+                const double om0 = zy * dzz - zz * dzy + ydx * zx;
+                const double om1 = zz * dzx - zx * dzz + ydx * zy;
+                const double om2 = zx * dzy - zy * dzx + ydx * zz;
+                const double g = tau[0] * om0 + tau[1] * om1 + tau[2] * om2;
+                atomicAdd(a.grad + 3 * atom + c, g);
+                if (a.want_box && s > 0)
+                    for (int k = 0; k < 3; ++k) red[2 + 3 * k + c] += -nimg[s - 1][k] * g;
             }
         }
     }

@@ -1395,7 +1395,7 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     sa.scal = h->d_scal + S_SELF;
     sa.tau_out = nullptr;
     if (h->lmax == 0) sa.f.axis_idx = nullptr;
-    LAUNCH(h, s, KC_SELF, k_self_frames<T><<<nblk(n, 32), 32, 0, s>>>(sa));
+    LAUNCH(h, s, KC_SELF, k_self_frames<T><<<nblk((int64_t)n * kSelfTasks, 128), 128, 0, s>>>(sa));
     if (forces) LAUNCH(h, s, KC_VEC, k_finalize_forces<T><<<nblk(3 * n, 256), 256, 0, s>>>(n, (const T*)h->d_gpair, h->d_grad, forces));
     CK(cudaGetLastError());
     h->have_pgrad = false;
