@@ -1969,12 +1969,19 @@ int upload_topology(dmffb_engine* h, const dmffb_admp_desc* d) {
     for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
     const int64_t nc = std::max<int64_t>(d->n_cov, 1);
     std::vector<int32_t> cj(nc), cn(nc), cur(cnt.begin(), cnt.end() - 1);
+    // each atom's smallest and largest covalent partner index (lo > hi: none): the neighbour
+    // build skips the map lookup for partners outside the range
+    std::vector<int32_t> plo(n, n), phi(n, -1);
     for (int64_t r = 0; r < d->n_cov; ++r) {
         int i = d->cov_rows[3 * r], j = d->cov_rows[3 * r + 1];
         int lo = std::min(i, j), hi = std::max(i, j);
         int k = cur[lo]++;
         cj[k] = hi;
         cn[k] = d->cov_rows[3 * r + 2];
+        plo[lo] = std::min(plo[lo], hi);
+        phi[lo] = std::max(phi[lo], hi);
+        plo[hi] = std::min(plo[hi], lo);
+        phi[hi] = std::max(phi[hi], lo);
     }
     int st;
     if (nc > h->cov_cap) {
@@ -1990,6 +1997,13 @@ int upload_topology(dmffb_engine* h, const dmffb_admp_desc* d) {
     CK(cudaMemcpyAsync(h->d_cov_ptr, cnt.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
     CK(cudaMemcpyAsync(h->d_cov_j, cj.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
     CK(cudaMemcpyAsync(h->d_cov_nb, cn.data(), nc * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    if (!h->d_cov_lo) {
+        if ((st = dalloc(h, &h->d_cov_lo, (size_t)h->n_cap * sizeof(int32_t))) ||
+            (st = dalloc(h, &h->d_cov_hi, (size_t)h->n_cap * sizeof(int32_t))))
+            return st;
+    }
+    CK(cudaMemcpyAsync(h->d_cov_lo, plo.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
+    CK(cudaMemcpyAsync(h->d_cov_hi, phi.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s1));
     CK(cudaStreamSynchronize(h->s1));  // the host vectors go out of scope
     return DMFFB_OK;
 }
@@ -2835,6 +2849,8 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     b.a.cov_ptr = h->d_cov_ptr;
     b.a.cov_j = h->d_cov_j;
     b.a.cov_nb = h->d_cov_nb;
+    b.a.cov_lo = h->d_cov_lo;
+    b.a.cov_hi = h->d_cov_hi;
     b.a.count = h->d_pcount;
     b.a.offset = h->d_poff;
     b.posf = h->d_posf;

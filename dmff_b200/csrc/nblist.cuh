@@ -26,6 +26,8 @@ struct NbArgs {
     const int32_t* cov_ptr;     // [n+1] rows of j > i
     const int32_t* cov_j;
     const int32_t* cov_nb;
+    const int32_t* cov_lo = nullptr;  // [n] smallest / largest covalent partner (either direction) or null
+    const int32_t* cov_hi = nullptr;
     int32_t* count;             // [n] (pass 0) per-atom pair counts
     const int64_t* offset;      // [n+1] (pass 1)
     int32_t* pairs;             // [cap*3]
@@ -540,6 +542,8 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
         int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1 && b.off_f) ? b.off_f[i] : 0;
         int cnt_h = 0, cnt_f = 0;
         int qc = 0;
+        // covalent partners of i lie in [plo, phi]: the map is read only for those
+        const int plo = a.cov_lo ? a.cov_lo[i] : 0, phi = a.cov_hi ? a.cov_hi[i] : a.n;
         const bool use_mask = b.mask && (total + 31) / 32 <= b.mask_stride;
         uint32_t* mrow = use_mask ? b.mask + (size_t)i * b.mask_stride : nullptr;
         for (int base = 0; base < total; base += 32) {
@@ -614,7 +618,7 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
             if (PASS == 0 && use_mask && lane == 0) mrow[base >> 5] = mf;
             if (PASS == 1) {
                 if (keep) {
-                    const int nbd = j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i);
+                    const int nbd = (j < plo || j > phi) ? 0 : (j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i));
                     int sidx = nbd - 1;
                     if (sidx < 0) sidx += 6;
                     const int64_t sf_ = out_f + __popc(mf & lt);
