@@ -75,6 +75,12 @@ struct dmffb_engine {
     double *d_b = nullptr, *d_r = nullptr, *d_z = nullptr, *d_p = nullptr, *d_Ap = nullptr, *d_fr = nullptr;
     double* d_gQ = nullptr;
     double* d_fmv = nullptr;  // CSR matvec output [3n]
+    // slots of the single-pass neighbour build (k_pairs_cell pass 2): capacities per atom from
+    // the largest counts of the last two-pass build (0: no slots yet)
+    int32_t* d_ell_rows = nullptr;  // [n_cap * ell_cap_h * 3]
+    int32_t* d_ell_ent = nullptr;   // [n_cap * ell_cap_f]
+    int ell_cap_h = 0, ell_cap_f = 0;
+    int* d_maxdeg = nullptr;        // [2]
     int64_t* d_csr_off = nullptr;
     int32_t *d_csr_ent = nullptr, *d_csr_deg = nullptr;
     int64_t csr_cap = 0;
@@ -2189,7 +2195,7 @@ void dmffb_destroy(dmffb_engine* h) {
                     h->d_q, h->d_qT, h->d_type, h->d_sigtt, h->d_epstt, h->d_dq, h->d_dsig, h->d_deps,
                     h->d_tidx[0], h->d_tidx[1], h->d_tidx[2], h->d_tprm[0], h->d_tprm[1], h->d_tprm[2],
                     h->d_tdprm[0], h->d_tdprm[1], h->d_tdprm[2], h->d_dQloc, h->d_dpa, h->d_dth, h->d_dpol, h->d_dsr, h->d_srows, h->d_nsel, h->d_cubsel,
-                    h->d_cub, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_fcW, h->d_pcg, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
+                    h->d_cub, h->d_ell_rows, h->d_ell_ent, h->d_maxdeg, h->d_stc_org, h->d_stc_w, h->d_nbmask, h->d_covrows, h->d_cov_lo, h->d_cov_hi, h->d_fcG, h->d_fcW, h->d_pcg, h->d_posc, h->d_srp, h->d_srdp, h->d_srgrad};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
@@ -2882,6 +2888,57 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
     const size_t stage_bytes = (size_t)chmax * sizeof(float4);
     const bool staged = stage_bytes <= kNbStageBytes;
     const bool ortho = m[1] == 0.0 && m[2] == 0.0 && m[3] == 0.0 && m[5] == 0.0 && m[6] == 0.0 && m[7] == 0.0;
+    if (!h->d_maxdeg && (st = dalloc(h, &h->d_maxdeg, 2 * sizeof(int)))) return st;
+    int maxdeg[2] = {0, 0};
+    // Single pass: the distance tests run once, each atom's rows and CSR entries go to its slots,
+    // the scans of the counts place them and k_ell_compact copies them there (the same row set
+    // and CSR as the two passes below).  Taken when the last two-pass build sized the slots; if a
+    // count or a total outgrows its capacity, the two-pass build runs after all.
+    if (fine && staged && h->ell_cap_h > 0 && (!want_csr || h->ell_cap_f > 0) && h->d_pairs &&
+        (!want_csr || h->d_csr_ent)) {
+        Nb2Args e = b;
+        e.mask = nullptr;
+        e.mask_stride = 0;
+        e.ell_rows = h->d_ell_rows;
+        e.ell_ent = want_csr ? h->d_ell_ent : nullptr;
+        e.ell_cap_h = h->ell_cap_h;
+        e.ell_cap_f = h->ell_cap_f;
+        e.maxdeg = h->d_maxdeg;
+        CK(cudaMemsetAsync(h->d_maxdeg, 0, 2 * sizeof(int), s));
+        if (ortho) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<2, 2, kNbWarps, true><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(e, chmax));
+        else LAUNCH(h, s, KC_NBLIST, k_pairs_cell<2, 2, kNbWarps, false><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(e, chmax));
+        CK(cudaMemsetAsync(h->d_poff, 0, sizeof(int64_t), s));
+        tb = h->cub_bytes;
+        LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount, h->d_poff + 1, n, s));
+        if (want_csr) {
+            CK(cudaMemsetAsync(h->d_csr_off, 0, sizeof(int64_t), s));
+            tb = h->cub_bytes;
+            LAUNCH(h, s, KC_NBLIST, cub::DeviceScan::InclusiveSum(h->d_cub, tb, h->d_pcount_f, h->d_csr_off + 1, n, s));
+        }
+        LAUNCH(h, s, KC_NBLIST, k_ell_compact<<<nblk((int64_t)n * 32, 256), 256, 0, s>>>(
+                                    n, h->d_pcount, h->d_pcount_f, h->d_poff, h->d_csr_off, h->d_ell_rows, h->ell_cap_h,
+                                    want_csr ? h->d_ell_ent : nullptr, h->ell_cap_f, h->d_pairs, h->pair_cap,
+                                    want_csr ? h->d_csr_ent : nullptr, h->csr_cap));
+        CK(cudaGetLastError());
+        int64_t tot1[2] = {0, 0};
+        if (want_csr) CK(cudaMemcpyAsync(&tot1[1], h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&tot1[0], h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(maxdeg, h->d_maxdeg, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (maxdeg[0] <= h->ell_cap_h && (!want_csr || maxdeg[1] <= h->ell_cap_f) && tot1[0] <= h->pair_cap &&
+            (!want_csr || tot1[1] <= h->csr_cap)) {
+            if (h->prof) prof_collect(h);
+            if (!h->e_build) CK(cudaEventCreateWithFlags(&h->e_build, cudaEventDisableTiming));
+            CK(cudaEventRecord(h->e_build, s));
+            h->npairs = tot1[0];
+            h->have_pairs = true;
+            h->pairs_gen++;
+            h->csr_from_build = want_csr;
+            return DMFFB_OK;
+        }
+    }
+    b.maxdeg = h->d_maxdeg;
+    CK(cudaMemsetAsync(h->d_maxdeg, 0, 2 * sizeof(int), s));
     if (fine && !staged) LAUNCH(h, s, KC_NBLIST, k_pairs_warp3<0, 2><<<nblk((int64_t)n * 32, 32 * kNbWarps), 32 * kNbWarps, 0, s>>>(b));
     else if (fine && ortho) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<0, 2, kNbWarps, true><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
     else if (fine) LAUNCH(h, s, KC_NBLIST, k_pairs_cell<0, 2, kNbWarps, false><<<ncell, 32 * kNbWarps, stage_bytes, s>>>(b, chmax));
@@ -2897,7 +2954,24 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
         CK(cudaMemcpyAsync(&tot[1], h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     }
     CK(cudaMemcpyAsync(&tot[0], h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(maxdeg, h->d_maxdeg, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    // slots for the next build's single pass: the largest counts with an eighth (at least 16) of
+    // headroom, for the cell-staged kernel only (the warp-per-atom kernels leave maxdeg at 0)
+    if (fine && staged && maxdeg[0] > 0) {
+        const int ch = maxdeg[0] + std::max(16, maxdeg[0] / 8), cf = maxdeg[1] + std::max(16, maxdeg[1] / 8);
+        if (ch > h->ell_cap_h || (want_csr && cf > h->ell_cap_f)) {
+            if (h->d_ell_rows) cudaFree(h->d_ell_rows);
+            if (h->d_ell_ent) cudaFree(h->d_ell_ent);
+            h->d_ell_rows = nullptr;
+            h->d_ell_ent = nullptr;
+            h->ell_cap_h = h->ell_cap_f = 0;
+            if ((st = dalloc(h, &h->d_ell_rows, (size_t)h->n_cap * ch * 3 * sizeof(int32_t)))) return st;
+            if (want_csr && (st = dalloc(h, &h->d_ell_ent, (size_t)h->n_cap * cf * sizeof(int32_t)))) return st;
+            h->ell_cap_h = ch;
+            h->ell_cap_f = want_csr ? cf : 0;
+        }
+    }
     if (tot[0] > h->pair_cap) {
         if (h->d_pairs) cudaFree(h->d_pairs);
         h->pair_cap = (int64_t)(tot[0] * 1.3) + 64;  // headroom as in nblist.py:37-38

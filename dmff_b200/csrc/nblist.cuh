@@ -248,6 +248,14 @@ struct Nb2Args {
     // reads them instead of repeating the distance tests (null: no masks)
     uint32_t* mask = nullptr;
     int mask_stride = 0;
+    // single-pass build (k_pairs_cell pass 2): the distance tests run once and each atom's full-
+    // list entries and half rows go to fixed slots, ell_ent[i * ell_cap_f + k] and
+    // ell_rows[3 (i * ell_cap_h + k)], which k_ell_compact then copies to the offsets the scans
+    // of the true counts give; slots past a capacity are dropped (the counts and maxdeg tell)
+    int32_t* ell_ent = nullptr;
+    int32_t* ell_rows = nullptr;
+    int ell_cap_f = 0, ell_cap_h = 0;
+    int* maxdeg = nullptr;  // [2] largest half-row and full-list count over the atoms (passes 0 and 2)
 };
 
 template <int PASS>
@@ -539,7 +547,13 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
         const int i = a.cell_atoms[cs0 + ai];
         const double* pi = a.pos + 3 * i;
         const float pix = b.posf[4 * i], piy = b.posf[4 * i + 1], piz = b.posf[4 * i + 2];
-        int64_t out_h = (PASS == 1) ? a.offset[i] : 0, out_f = (PASS == 1 && b.off_f) ? b.off_f[i] : 0;
+        const int64_t base_h = PASS == 2 ? (int64_t)i * b.ell_cap_h : 0, base_f = PASS == 2 ? (int64_t)i * b.ell_cap_f : 0;
+        int64_t out_h = (PASS == 1) ? a.offset[i] : base_h, out_f = (PASS == 1 && b.off_f) ? b.off_f[i] : base_f;
+        // where this pass writes: the final rows / CSR (pass 1) or the atom's slots (pass 2)
+        int32_t* const rows_out = PASS == 2 ? b.ell_rows : a.pairs;
+        int32_t* const ent_out = PASS == 2 ? b.ell_ent : b.ent;
+        const int64_t lim_h = PASS == 2 ? base_h + b.ell_cap_h : a.cap;
+        const int64_t lim_f = PASS == 2 ? base_f + b.ell_cap_f : b.cap_f;
         int cnt_h = 0, cnt_f = 0;
         int qc = 0;
         // covalent partners of i lie in [plo, phi]: the map is read only for those
@@ -616,19 +630,19 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
             const unsigned mf = __ballot_sync(0xffffffffu, keep);
             const unsigned mh = __ballot_sync(0xffffffffu, up);
             if (PASS == 0 && use_mask && lane == 0) mrow[base >> 5] = mf;
-            if (PASS == 1) {
+            if (PASS == 1 || PASS == 2) {
                 if (keep) {
                     const int nbd = (j < plo || j > phi) ? 0 : (j > i ? lookup_nbond(a, i, j) : lookup_nbond(a, j, i));
                     int sidx = nbd - 1;
                     if (sidx < 0) sidx += 6;
                     const int64_t sf_ = out_f + __popc(mf & lt);
-                    if (b.ent && sf_ < b.cap_f) b.ent[sf_] = j | (sidx << 28);
+                    if (ent_out && sf_ < lim_f) ent_out[sf_] = j | (sidx << 28);
                     if (up) {
                         const int64_t sh = out_h + __popc(mh & lt);
-                        if (sh < a.cap) {
-                            a.pairs[3 * sh] = i;
-                            a.pairs[3 * sh + 1] = j;
-                            a.pairs[3 * sh + 2] = nbd;
+                        if (sh < lim_h) {
+                            rows_out[3 * sh] = i;
+                            rows_out[3 * sh + 1] = j;
+                            rows_out[3 * sh + 2] = nbd;
                         }
                     }
                 }
@@ -639,10 +653,46 @@ __global__ void __launch_bounds__(32 * NW) k_pairs_cell(Nb2Args b, int chmax) {
                 cnt_h += __popc(mh);
             }
         }
-        if (PASS == 0 && lane == 0) {
+        if (PASS == 2) {
+            cnt_h = (int)(out_h - base_h);
+            cnt_f = (int)(out_f - base_f);
+        }
+        if (PASS != 1 && lane == 0) {
             a.count[i] = cnt_h;
             if (b.count_f) b.count_f[i] = cnt_f;
+            if (b.maxdeg) {
+                atomicMax(b.maxdeg, cnt_h);
+                atomicMax(b.maxdeg + 1, cnt_f);
+            }
         }
+    }
+}
+
+// Copies each atom's slots of the single-pass build to its offsets in the half rows and the CSR
+// (one warp per atom); nothing is written past the capacities, which the caller checks against
+// the totals before it uses the lists.
+static __global__ void k_ell_compact(int n, const int32_t* count_h, const int32_t* count_f, const int64_t* off_h,
+                                     const int64_t* off_f, const int32_t* ell_rows, int cap_h, const int32_t* ell_ent,
+                                     int cap_f, int32_t* rows, int64_t rows_cap, int32_t* ent, int64_t ent_cap) {
+    const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int nh = min(count_h[i], cap_h);
+    const int64_t bh = off_h[i];
+    for (int k = lane; k < nh; k += 32) {
+        if (bh + k >= rows_cap) break;
+        const int32_t* src = ell_rows + 3 * ((int64_t)i * cap_h + k);
+        int32_t* dst = rows + 3 * (bh + k);
+        dst[0] = src[0];
+        dst[1] = src[1];
+        dst[2] = src[2];
+    }
+    if (!ent) return;
+    const int nf = min(count_f[i], cap_f);
+    const int64_t bf = off_f[i];
+    for (int k = lane; k < nf; k += 32) {
+        if (bf + k >= ent_cap) break;
+        ent[bf + k] = ell_ent[(int64_t)i * cap_f + k];
     }
 }
 
