@@ -81,6 +81,14 @@ struct dmffb_engine {
     int32_t* d_ell_ent = nullptr;   // [n_cap * ell_cap_f]
     int ell_cap_h = 0, ell_cap_f = 0;
     int* d_maxdeg = nullptr;        // [2]
+    // a single-pass build whose totals are still on their way to the host: nb_finish waits for
+    // them when the list is first used (and rebuilds with two passes if a slot overflowed)
+    bool nb_pending = false, nb_want_csr = false;
+    cudaEvent_t e_nbtot = nullptr;
+    int64_t* h_nbtot = nullptr;     // pinned [4]: half rows, CSR entries, largest counts (2 x int32)
+    cudaStream_t nb_stream = nullptr;
+    const double* nb_pos = nullptr;
+    double nb_box[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int64_t* d_csr_off = nullptr;
     int32_t *d_csr_ent = nullptr, *d_csr_deg = nullptr;
     int64_t csr_cap = 0;
@@ -217,6 +225,10 @@ struct dmffb_engine {
     int64_t bk_cap = 0;
     std::map<std::array<int, 3>, std::pair<cufftHandle, cufftHandle>> plan_cache;  // mesh -> (R2C, C2R)
 };
+
+// completion of a single-pass neighbour build (defined after the kernels)
+int nb_finish(dmffb_engine* h);
+void nb_discard(dmffb_engine* h);
 
 namespace {
 
@@ -1309,20 +1321,10 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     memset(res, 0, sizeof(*res));
     const int n = h->n;
     int st;
-    if (!pairs) {
-        if (!h->have_pairs)
-            if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
-        if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
-        pairs = h->d_pairs;
-        npairs = h->npairs;
-    }
-    res->n_pairs = npairs;
-    h->last_pairs = pairs;
-    h->last_npairs = npairs;
-    h->last_U = U;
-    h->have_last = true;
-    if (sizeof(T) == 4 && npairs > 0)
-        if ((st = scaled_rows(h, s, pairs, npairs))) return st;
+    const bool own_list = !pairs;
+    if (own_list && !h->have_pairs)
+        if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+    if (own_list && h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
     if (h->timing) CK(cudaEventRecord(h->ev[0], s));
     CK(cudaMemsetAsync(h->d_scal, 0, N_SCAL * sizeof(double), s));
     CK(cudaMemsetAsync(h->d_gpair, 0, (size_t)3 * n * sizeof(T), s));
@@ -1342,6 +1344,20 @@ int compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const doubl
     pa.Qg = h->d_Qg;
     LAUNCH(h, s, KC_PREP, k_prepare<T><<<nblk(n, 128), 128, 0, s>>>(pa));
     CK(cudaGetLastError());
+    // the work above needs no pair list: it runs while a single-pass build's totals come back
+    if (own_list) {
+        if ((st = nb_finish(h))) return st;
+        if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
+        pairs = h->d_pairs;
+        npairs = h->npairs;
+    }
+    res->n_pairs = npairs;
+    h->last_pairs = pairs;
+    h->last_npairs = npairs;
+    h->last_U = U;
+    h->have_last = true;
+    if (sizeof(T) == 4 && npairs > 0)
+        if ((st = scaled_rows(h, s, pairs, npairs))) return st;
     if (h->timing) CK(cudaEventRecord(h->ev[1], s));
     if (h->lpol && !h->fixed_U) {
         if ((st = solve_dipoles<T>(h, s, pos, bx, pairs, npairs, U, res))) return st;
@@ -1603,6 +1619,7 @@ int disp_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, const 
     if (!pairs) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if ((st = nb_finish(h))) return st;
         if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
@@ -1767,6 +1784,7 @@ int classical_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, c
     if (nonbonded && !pairs && !cellpass) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if ((st = nb_finish(h))) return st;
         if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
@@ -2078,6 +2096,33 @@ int setup_mesh(dmffb_engine* h) {
 
 }  // namespace
 
+// Completes a single-pass build: waits for its totals; if a count or a total outgrew its
+// capacity, the list is rebuilt with the two passes (which resize the slots) from the positions
+// the build was given, on its stream.
+int nb_finish(dmffb_engine* h) {
+    if (!h->nb_pending) return DMFFB_OK;
+    h->nb_pending = false;
+    CK(cudaEventSynchronize(h->e_nbtot));
+    const int* md = (const int*)(h->h_nbtot + 2);
+    if (md[0] <= h->ell_cap_h && (!h->nb_want_csr || md[1] <= h->ell_cap_f) && h->h_nbtot[0] <= h->pair_cap &&
+        (!h->nb_want_csr || h->h_nbtot[1] <= h->csr_cap)) {
+        h->npairs = h->h_nbtot[0];
+        return DMFFB_OK;
+    }
+    h->have_pairs = false;
+    h->ell_cap_h = h->ell_cap_f = 0;  // the two passes this time
+    return dmffb_admp_build_neighbors(h, (void*)h->nb_stream, h->nb_pos, h->nb_box);
+}
+
+// Drops a single-pass build whose list will not be used (the engine is reconfigured, staged rows
+// replace the list, or it is destroyed) once its copies to the host are done.
+void nb_discard(dmffb_engine* h) {
+    if (!h->nb_pending) return;
+    cudaEventSynchronize(h->e_nbtot);
+    h->nb_pending = false;
+    h->have_pairs = false;
+}
+
 // ====================================================================== C ABI
 extern "C" {
 
@@ -2165,6 +2210,7 @@ int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* d) {
     if ((st = upload_topology(h, d))) return st;
     if (h->lpme && (st = setup_mesh(h))) return st;
     // everything derived from the previous system is stale
+    nb_discard(h);
     h->have_pairs = false;
     h->npairs = 0;
     h->csr_from_build = false;
@@ -2186,6 +2232,9 @@ int dmffb_admp_reconfigure(dmffb_engine* h, const dmffb_admp_desc* d) {
 
 void dmffb_destroy(dmffb_engine* h) {
     if (!h) return;
+    nb_discard(h);
+    if (h->h_nbtot) cudaFreeHost(h->h_nbtot);
+    if (h->e_nbtot) cudaEventDestroy(h->e_nbtot);
     void* ptrs[] = {h->d_axis_type, h->d_axis_idx, h->d_cov_ptr, h->d_cov_j, h->d_cov_nb, h->d_Qloc, h->d_pol,
                     h->d_thole, h->d_polsix, h->d_pos, h->d_U, h->d_forces, h->d_posT, h->d_Qg, h->d_QgT,
                     h->d_gpair, h->d_torque, h->d_fieldT, h->d_grad, h->d_scal, h->d_b, h->d_r, h->d_z, h->d_p,
@@ -2274,6 +2323,7 @@ int dmffb_admp_compute_host(dmffb_engine* h, const double* pos, const double* bo
     CK(cudaMemcpyAsync(h->d_pos, pos, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     int32_t* dp = nullptr;
     if (pairs) {  // staged in the engine's pair buffer (grown when short)
+        nb_discard(h);
         if (npairs > h->pair_cap) {
             CK(cudaStreamSynchronize(s));
             if (h->d_pairs) cudaFree(h->d_pairs);
@@ -2567,6 +2617,10 @@ int dmffb_admp_field(dmffb_engine* h, void* stream, const double* pos, const dou
             int st = dmffb_admp_build_neighbors(h, stream, pos, box);
             if (st) return st;
         }
+        {
+            int st = nb_finish(h);
+            if (st) return st;
+        }
         if (h->e_build) CK(cudaStreamWaitEvent((cudaStream_t)stream, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
@@ -2758,6 +2812,7 @@ int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, cons
 
 int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box) {
     if (!h || !pos || !box) return DMFFB_BAD_ARG;
+    if (h->nb_pending) nb_discard(h);  // this build replaces it
     cudaStream_t s = (cudaStream_t)stream;
     const int n = h->n;
     Box bx;
@@ -2920,22 +2975,32 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
                                     want_csr ? h->d_ell_ent : nullptr, h->ell_cap_f, h->d_pairs, h->pair_cap,
                                     want_csr ? h->d_csr_ent : nullptr, h->csr_cap));
         CK(cudaGetLastError());
-        int64_t tot1[2] = {0, 0};
-        if (want_csr) CK(cudaMemcpyAsync(&tot1[1], h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(&tot1[0], h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(maxdeg, h->d_maxdeg, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        if (maxdeg[0] <= h->ell_cap_h && (!want_csr || maxdeg[1] <= h->ell_cap_f) && tot1[0] <= h->pair_cap &&
-            (!want_csr || tot1[1] <= h->csr_cap)) {
-            if (h->prof) prof_collect(h);
-            if (!h->e_build) CK(cudaEventCreateWithFlags(&h->e_build, cudaEventDisableTiming));
-            CK(cudaEventRecord(h->e_build, s));
-            h->npairs = tot1[0];
-            h->have_pairs = true;
-            h->pairs_gen++;
-            h->csr_from_build = want_csr;
-            return DMFFB_OK;
+        // the totals travel to pinned memory behind an event; no host wait here (nb_finish)
+        if (!h->h_nbtot && cudaMallocHost((void**)&h->h_nbtot, 4 * sizeof(int64_t)) != cudaSuccess)
+            return fail(h, DMFFB_OOM, "cudaMallocHost failed");
+        h->h_nbtot[0] = h->h_nbtot[1] = h->h_nbtot[2] = h->h_nbtot[3] = 0;
+        if (want_csr) CK(cudaMemcpyAsync(h->h_nbtot + 1, h->d_csr_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(h->h_nbtot, h->d_poff + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(h->h_nbtot + 2, h->d_maxdeg, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (!h->e_nbtot) CK(cudaEventCreateWithFlags(&h->e_nbtot, cudaEventDisableTiming));
+        CK(cudaEventRecord(h->e_nbtot, s));
+        if (!h->e_build) CK(cudaEventCreateWithFlags(&h->e_build, cudaEventDisableTiming));
+        CK(cudaEventRecord(h->e_build, s));
+        h->nb_pending = true;
+        h->nb_want_csr = want_csr;
+        h->nb_stream = s;
+        h->nb_pos = pos;
+        for (int k = 0; k < 9; ++k) h->nb_box[k] = box[k];
+        h->npairs = 0;
+        h->have_pairs = true;
+        h->pairs_gen++;
+        h->csr_from_build = want_csr;
+        if (h->prof) {
+            const int stf = nb_finish(h);
+            if (stf) return stf;
+            prof_collect(h);
         }
+        return DMFFB_OK;
     }
     b.maxdeg = h->d_maxdeg;
     CK(cudaMemsetAsync(h->d_maxdeg, 0, 2 * sizeof(int), s));
@@ -3009,6 +3074,10 @@ int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos,
 int dmffb_engine_pairs(dmffb_engine* h, void* stream, int32_t* pairs_out, int64_t capacity, int64_t* npairs_out) {
     if (!h || !npairs_out) return fail(h, DMFFB_BAD_ARG, "null argument");
     if (!h->have_pairs) return fail(h, DMFFB_BAD_ARG, "the engine has no neighbour list yet");
+    {
+        const int st = nb_finish(h);
+        if (st) return st;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     *npairs_out = h->npairs;
     if (h->npairs > capacity || (!pairs_out && h->npairs > 0)) {
@@ -3141,6 +3210,7 @@ int pairwise_compute_impl(dmffb_engine* h, cudaStream_t s, const double* pos, co
     if (!pairs) {
         if (!h->have_pairs)
             if ((st = dmffb_admp_build_neighbors(h, (void*)s, pos, box))) return st;
+        if ((st = nb_finish(h))) return st;
         if (h->e_build) CK(cudaStreamWaitEvent(s, h->e_build, 0));
         pairs = h->d_pairs;
         npairs = h->npairs;
