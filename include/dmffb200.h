@@ -189,7 +189,11 @@ int dmffb_admp_backward(dmffb_engine* h, void* stream, const dmffb_admp_cotangen
 int dmffb_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box, double rc,
                           int32_t* pairs_out, int64_t capacity, int64_t* npairs_out);
 
-/* Rebuild the engine-owned pair list used when compute() gets pairs == NULL. */
+/* Rebuild the engine-owned pair list used when compute() gets pairs == NULL.  From an engine's
+ * second build on, this returns without waiting for the device: the row count reaches the host
+ * behind an event, and the list's first user (compute(), dmffb_engine_pairs) waits for it.  The
+ * build reads pos on the given stream; if a slot outgrows its capacity, that first user rebuilds
+ * the list from the same pos pointer, so keep the positions unchanged until then. */
 int dmffb_admp_build_neighbors(dmffb_engine* h, void* stream, const double* pos, const double* box);
 
 /* Copy of the engine's own neighbour list (the rows compute() uses when pairs == NULL), the
